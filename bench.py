@@ -1,0 +1,436 @@
+"""Throughput of the mgbrain_b200 simulation core on the large Brunel network.
+
+Workload (one bench step = 10,000 timesteps = 1 s simulated at dt = 0.1 ms):
+  1,000,000 LIFB neurons (800k exc, 200k inh; V_th 20 mV, V_reset 10 mV,
+  t_ref 2 ms, leak dt/tau_m = 0.005, V0 ~ U[0, 20 mV)) plus 100,000 POISSON
+  inputs at 20 Hz (0.002 per step); fixed in-degree 800 exc + 200 inh + 100
+  external per neuron (1.1e9 synapses, 8 B each on the device), J = 0.1 mV,
+  g = 5, delays uniform in 10..50 steps.  Synthetic, seeded, generated on
+  the device.  A driven variant (inputs at 200 Hz) is measured beside it
+  because the network as specified is quiescent apart from its inputs.
+
+Metric: synaptic events delivered per second of wall time (value), with
+simulated seconds per wall second and the HBM roofline of the dominant
+kernel.  `value` is device time over K bench steps (CUDA events on the
+core's stream, inputs resident); `e2e` goes through the C ABI with the
+POISSON rates copied from pinned host memory and the raster read back every
+bench step.  The CSR (8.8 GB) is larger than L2, so no flush is needed.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+With N > 1 every rank advances its own independent instance (replicas);
+value is the sum over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "synaptic events/s & sim-s per wall-s, 1M-neuron Brunel; % of HBM roofline"
+DT = 1e-4
+CHUNK = 10_000            # timesteps per bench step (1 s simulated)
+NE, NI, NP = 800_000, 200_000, 100_000
+KE, KI, KX = 800, 200, 100
+J, G = 1e-4, 5.0
+DMIN, DMAX = 10, 50
+NU_STEP = 0.002           # 20 Hz at 0.1 ms
+NU_DRIVEN = 0.02          # 200 Hz
+
+
+def workload(scale=1.0, nu=NU_STEP, seed=1):
+    ne, ni, nx = int(NE * scale), int(NI * scale), int(NP * scale)
+    n = ne + ni + nx
+    pops = [(0, ne, 5), (ne, ni, 5), (ne + ni, nx, 2)]   # LIFB, LIFB, POISSON
+    projs = []
+    for tgt in (0, 1):
+        projs += [(0, tgt, KE, J, DMIN, DMAX), (1, tgt, KI, -G * J, DMIN, DMAX),
+                  (2, tgt, KX, J, DMIN, DMAX)]
+    lif = np.zeros(30, np.float32)
+    lif[0], lif[3], lif[4], lif[8] = DT, 0.01, 0.02, 0.002
+    rate = np.zeros(n, np.float32)
+    rate[ne + ni:] = nu
+    v0 = np.random.default_rng(seed).uniform(0.0, 0.02, n).astype(np.float32)
+    return dict(n=n, n_lif=ne + ni, pops=pops, projs=projs, lif=lif, rate=rate, v0=v0)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------
+# CPU legs (the oracle restatement of the reference path; no GPU)
+# --------------------------------------------------------------------------
+def oracle_sim(w, threads):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import mgb_testlib as T
+    L = T.oracle()
+    P = np.array(w["pops"], np.int32)
+    R = w["projs"]
+    arr = lambda x, dt: np.ascontiguousarray(x, dt)  # noqa: E731
+    keep = [arr(P[:, 0], np.int32), arr(P[:, 1], np.int32), arr(P[:, 2], np.int32),
+            arr([r[0] for r in R], np.int32), arr([r[1] for r in R], np.int32),
+            arr([r[2] for r in R], np.int32), arr([r[3] for r in R], np.float32),
+            arr([r[4] for r in R], np.int32), arr([r[5] for r in R], np.int32)]
+    h = L.mgbo_create_fixed_indegree(*[T._p(k) for k in keep[:3]], len(P),
+                                     *[T._p(k) for k in keep[3:]], len(R), T._p(w["rate"]),
+                                     T._p(w["v0"]), T._p(w["lif"]), 1, 1, threads)
+    if not h:
+        raise MemoryError("oracle could not allocate the network")
+    return L, h, T
+
+
+def oracle_rate(L, h, steps):
+    """events/s of the oracle over `steps` steps (wall clock)."""
+    import ctypes as C
+    e0 = L.mgbo_events(h)
+    nid = C.c_int64()
+    t0 = time.perf_counter()
+    L.mgbo_run(h, steps, None, None, 0, C.byref(nid))
+    dt = time.perf_counter() - t0
+    return (L.mgbo_events(h) - e0) / dt, dt
+
+
+def cpu_baseline(w, sample_steps):
+    L, h, T = oracle_sim(w, os.cpu_count() or 1)
+    try:
+        L.mgbo_set_threads(h, 1)
+        v, dt = oracle_rate(L, h, sample_steps)
+    finally:
+        L.mgbo_destroy(h)
+    return {"value": v, "unit": "events/s", "cores": 1, "kind": "port",
+            "sample": f"oracle (C restatement of the reference kernels), 1 thread, first "
+                      f"{sample_steps} timesteps of the same network ({dt:.1f} s)"}
+
+
+def run_reference(a, ws, rank):
+    if rank != 0:
+        return
+    w = workload()
+    cores = os.cpu_count() or 1
+    L, h, T = oracle_sim(w, cores)
+    sample = a.ref_sample
+    try:
+        for _ in range(a.warmup):
+            oracle_rate(L, h, sample)
+        vals, times = [], []
+        for _ in range(a.steps):
+            v, dt = oracle_rate(L, h, sample)
+            vals.append(v)
+            times.append(dt)
+    finally:
+        L.mgbo_destroy(h)
+    value = float(np.sum([v * t for v, t in zip(vals, times)]) / np.sum(times))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "events/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1000 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "large Brunel (1M LIFB + 100k POISSON @20 Hz, fixed in-degree "
+                               "800/200/100, delays 10-50 steps, dt 0.1 ms)",
+                   "bench_step": f"{sample} timesteps", "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "events/s", "cores": cores, "kind": "port",
+                         "sample": f"oracle (C restatement of the reference kernels; the reference "
+                                   f"has no CPU simulator), {cores} OpenMP threads, {sample} "
+                                   f"timesteps per step"},
+        "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "sim_s_per_wall_s": sample * DT / float(np.mean(times)),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+def make_sim(w, device, seed, record=True):
+    import mgbrain_b200 as mgb
+    return mgb.Simulator.fixed_indegree(
+        w["pops"], w["projs"], w["lif"], rate=w["rate"], v_init=w["v0"], conn_seed=1,
+        seed=seed, device=device, raster_steps=CHUNK * 2, raster_ids=-1 if not record else 0)
+
+
+def timed_device(sim, steps_per, k, ws):
+    """Device time of k bench steps: CUDA events on the core's stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ev0 = sim.info()["events"]
+    l0 = sim.kernel_launches
+    e0.record(stream)
+    for _ in range(k):
+        sim.run(steps_per)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    return ms, sim.info()["events"] - ev0, sim.kernel_launches - l0
+
+
+def run_ours(a, ws, rank, local):
+    import torch
+
+    import mgbrain_b200 as mgb
+    torch.cuda.set_device(local)
+    hbm, peak_kind = peaks()
+    w = workload(a.scale)
+    t0 = time.perf_counter()
+    sim = make_sim(w, local, seed=1 + rank, record=False)
+    build_s = time.perf_counter() - t0
+    info = sim.info()
+    for _ in range(a.warmup):
+        sim.run(CHUNK)
+    sim.sync()
+    with ClockSampler(local) as clk:
+        ms, events, launches = timed_device(sim, CHUNK, a.steps, ws)
+    ms_max = allmax(ws, ms)
+    ev_all = allsum(ws, events)
+    value = ev_all / (ms_max / 1e3)
+    sim_s_wall = a.steps * CHUNK * DT / (ms_max / 1e3)
+    spikes_per_step = None
+
+    # per-kernel timing with CUDA events (no graphs) for the roofline
+    prof_steps = 2000
+    ev_p0 = sim.info()["events"]
+    kms = sim.profile(prof_steps)
+    ev_p = sim.info()["events"] - ev_p0
+    n_lif = w["n_lif"]
+    neuron_bytes = 24.0 * n_lif            # per launch (spike-id bytes are negligible here)
+    push_bytes = 8.0 * ev_p / prof_steps
+    kern = {
+        "neuron_update": {"avg_us": 1e3 * kms[0] / prof_steps, "bytes": neuron_bytes},
+        "event_push": {"avg_us": 1e3 * kms[1] / prof_steps, "bytes": push_bytes},
+    }
+    for k_, v in kern.items():
+        v["achieved_gbs"] = v["bytes"] / (v["avg_us"] * 1e-6) / 1e9 if v["avg_us"] > 0 else 0.0
+        v["frac"] = v["achieved_gbs"] / hbm
+        v["share"] = kms[0 if k_ == "neuron_update" else 1] / max(1e-9, sum(kms))
+    dom = max(kern, key=lambda k_: kern[k_]["avg_us"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["achieved_gbs"],
+                "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": kern[dom]["frac"],
+                "traffic": traffic}
+
+    # end to end through the C ABI: rates H2D from pinned memory, run, raster D2H
+    sim.close()
+    sim = make_sim(w, local, seed=1 + rank, record=True)
+    pinned = torch.empty(w["n"], dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = w["rate"]
+    import ctypes as C
+    L = mgb.lib()
+    for _ in range(1):
+        sim.run(CHUNK)
+        sim.read_raster(max_steps=CHUNK, max_ids=w["n"] * 8)
+    torch.cuda.synchronize()
+    barrier(ws)
+    h2d = d2h = 0
+    ev0 = sim.info()["events"]
+    t0 = time.perf_counter()
+    for _ in range(a.e2e_steps):
+        mgb.capi.check(L.mgc_set_rates(sim._h, C.c_void_p(pinned.data_ptr()), w["n"]))
+        h2d += 4 * w["n"]
+        sim.run(CHUNK)
+        _, counts, ids = sim.read_raster(max_steps=CHUNK, max_ids=w["n"] * 8)
+        d2h += 4 * len(counts) + 4 * len(ids)
+    sim.sync()
+    e2e_s = allmax(ws, time.perf_counter() - t0)
+    e2e_ev = allsum(ws, sim.info()["events"] - ev0)
+    e2e = {"value": e2e_ev / e2e_s, "unit": "events/s",
+           "h2d_bytes_per_step": int(h2d / a.e2e_steps), "d2h_bytes_per_step": int(d2h / a.e2e_steps),
+           "sim_s_per_wall_s": a.e2e_steps * CHUNK * DT / e2e_s}
+    sim.close()
+
+    # driven variant (inputs at 200 Hz): the same network with activity
+    driven = None
+    if not a.no_driven:
+        wd = workload(a.scale, nu=NU_DRIVEN)
+        simd = make_sim(wd, local, seed=1 + rank, record=False)
+        simd.run(CHUNK // 2)
+        simd.sync()
+        dms, dev, _ = timed_device(simd, CHUNK, 1, ws)
+        dms = allmax(ws, dms)
+        dev = allsum(ws, dev)
+        kd0 = simd.info()["events"]
+        kmd = simd.profile(500)
+        evd = simd.info()["events"] - kd0
+        push_us = 1e3 * kmd[1] / 500
+        driven = {"inputs_hz": 200, "events_per_s": dev / (dms / 1e3),
+                  "sim_s_per_wall_s": CHUNK * DT / (dms / 1e3),
+                  "event_push": {"avg_us": push_us, "bytes": 8.0 * evd / 500,
+                                 "achieved_gbs": 8.0 * evd / 500 / (push_us * 1e-6) / 1e9,
+                                 "frac": 8.0 * evd / 500 / (push_us * 1e-6) / 1e9 / hbm},
+                  "neuron_update_avg_us": 1e3 * kmd[0] / 500}
+        simd.close()
+
+    cpu = None
+    if rank == 0 and not a.no_cpu:
+        try:
+            cpu = cpu_baseline(w, a.cpu_sample)
+        except Exception as e:  # the host may lack the memory for the full network
+            cpu = {"value": None, "unit": "events/s", "cores": 1, "kind": "port",
+                   "sample": f"not run: {e}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded, generated on the device)",
+            "config": {"workload": "large Brunel: 1M LIFB (800k/200k) + 100k POISSON @20 Hz, fixed "
+                                   "in-degree 800/200/100, J 0.1 mV, g 5, delays U{10..50} steps, "
+                                   "dt 0.1 ms",
+                       "scale": a.scale, "synapses": info["n_synapses"], "bench_step": "1 s simulated "
+                       "(10,000 timesteps)", "l2": "inputs larger than L2 (8.8 GB CSR)",
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "sim_s_per_wall_s": sim_s_wall,
+            "events_per_step": ev_all / (a.steps * CHUNK * ws),
+            "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
+            "clocks": clk.summary(), "gpu_launches": int(launches),
+            "build_s": build_s, "driven_variant": driven,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", type=int, default=300)
+    ap.add_argument("--ref-sample", type=int, default=200)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-driven", action="store_true")
+    a = ap.parse_args()
+    ws, rank, local = dist_init()
+    try:
+        if a.impl == "reference":
+            run_reference(a, ws, rank)
+        else:
+            run_ours(a, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

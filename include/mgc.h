@@ -1,0 +1,186 @@
+/*
+ * mgc.h — C ABI of the mgbrain_b200 single-GPU simulation core.
+ *
+ * Plain pointers and sizes only; every call returns an mgc_status (0 = ok)
+ * and never exits the process.  One handle owns its device memory and its
+ * CUDA stream; handles share no global state, so several can live on one
+ * device.  Calls on one handle must not race each other.
+ *
+ * Each entry point names the reference interface it replaces
+ * (RAICLab-SNNGroup/MGBrain, file:line).
+ */
+#ifndef MGC_H
+#define MGC_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum mgc_status {
+    MGC_OK = 0,
+    MGC_ERR_INVALID = 1,   /* bad argument or network description */
+    MGC_ERR_CUDA = 2,      /* CUDA runtime error (mgc_last_error has the text) */
+    MGC_ERR_NOMEM = 3,     /* device or host allocation failed */
+    MGC_ERR_OVERFLOW = 4,  /* raster buffer overflowed; returned data is truncated */
+    MGC_ERR_NODEVICE = 5   /* no CUDA device / extension built for another GPU */
+} mgc_status;
+
+/* NeuronType values, src/macro.h:40-48. */
+enum { MGC_RAW = 0, MGC_LIF0 = 1, MGC_POISSON = 2, MGC_LIF = 3, MGC_LIFE = 4, MGC_LIFB = 5 };
+
+/* Propagation method. */
+enum {
+    MGC_MODE_AUTO = 0,   /* core picks */
+    MGC_MODE_PUSH = 1    /* event push from spiking rows into the delay ring */
+};
+
+typedef struct mgc_sim mgc_sim;
+
+/* Network handed over as the reference's Network holds it
+ * (src/model/network.h:50-68) after build_multinet's delay quantisation
+ * (src/simulator/mgsim/adj/mgsim.cpp:49): neurons in id order, synapses in
+ * list order.  All arrays are host memory and are copied; the caller may
+ * free them after mgc_create returns. */
+typedef struct mgc_net_desc {
+    int32_t n_neurons;
+    const int8_t* type;        /* [n] NeuronType */
+    const float* rate;         /* [n] POISSON per-step probability, or NULL (0) */
+    const float* v_init;       /* [n] initial V, or NULL (lifconst[1] for all) */
+    int64_t n_synapses;
+    const int32_t* syn_src;    /* [S] */
+    const int32_t* syn_tar;    /* [S] */
+    const float* syn_weight;   /* [S] */
+    const int32_t* syn_delay;  /* [S] delay in steps, >= 1 */
+    const uint8_t* syn_plastic;/* [S] or NULL: every synapse plastic when stdp */
+    float lifconst[30];        /* LIFECONSTS, mgcore.cu:32-63 */
+    float stdpconst[6];        /* STDPCONSTS, mgcore.cu:73-80 */
+    int32_t stdp;              /* Config::STDP */
+    int32_t mode;              /* MGC_MODE_* */
+    uint64_t seed;             /* key of the POISSON draws */
+    int32_t device;            /* CUDA device ordinal */
+    int64_t raster_steps;      /* steps the raster holds between reads (0: default) */
+    int64_t raster_ids;        /* spike ids it holds between reads (0: default, <0: off) */
+} mgc_net_desc;
+
+/* Procedural fixed in-degree network built on the device.  Population p
+ * occupies neuron ids [pop_start[p], pop_start[p]+pop_num[p]).  Projection
+ * r gives every neuron of pop pr_tar[r] exactly pr_k[r] synapses whose
+ * sources are drawn uniformly, with replacement, from pop pr_src[r], with
+ * weight pr_w[r] and delay uniform in [pr_dmin[r], pr_dmax[r]] steps,
+ * from Philox4x32-10 keyed by conn_seed. */
+typedef struct mgc_fixed_indegree_desc {
+    int32_t n_pops;
+    const int32_t* pop_start;
+    const int32_t* pop_num;
+    const int32_t* pop_type;
+    int32_t n_proj;
+    const int32_t* pr_src;
+    const int32_t* pr_tar;
+    const int32_t* pr_k;
+    const float* pr_w;
+    const int32_t* pr_dmin;
+    const int32_t* pr_dmax;
+    const float* rate;         /* [n] or NULL */
+    const float* v_init;       /* [n] or NULL */
+    float lifconst[30];
+    uint64_t conn_seed;
+    uint64_t seed;
+    int32_t mode;
+    int32_t device;
+    int64_t raster_steps;
+    int64_t raster_ids;
+} mgc_fixed_indegree_desc;
+
+typedef struct mgc_info {
+    int32_t n_neurons;
+    int32_t ring_len;          /* M = max_delay + 1 (mgsim.cpp:71) */
+    int32_t min_delay;         /* mgsim.cpp:51 */
+    int32_t max_delay;
+    int64_t n_synapses;
+    int64_t step;              /* steps simulated so far */
+    int64_t events;            /* synaptic events delivered so far */
+    int32_t mode;
+    int32_t graph_steps;       /* steps per captured CUDA graph */
+    int64_t device_bytes;      /* device memory held by the handle */
+} mgc_info;
+
+/* Replaces MGSimulator::MGSimulator(Network&, std::vector<int>&, int)
+ * (src/simulator/mgsim/adj/mgsim.cpp:337-363) for npart=1: build_multinet
+ * (mgsim.cpp:8-144), copy_subnet_gpu (mgnet.cpp:92-146), init_state
+ * (mgcore.cu:665-669) and copy_consts_gpu (mgcore.cu:685-748). */
+mgc_status mgc_create(const mgc_net_desc* desc, mgc_sim** out);
+
+/* Device-side network generation for networks too large to list on the
+ * host; no reference counterpart (netgen.cpp:39-229 is host-only and
+ * cannot express a fixed in-degree). */
+mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* desc, mgc_sim** out);
+
+/* Enqueues `steps` steps on the handle's stream and returns without
+ * waiting.  Replaces the step loop of MGSimulator::simulate_sparse
+ * (mgsim.cpp:794-857) calling mgsim_step_sparse (mgcore.cu:535-554);
+ * the caller applies the reference's step-count rule (see
+ * mgc_effective_steps).  Steps continue from the previous call. */
+mgc_status mgc_run(mgc_sim* sim, int64_t steps);
+
+/* Waits for the handle's stream and reports device-side errors. */
+mgc_status mgc_sync(mgc_sim* sim);
+
+/* Copies n POISSON per-step probabilities from host memory (pinned memory
+ * makes the copy asynchronous); takes effect from the next enqueued step.
+ * Replaces writing Neuron::rate before construction (e.g.
+ * bench/single_brunel.cpp:46-50). */
+mgc_status mgc_set_rates(mgc_sim* sim, const float* rate, int32_t n);
+
+/* Copies out the raster recorded since the previous read and clears it:
+ * counts[i] = spikes of step first_step+i, ids = their neuron ids, ascending
+ * inside each step.  The reference records no raster; its only output is
+ * fire_cnt (mgsim.cpp:596-615). */
+mgc_status mgc_read_raster(mgc_sim* sim, int64_t* first_step, int64_t* counts, int64_t counts_cap,
+                           int32_t* ids, int64_t ids_cap, int64_t* n_steps, int64_t* n_ids);
+
+/* Copies neuron state to host arrays of n entries; any pointer may be NULL.
+ * Replaces get_subnet_firecnt (mgnet.cpp:148-158) / copy_subnet_cpu
+ * (mgnet.cpp:283-300). */
+mgc_status mgc_read_state(mgc_sim* sim, float* v, float* i_exc, float* i_inh, int32_t* refrac,
+                          int32_t* last_fired, int32_t* fire_cnt);
+
+/* Copies the S synaptic weights in synapse-list order (mgc_create networks). */
+mgc_status mgc_read_weights(mgc_sim* sim, float* weight);
+
+/* Copies the CSR the core built: row_ptr[n+1], tgt[S], weight[S], delay[S]
+ * (any may be NULL). */
+mgc_status mgc_export_csr(mgc_sim* sim, int64_t* row_ptr, int32_t* tgt, float* weight, int32_t* delay);
+
+mgc_status mgc_get_info(mgc_sim* sim, mgc_info* info);
+
+/* Runs `steps` steps without graphs, timing each kernel class with CUDA
+ * events on the handle's stream: ms[0] neuron update, ms[1] event push,
+ * ms[2] STDP, summed over the steps.  No reference counterpart (the
+ * reference was profiled externally with nvprof, shell/single.sh:15). */
+mgc_status mgc_profile_steps(mgc_sim* sim, int64_t steps, float* ms);
+
+/* The handle's cudaStream_t, for event timing by the caller. */
+mgc_status mgc_get_stream(mgc_sim* sim, void** stream);
+
+/* Number of steps MGSimulator::simulate runs for `steps` requested steps
+ * and the network's minimum delay: cycles = steps/min_delay +
+ * (steps%min_delay == 0), each cycle bounded by steps (mgsim.cpp:801-838).
+ * Returns -1 when min_delay < 1. */
+int64_t mgc_effective_steps(int64_t steps, int32_t min_delay);
+
+/* Frees the handle.  Replaces MGSimulator::~MGSimulator (mgsim.cpp:364-406)
+ * without its cudaDeviceReset. */
+void mgc_destroy(mgc_sim* sim);
+
+/* Text of the last error on the calling thread. */
+const char* mgc_last_error(void);
+
+/* Kernels this library launched on this handle so far. */
+int64_t mgc_kernel_launches(mgc_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

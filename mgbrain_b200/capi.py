@@ -1,0 +1,270 @@
+"""ctypes binding of the C ABI in include/mgc.h.
+
+The library is the in-tree build mgbrain_b200/lib/libmgbrain_b200.so.  There
+is no fallback: if it is missing or cannot run on this machine, every entry
+point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libmgbrain_b200.so")
+
+MGC_OK, MGC_ERR_INVALID, MGC_ERR_CUDA, MGC_ERR_NOMEM, MGC_ERR_OVERFLOW, MGC_ERR_NODEVICE = range(6)
+RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)
+MODE_AUTO, MODE_PUSH = 0, 1
+
+EXPORTED = (
+    "mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
+    "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
+    "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
+    "mgc_kernel_launches", "mgc_profile_steps",
+)
+
+
+class MgcError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"mgc status {status}: {msg}")
+        self.status = status
+
+
+class NetDesc(C.Structure):
+    _fields_ = [
+        ("n_neurons", C.c_int32), ("type", C.c_void_p), ("rate", C.c_void_p),
+        ("v_init", C.c_void_p), ("n_synapses", C.c_int64), ("syn_src", C.c_void_p),
+        ("syn_tar", C.c_void_p), ("syn_weight", C.c_void_p), ("syn_delay", C.c_void_p),
+        ("syn_plastic", C.c_void_p), ("lifconst", C.c_float * 30), ("stdpconst", C.c_float * 6),
+        ("stdp", C.c_int32), ("mode", C.c_int32), ("seed", C.c_uint64), ("device", C.c_int32),
+        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64),
+    ]
+
+
+class FixedInDegreeDesc(C.Structure):
+    _fields_ = [
+        ("n_pops", C.c_int32), ("pop_start", C.c_void_p), ("pop_num", C.c_void_p),
+        ("pop_type", C.c_void_p), ("n_proj", C.c_int32), ("pr_src", C.c_void_p),
+        ("pr_tar", C.c_void_p), ("pr_k", C.c_void_p), ("pr_w", C.c_void_p),
+        ("pr_dmin", C.c_void_p), ("pr_dmax", C.c_void_p), ("rate", C.c_void_p),
+        ("v_init", C.c_void_p), ("lifconst", C.c_float * 30), ("conn_seed", C.c_uint64),
+        ("seed", C.c_uint64), ("mode", C.c_int32), ("device", C.c_int32),
+        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("n_neurons", C.c_int32), ("ring_len", C.c_int32), ("min_delay", C.c_int32),
+        ("max_delay", C.c_int32), ("n_synapses", C.c_int64), ("step", C.c_int64),
+        ("events", C.c_int64), ("mode", C.c_int32), ("graph_steps", C.c_int32),
+        ("device_bytes", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library; raises when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build the CUDA extension first "
+            "(python -c 'import __graft_entry__ as g; g.build()')")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
+    L.mgc_create.argtypes = [C.POINTER(NetDesc), C.POINTER(vp)]
+    L.mgc_create_fixed_indegree.argtypes = [C.POINTER(FixedInDegreeDesc), C.POINTER(vp)]
+    L.mgc_run.argtypes = [vp, i64]
+    L.mgc_sync.argtypes = [vp]
+    L.mgc_set_rates.argtypes = [vp, vp, i32]
+    L.mgc_read_raster.argtypes = [vp, vp, vp, i64, vp, i64, vp, vp]
+    L.mgc_read_state.argtypes = [vp] * 7
+    L.mgc_read_weights.argtypes = [vp, vp]
+    L.mgc_export_csr.argtypes = [vp] * 5
+    L.mgc_get_info.argtypes = [vp, C.POINTER(Info)]
+    L.mgc_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.mgc_profile_steps.argtypes = [vp, i64, vp]
+    L.mgc_effective_steps.argtypes = [i64, i32]
+    L.mgc_effective_steps.restype = i64
+    L.mgc_destroy.argtypes = [vp]
+    L.mgc_destroy.restype = None
+    L.mgc_last_error.restype = C.c_char_p
+    L.mgc_kernel_launches.argtypes = [vp]
+    L.mgc_kernel_launches.restype = i64
+    for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
+                 "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
+                 "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
+        getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != MGC_OK:
+        raise MgcError(status, lib().mgc_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def effective_steps(steps, min_delay):
+    return int(lib().mgc_effective_steps(int(steps), int(min_delay)))
+
+
+class Simulator:
+    """One simulation handle of the CUDA core (an MGSimulator for npart=1)."""
+
+    def __init__(self, handle, n, S, keep=()):
+        self._h = C.c_void_p(handle)
+        self.n = n
+        self.S = S
+        self._keep = keep
+
+    # ---- construction ---------------------------------------------------
+    @classmethod
+    def from_arrays(cls, n, type_, src, tar, weight, delay_steps, lifconst, stdpconst=None,
+                    rate=None, v_init=None, stdp=False, plastic=None, seed=1, device=0,
+                    mode=MODE_AUTO, raster_steps=0, raster_ids=0):
+        L = lib()
+        arrs = dict(
+            type=np.ascontiguousarray(type_, np.int8),
+            rate=None if rate is None else np.ascontiguousarray(rate, np.float32),
+            v_init=None if v_init is None else np.ascontiguousarray(v_init, np.float32),
+            src=np.ascontiguousarray(src, np.int32), tar=np.ascontiguousarray(tar, np.int32),
+            weight=np.ascontiguousarray(weight, np.float32),
+            delay=np.ascontiguousarray(delay_steps, np.int32),
+            plastic=None if plastic is None else np.ascontiguousarray(plastic, np.uint8),
+        )
+        d = NetDesc()
+        d.n_neurons = int(n)
+        d.type, d.rate, d.v_init = _ptr(arrs["type"]), _ptr(arrs["rate"]), _ptr(arrs["v_init"])
+        d.n_synapses = len(arrs["src"])
+        d.syn_src, d.syn_tar = _ptr(arrs["src"]), _ptr(arrs["tar"])
+        d.syn_weight, d.syn_delay = _ptr(arrs["weight"]), _ptr(arrs["delay"])
+        d.syn_plastic = _ptr(arrs["plastic"])
+        d.lifconst[:] = [float(x) for x in np.asarray(lifconst, np.float32)]
+        sc = np.asarray(stdpconst if stdpconst is not None else [0.1, -0.01, 17, 34, 40, 0], np.float32)
+        d.stdpconst[:] = [float(x) for x in sc]
+        d.stdp, d.mode, d.seed, d.device = int(bool(stdp)), int(mode), int(seed), int(device)
+        d.raster_steps, d.raster_ids = int(raster_steps), int(raster_ids)
+        h = C.c_void_p()
+        check(L.mgc_create(C.byref(d), C.byref(h)))
+        return cls(h.value, int(n), d.n_synapses)
+
+    @classmethod
+    def fixed_indegree(cls, pops, projs, lifconst, rate=None, v_init=None, conn_seed=1, seed=1,
+                       device=0, mode=MODE_AUTO, raster_steps=0, raster_ids=0):
+        """pops: list of (start, num, type); projs: (src_pop, tar_pop, k, w, dmin, dmax)."""
+        L = lib()
+        P = np.asarray(pops, np.int64).reshape(-1, 3)
+        R = list(projs)
+        a = dict(
+            ps=np.ascontiguousarray(P[:, 0], np.int32), pn=np.ascontiguousarray(P[:, 1], np.int32),
+            pt=np.ascontiguousarray(P[:, 2], np.int32),
+            rs=np.array([r[0] for r in R], np.int32), rt=np.array([r[1] for r in R], np.int32),
+            rk=np.array([r[2] for r in R], np.int32), rw=np.array([r[3] for r in R], np.float32),
+            rd0=np.array([r[4] for r in R], np.int32), rd1=np.array([r[5] for r in R], np.int32),
+            rate=None if rate is None else np.ascontiguousarray(rate, np.float32),
+            v0=None if v_init is None else np.ascontiguousarray(v_init, np.float32),
+        )
+        d = FixedInDegreeDesc()
+        d.n_pops = len(P)
+        d.pop_start, d.pop_num, d.pop_type = _ptr(a["ps"]), _ptr(a["pn"]), _ptr(a["pt"])
+        d.n_proj = len(R)
+        d.pr_src, d.pr_tar, d.pr_k, d.pr_w = _ptr(a["rs"]), _ptr(a["rt"]), _ptr(a["rk"]), _ptr(a["rw"])
+        d.pr_dmin, d.pr_dmax = _ptr(a["rd0"]), _ptr(a["rd1"])
+        d.rate, d.v_init = _ptr(a["rate"]), _ptr(a["v0"])
+        d.lifconst[:] = [float(x) for x in np.asarray(lifconst, np.float32)]
+        d.conn_seed, d.seed, d.mode, d.device = int(conn_seed), int(seed), int(mode), int(device)
+        d.raster_steps, d.raster_ids = int(raster_steps), int(raster_ids)
+        h = C.c_void_p()
+        check(L.mgc_create_fixed_indegree(C.byref(d), C.byref(h)))
+        n = int((P[:, 0] + P[:, 1]).max())
+        S = int(sum(int(P[r[1], 1]) * int(r[2]) for r in R))
+        return cls(h.value, n, S)
+
+    # ---- stepping -------------------------------------------------------
+    def run(self, steps):
+        check(lib().mgc_run(self._h, int(steps)))
+
+    def sync(self):
+        check(lib().mgc_sync(self._h))
+
+    def set_rates(self, rate):
+        r = np.ascontiguousarray(rate, np.float32)
+        check(lib().mgc_set_rates(self._h, _ptr(r), self.n))
+        self.sync()  # the host array may be pageable and temporary
+
+    @property
+    def stream(self):
+        s = C.c_void_p()
+        check(lib().mgc_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
+    # ---- readout --------------------------------------------------------
+    def read_raster(self, max_steps=1 << 20, max_ids=None):
+        info = self.info()
+        if max_ids is None:
+            max_ids = max(1, self.n) * 64
+        counts = np.zeros(max_steps, np.int64)
+        ids = np.zeros(max_ids, np.int32)
+        first, ns, ni = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mgc_read_raster(self._h, C.byref(first), _ptr(counts), max_steps, _ptr(ids),
+                                    max_ids, C.byref(ns), C.byref(ni)))
+        del info
+        return first.value, counts[:ns.value].copy(), ids[:ni.value].copy()
+
+    def state(self):
+        n = self.n
+        out = {k: np.zeros(n, np.float32) for k in ("V", "Iexc", "Iinh")}
+        for k in ("refrac", "last_fired", "fire_cnt"):
+            out[k] = np.zeros(n, np.int32)
+        check(lib().mgc_read_state(self._h, _ptr(out["V"]), _ptr(out["Iexc"]), _ptr(out["Iinh"]),
+                                   _ptr(out["refrac"]), _ptr(out["last_fired"]), _ptr(out["fire_cnt"])))
+        return out
+
+    def weights(self):
+        w = np.zeros(self.S, np.float32)
+        check(lib().mgc_read_weights(self._h, _ptr(w)))
+        return w
+
+    def export_csr(self):
+        rp = np.zeros(self.n + 1, np.int64)
+        t = np.zeros(self.S, np.int32)
+        w = np.zeros(self.S, np.float32)
+        d = np.zeros(self.S, np.int32)
+        check(lib().mgc_export_csr(self._h, _ptr(rp), _ptr(t), _ptr(w), _ptr(d)))
+        return rp, t, w, d
+
+    def profile(self, steps):
+        """Milliseconds spent in (neuron update, event push, STDP) over `steps`
+        steps run without graphs, measured with CUDA events."""
+        ms = np.zeros(3, np.float32)
+        check(lib().mgc_profile_steps(self._h, int(steps), _ptr(ms)))
+        return [float(x) for x in ms]
+
+    def info(self):
+        i = Info()
+        check(lib().mgc_get_info(self._h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in Info._fields_}
+
+    @property
+    def kernel_launches(self):
+        return int(lib().mgc_kernel_launches(self._h))
+
+    def close(self):
+        if self._h:
+            lib().mgc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

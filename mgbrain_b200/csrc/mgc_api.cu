@@ -1,0 +1,823 @@
+// C ABI of the simulation core (include/mgc.h): network upload and CSR
+// construction on the device, the step driver (CUDA graphs of whole step
+// groups), raster and state readout.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/mgc.h"
+#include "kernels.cuh"
+
+using namespace mgc;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+mgc_status fail(mgc_status st, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+#define CK(expr)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            if (e_ == cudaErrorMemoryAllocation) {                                            \
+                cudaGetLastError();                                                           \
+                return fail(MGC_ERR_NOMEM, "%s: %s", #expr, cudaGetErrorString(e_));          \
+            }                                                                                 \
+            return fail(MGC_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                            \
+        }                                                                                     \
+    } while (0)
+
+#define CKS(expr)                        \
+    do {                                 \
+        mgc_status s_ = (expr);          \
+        if (s_ != MGC_OK) return s_;     \
+    } while (0)
+
+constexpr int64_t kDefaultRasterSteps = 1 << 16;
+constexpr int kGraphSteps = 64;
+
+int bits_for(int64_t n)
+{
+    int b = 1;
+    while ((int64_t(1) << b) < n) ++b;
+    return b;
+}
+
+}  // namespace
+
+struct mgc_sim {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    StepArgs a{};
+    int32_t n = 0, M = 0, dmin = 0, dmax = 0;
+    int64_t S = 0;
+    int mode = MGC_MODE_PUSH;
+    bool stdp = false;
+    int neuron_grid = 1, push_grid = 1, stdp_grid = 1;
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+    int64_t* csr_syn64 = nullptr;     // synapse-list index of each CSR position (explicit nets)
+    int64_t host_step = 0;            // steps enqueued
+    int64_t launches = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    int64_t raster_steps_cap = 0, raster_ids_cap = 0;
+
+    ~mgc_sim()
+    {
+        if (device >= 0) cudaSetDevice(device);
+        if (graph) cudaGraphExecDestroy(graph);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocs) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    mgc_status alloc(T** p, size_t count, bool zero = true)
+    {
+        void* v = nullptr;
+        size_t b = std::max<size_t>(count, 1) * sizeof(T);
+        CK(cudaMalloc(&v, b));
+        allocs.push_back(v);
+        bytes += b;
+        if (zero) CK(cudaMemsetAsync(v, 0, b, stream));
+        *p = static_cast<T*>(v);
+        return MGC_OK;
+    }
+
+    template <class T>
+    mgc_status upload(T** p, const T* host, size_t count)
+    {
+        CKS(alloc(p, count, host == nullptr));
+        if (host && count) CK(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+        return MGC_OK;
+    }
+
+    void release(void* p)
+    {
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) {
+            allocs.erase(it);
+            cudaFree(p);
+        }
+    }
+};
+
+namespace {
+
+// Temporary device buffer freed on scope exit.
+struct DevTmp {
+    void* p = nullptr;
+    ~DevTmp()
+    {
+        if (p) cudaFree(p);
+    }
+};
+
+template <class T>
+mgc_status tmp_alloc(DevTmp& t, T** p, size_t count)
+{
+    CK(cudaMalloc(&t.p, std::max<size_t>(count, 1) * sizeof(T)));
+    *p = static_cast<T*>(t.p);
+    return MGC_OK;
+}
+
+__global__ void k_iota32(uint32_t* v, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = (uint32_t)i;
+}
+
+__global__ void k_count_rows(const int32_t* key, int64_t S, int64_t* deg)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < S; k += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(reinterpret_cast<unsigned long long*>(deg + key[k]), 1ull);
+}
+
+__global__ void k_validate(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int32_t n,
+                           int32_t dlim, int32_t* bad)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < S; k += (int64_t)gridDim.x * blockDim.x) {
+        if (src[k] < 0 || src[k] >= n || tar[k] < 0 || tar[k] >= n || delay[k] < 1 || delay[k] >= dlim)
+            atomicOr(bad, 1);
+    }
+}
+
+// CSR words from an explicit synapse list gathered in sorted order.
+__global__ void k_gather_explicit(const uint32_t* order, const int32_t* keys, const int32_t* tar, const float* w,
+                                  const int32_t* delay, const uint8_t* plastic_in, int64_t S, int tbits,
+                                  uint2* syn, int64_t* csr_syn, int32_t* csr_src, uint8_t* plastic_out)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = order[p];
+        syn[p] = make_uint2((uint32_t)tar[k] | ((uint32_t)delay[k] << tbits), __float_as_uint(w[k]));
+        csr_syn[p] = k;
+        if (csr_src) csr_src[p] = keys[p];
+        if (plastic_out) plastic_out[p] = plastic_in ? (plastic_in[k] != 0) : 1;
+    }
+}
+
+__global__ void k_inverse(const int64_t* csr_syn, int64_t S, uint32_t* pos_of)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x)
+        pos_of[csr_syn[p]] = (uint32_t)p;
+}
+
+__global__ void k_widen(const uint32_t* in, int64_t S, int64_t* out)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x)
+        out[p] = in[p];
+}
+
+// Fixed in-degree generator (see mgc_fixed_indegree_desc): synapse index
+// i -> projection r (by prefix), target t, draw k.
+struct ProjTable {
+    int32_t n;
+    int64_t base[17];
+    int32_t src_start[16], src_num[16], tar_start[16], k[16], dmin[16], dspan[16];
+    float w[16];
+};
+
+__device__ __forceinline__ void fid_decode(const ProjTable& pt, uint64_t seed, int64_t i, int32_t& src, int32_t& tar,
+                                           int32_t& delay, float& w)
+{
+    int r = 0;
+    while (r + 1 < pt.n && i >= pt.base[r + 1]) ++r;
+    const int64_t loc = i - pt.base[r];
+    const int32_t tl = (int32_t)(loc / pt.k[r]);
+    const int32_t k = (int32_t)(loc - (int64_t)tl * pt.k[r]);
+    tar = pt.tar_start[r] + tl;
+    const U32x4 x = conn_draw(seed, (uint32_t)tar, (uint32_t)k, (uint32_t)r);
+    src = pt.src_start[r] + (int32_t)scale_u32(x.x, (uint32_t)pt.src_num[r]);
+    delay = pt.dmin[r] + (int32_t)scale_u32(x.y, (uint32_t)pt.dspan[r]);
+    w = pt.w[r];
+}
+
+__global__ void k_fid_keys(ProjTable pt, uint64_t seed, int64_t S, int32_t* keys, uint32_t* vals, int64_t* deg)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < S; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t src, tar, d;
+        float w;
+        fid_decode(pt, seed, i, src, tar, d, w);
+        keys[i] = src;
+        vals[i] = (uint32_t)i;
+        atomicAdd(reinterpret_cast<unsigned long long*>(deg + src), 1ull);
+    }
+}
+
+__global__ void k_fid_gather(ProjTable pt, uint64_t seed, const uint32_t* order, int64_t S, int tbits, uint2* syn)
+{
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x) {
+        int32_t src, tar, d;
+        float w;
+        fid_decode(pt, seed, order[p], src, tar, d, w);
+        syn[p] = make_uint2((uint32_t)tar | ((uint32_t)d << tbits), __float_as_uint(w));
+    }
+}
+
+int grid_for(int64_t n, int block = 256)
+{
+    int64_t g = (n + block - 1) / block;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(g, 148 * 32));
+}
+
+// Stable radix sort of (key, value) pairs by key; keys < 2^key_bits.
+mgc_status sort_pairs(const int32_t* keys_in, int32_t* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
+                      int64_t S, int key_bits, cudaStream_t st)
+{
+    // CUB takes item counts as int per call: sort in one call when it fits.
+    if (S > (int64_t)0x7fffffff) return fail(MGC_ERR_INVALID, "more than 2^31-1 synapses in one sort");
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
+    DevTmp t;
+    void* tp = nullptr;
+    CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
+    tp = t.p;
+    CK(cub::DeviceRadixSort::SortPairs(tp, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
+    CK(cudaStreamSynchronize(st));
+    return MGC_OK;
+}
+
+mgc_status exclusive_scan(int64_t* deg_then_ptr, int32_t n, cudaStream_t st)
+{
+    // deg has n+1 entries; turns deg[0..n) into row offsets row_ptr[0..n].
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg_then_ptr, deg_then_ptr, n + 1, st));
+    DevTmp t;
+    CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
+    CK(cub::DeviceScan::ExclusiveSum(t.p, tb, deg_then_ptr, deg_then_ptr, n + 1, st));
+    return MGC_OK;
+}
+
+mgc_status max_row(const int64_t* row_ptr, int32_t n, int64_t* out)
+{
+    std::vector<int64_t> h(n + 1);
+    CK(cudaMemcpy(h.data(), row_ptr, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+    int64_t m = 0;
+    for (int32_t i = 0; i < n; ++i) m = std::max(m, h[i + 1] - h[i]);
+    *out = m;
+    return MGC_OK;
+}
+
+mgc_status pick_device(int device)
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(MGC_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= count) return fail(MGC_ERR_INVALID, "device %d out of range", device);
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return fail(MGC_ERR_NODEVICE, "device %d is sm_%d%d; this library holds sm_100a code only", device,
+                    prop.major, prop.minor);
+    return MGC_OK;
+}
+
+// Neuron arrays, constants, step bookkeeping and raster buffers.
+mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* rate, const float* v_init,
+                       const float* lifc, const float* stdpc, uint64_t seed, int64_t raster_steps,
+                       int64_t raster_ids)
+{
+    StepArgs& a = s->a;
+    a.n = n;
+    a.seed = seed;
+    memcpy(a.C, lifc, sizeof(a.C));
+    if (stdpc) memcpy(a.P, stdpc, sizeof(a.P));
+    if (!(lifc[0] > 0.0f)) return fail(MGC_ERR_INVALID, "lifconst[0] (DT) must be > 0");
+    a.refrac_steps = (int32_t)roundf(lifc[8] / lifc[0]) - 1;  // mgcore.cu:184
+    a.lifb_leak = lifc[9] != 0.0f ? lifc[9] : 0.005f;          // mgcore.cu:190
+    int8_t* d_type;
+    CKS(s->upload(&d_type, type, n));
+    a.type = d_type;
+    float* d_rate;
+    CKS(s->upload(&d_rate, rate, n));
+    a.rate = d_rate;
+    std::vector<float> v0(n);
+    for (int32_t i = 0; i < n; ++i) v0[i] = v_init ? v_init[i] : lifc[1];  // mgsim.cpp:97
+    CKS(s->upload(&a.V, v0.data(), n));
+    CKS(s->alloc(&a.Iexc, n));
+    CKS(s->alloc(&a.Iinh, n));
+    CKS(s->alloc(&a.refrac, n));
+    CKS(s->alloc(&a.last_fired, n));
+    CKS(s->alloc(&a.fire_cnt, n));
+    CKS(s->alloc(&a.spk, n));
+    CKS(s->alloc(&a.spk_count, 1));
+    CKS(s->alloc(&a.step, 1));
+    CKS(s->alloc(&a.done, 1));
+    CKS(s->alloc(&a.events, 1));
+    CKS(s->alloc(&a.status, 1));
+    CKS(s->alloc(&a.raster_pos, 1));
+    CKS(s->alloc(&a.raster_step0, 1));
+    s->raster_steps_cap = raster_steps > 0 ? raster_steps : kDefaultRasterSteps;
+    if (raster_ids < 0) {
+        a.record = 0;
+        s->raster_ids_cap = 0;
+    } else {
+        a.record = 1;
+        s->raster_ids_cap = raster_ids > 0 ? raster_ids : std::max<int64_t>(1 << 20, (int64_t)n * 64);
+    }
+    a.raster_steps_cap = a.record ? s->raster_steps_cap : 0;
+    a.raster_ids_cap = s->raster_ids_cap;
+    CKS(s->alloc(&a.raster_counts, a.record ? s->raster_steps_cap : 1, false));
+    CKS(s->alloc(&a.raster_ids, a.record ? s->raster_ids_cap : 1, false));
+    return MGC_OK;
+}
+
+mgc_status init_ring_and_launch(mgc_sim* s, int64_t max_row_len)
+{
+    StepArgs& a = s->a;
+    a.M = s->M;
+    CKS(s->alloc(&a.ring_e, (size_t)s->M * s->n));
+    CKS(s->alloc(&a.ring_i, (size_t)s->M * s->n));
+    a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_row_len + kChunk - 1) / kChunk);
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, s->device));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push, kPushBlock, 0));
+    s->push_grid = prop.multiProcessorCount * std::max(1, occ);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stdp, kPushBlock, 0));
+    s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
+    s->neuron_grid = (s->n + kNeuronBlock - 1) / kNeuronBlock;
+    CK(cudaStreamSynchronize(s->stream));
+    return MGC_OK;
+}
+
+mgc_status enqueue_step(mgc_sim* s)
+{
+    k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+    k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+    s->launches += 2;
+    if (s->stdp) {
+        k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+        s->launches += 1;
+    }
+    CK(cudaGetLastError());
+    return MGC_OK;
+}
+
+mgc_status build_graph(mgc_sim* s)
+{
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = s->launches;
+    for (int i = 0; i < kGraphSteps; ++i) {
+        mgc_status st = enqueue_step(s);
+        if (st != MGC_OK) {
+            cudaStreamEndCapture(s->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+    }
+    s->launches = before;  // captured, not launched
+    CK(cudaStreamEndCapture(s->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    s->graph_steps = kGraphSteps;
+    return MGC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
+{
+    if (!d || !out) return fail(MGC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->n_neurons <= 0 || !d->type) return fail(MGC_ERR_INVALID, "network needs neurons and types");
+    if (d->n_synapses < 0 || (d->n_synapses > 0 && (!d->syn_src || !d->syn_tar || !d->syn_weight || !d->syn_delay)))
+        return fail(MGC_ERR_INVALID, "synapse arrays missing");
+    if (d->mode != MGC_MODE_AUTO && d->mode != MGC_MODE_PUSH) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
+    CKS(pick_device(d->device));
+    std::unique_ptr<mgc_sim> s(new mgc_sim);
+    s->device = d->device;
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->n = d->n_neurons;
+    s->S = d->n_synapses;
+    s->stdp = d->stdp != 0;
+    s->mode = MGC_MODE_PUSH;
+    CKS(init_common(s.get(), s->n, d->type, d->rate, d->v_init, d->lifconst, d->stdpconst, d->seed,
+                    d->raster_steps, d->raster_ids));
+    StepArgs& a = s->a;
+    a.stdp = s->stdp;
+    const int64_t S = s->S;
+    // delay range (mgsim.cpp:42-51); M = max_delay + 1 (:71)
+    int32_t dmin = 0x7fffffff, dmax = 0;
+    for (int64_t k = 0; k < S; ++k) {
+        dmin = std::min(dmin, d->syn_delay[k]);
+        dmax = std::max(dmax, d->syn_delay[k]);
+    }
+    if (S == 0) dmin = dmax = 1;
+    if (dmin < 1) return fail(MGC_ERR_INVALID, "synaptic delay below one step (%d)", dmin);
+    s->dmin = dmin;
+    s->dmax = dmax;
+    s->M = dmax + 1;
+    a.tbits = bits_for(s->n);
+    a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
+    if (a.tbits + bits_for((int64_t)dmax + 1) > 32)
+        return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", dmax, s->n);
+
+    int64_t* row_ptr;
+    CKS(s->alloc(&row_ptr, (size_t)s->n + 1));
+    a.row_ptr = row_ptr;
+    uint2* syn;
+    CKS(s->alloc(&syn, S, false));
+    a.syn = syn;
+    CKS(s->alloc(&s->csr_syn64, S, false));
+    int64_t max_len = 0;
+    if (S > 0) {
+        DevTmp t_src, t_tar, t_w, t_d, t_pl, t_keys, t_vals, t_order, t_bad;
+        int32_t *src, *tar, *dl, *keys, *bad;
+        float* w;
+        uint8_t* pl = nullptr;
+        uint32_t *vals, *order;
+        CKS(tmp_alloc(t_src, &src, S));
+        CKS(tmp_alloc(t_tar, &tar, S));
+        CKS(tmp_alloc(t_w, &w, S));
+        CKS(tmp_alloc(t_d, &dl, S));
+        CKS(tmp_alloc(t_bad, &bad, 1));
+        CK(cudaMemcpyAsync(src, d->syn_src, 4 * S, cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(tar, d->syn_tar, 4 * S, cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(w, d->syn_weight, 4 * S, cudaMemcpyHostToDevice, s->stream));
+        CK(cudaMemcpyAsync(dl, d->syn_delay, 4 * S, cudaMemcpyHostToDevice, s->stream));
+        if (s->stdp && d->syn_plastic) {
+            CKS(tmp_alloc(t_pl, &pl, S));
+            CK(cudaMemcpyAsync(pl, d->syn_plastic, S, cudaMemcpyHostToDevice, s->stream));
+        }
+        CK(cudaMemsetAsync(bad, 0, 4, s->stream));
+        k_validate<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, s->n, 1 << (32 - a.tbits), bad);
+        int32_t hbad = 0;
+        CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        if (hbad) return fail(MGC_ERR_INVALID, "synapse with out-of-range source, target or delay");
+        // CSR by source, synapse-list order inside a row (stable sort)
+        k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(src, S, row_ptr);
+        CKS(exclusive_scan(row_ptr, s->n, s->stream));
+        CKS(tmp_alloc(t_keys, &keys, S));
+        CKS(tmp_alloc(t_vals, &vals, S));
+        CKS(tmp_alloc(t_order, &order, S));
+        k_iota32<<<grid_for(S), 256, 0, s->stream>>>(vals, S);
+        CKS(sort_pairs(src, keys, vals, order, S, a.tbits, s->stream));
+        int32_t* csr_src = nullptr;
+        uint8_t* plastic = nullptr;
+        if (s->stdp) {
+            CKS(s->alloc(&csr_src, S, false));
+            if (d->syn_plastic) CKS(s->alloc(&plastic, S, false));
+        }
+        k_gather_explicit<<<grid_for(S), 256, 0, s->stream>>>(order, keys, tar, w, dl, pl, S, a.tbits, syn,
+                                                               s->csr_syn64, csr_src, plastic);
+        a.csr_src = csr_src;
+        a.plastic = plastic;
+        if (s->stdp) {
+            // incoming lists: CSR positions sorted by target, synapse-list order
+            int64_t* dend_off;
+            int64_t* dend_pos;
+            CKS(s->alloc(&dend_off, (size_t)s->n + 1));
+            CKS(s->alloc(&dend_pos, S, false));
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(tar, S, dend_off);
+            CKS(exclusive_scan(dend_off, s->n, s->stream));
+            k_inverse<<<grid_for(S), 256, 0, s->stream>>>(s->csr_syn64, S, vals);  // vals := pos_of
+            CKS(sort_pairs(tar, keys, vals, order, S, a.tbits, s->stream));
+            k_widen<<<grid_for(S), 256, 0, s->stream>>>(order, S, dend_pos);
+            a.dend_off = dend_off;
+            a.dend_pos = dend_pos;
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s->stream));
+        CKS(max_row(row_ptr, s->n, &max_len));
+    }
+    CKS(init_ring_and_launch(s.get(), max_len));
+    *out = s.release();
+    return MGC_OK;
+}
+
+mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim** out)
+{
+    if (!d || !out) return fail(MGC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->n_pops <= 0 || d->n_proj < 0 || d->n_proj > 16)
+        return fail(MGC_ERR_INVALID, "need 1+ populations and at most 16 projections");
+    CKS(pick_device(d->device));
+    int32_t n = 0;
+    for (int p = 0; p < d->n_pops; ++p) {
+        if (d->pop_start[p] < 0 || d->pop_num[p] < 0) return fail(MGC_ERR_INVALID, "bad population %d", p);
+        n = std::max(n, d->pop_start[p] + d->pop_num[p]);
+    }
+    std::vector<int8_t> type(n, (int8_t)MGC_RAW);
+    for (int p = 0; p < d->n_pops; ++p)
+        for (int32_t i = 0; i < d->pop_num[p]; ++i) type[d->pop_start[p] + i] = (int8_t)d->pop_type[p];
+    ProjTable pt{};
+    pt.n = d->n_proj;
+    int64_t S = 0;
+    int32_t dmin = 0x7fffffff, dmax = 0;
+    for (int r = 0; r < d->n_proj; ++r) {
+        const int sp = d->pr_src[r], tp = d->pr_tar[r];
+        if (sp < 0 || sp >= d->n_pops || tp < 0 || tp >= d->n_pops || d->pr_k[r] < 0 ||
+            d->pr_dmin[r] < 1 || d->pr_dmax[r] < d->pr_dmin[r] || (d->pr_k[r] > 0 && d->pop_num[sp] == 0))
+            return fail(MGC_ERR_INVALID, "bad projection %d", r);
+        pt.base[r] = S;
+        pt.src_start[r] = d->pop_start[sp];
+        pt.src_num[r] = d->pop_num[sp];
+        pt.tar_start[r] = d->pop_start[tp];
+        pt.k[r] = std::max(1, d->pr_k[r]);
+        pt.dmin[r] = d->pr_dmin[r];
+        pt.dspan[r] = d->pr_dmax[r] - d->pr_dmin[r] + 1;
+        pt.w[r] = d->pr_w[r];
+        S += (int64_t)d->pop_num[tp] * d->pr_k[r];
+        if (d->pr_k[r] > 0 && d->pop_num[tp] > 0) {
+            dmin = std::min(dmin, d->pr_dmin[r]);
+            dmax = std::max(dmax, d->pr_dmax[r]);
+        }
+    }
+    pt.base[d->n_proj] = S;
+    if (S == 0) dmin = dmax = 1;
+    std::unique_ptr<mgc_sim> s(new mgc_sim);
+    s->device = d->device;
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->n = n;
+    s->S = S;
+    s->stdp = false;
+    s->mode = MGC_MODE_PUSH;
+    float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
+    CKS(init_common(s.get(), n, type.data(), d->rate, d->v_init, d->lifconst, stdpc, d->seed, d->raster_steps,
+                    d->raster_ids));
+    StepArgs& a = s->a;
+    s->dmin = dmin;
+    s->dmax = dmax;
+    s->M = dmax + 1;
+    a.tbits = bits_for(n);
+    a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
+    if (a.tbits + bits_for((int64_t)dmax + 1) > 32)
+        return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", dmax, n);
+    int64_t* row_ptr;
+    CKS(s->alloc(&row_ptr, (size_t)n + 1));
+    a.row_ptr = row_ptr;
+    uint2* syn;
+    CKS(s->alloc(&syn, S, false));
+    a.syn = syn;
+    int64_t max_len = 0;
+    if (S > 0) {
+        DevTmp t_keys, t_vals, t_k2, t_order;
+        int32_t *keys, *keys2;
+        uint32_t *vals, *order;
+        CKS(tmp_alloc(t_keys, &keys, S));
+        CKS(tmp_alloc(t_vals, &vals, S));
+        k_fid_keys<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, S, keys, vals, row_ptr);
+        CKS(exclusive_scan(row_ptr, n, s->stream));
+        CKS(tmp_alloc(t_k2, &keys2, S));
+        CKS(tmp_alloc(t_order, &order, S));
+        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits, s->stream));
+        k_fid_gather<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, order, S, a.tbits, syn);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s->stream));
+        CKS(max_row(row_ptr, n, &max_len));
+    }
+    CKS(init_ring_and_launch(s.get(), max_len));
+    *out = s.release();
+    return MGC_OK;
+}
+
+mgc_status mgc_run(mgc_sim* s, int64_t steps)
+{
+    if (!s || steps < 0) return fail(MGC_ERR_INVALID, "bad run arguments");
+    CK(cudaSetDevice(s->device));
+    int64_t left = steps;
+    if (left >= kGraphSteps) {
+        if (!s->graph) CKS(build_graph(s));
+        while (left >= s->graph_steps) {
+            CK(cudaGraphLaunch(s->graph, s->stream));
+            s->launches += (int64_t)s->graph_steps * (s->stdp ? 3 : 2);
+            left -= s->graph_steps;
+        }
+    }
+    for (; left > 0; --left) CKS(enqueue_step(s));
+    s->host_step += steps;
+    return MGC_OK;
+}
+
+mgc_status mgc_sync(mgc_sim* s)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    int32_t st = 0;
+    CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
+    if (st) return fail(MGC_ERR_OVERFLOW, "raster buffer overflow (status %d)", st);
+    return MGC_OK;
+}
+
+mgc_status mgc_set_rates(mgc_sim* s, const float* rate, int32_t n)
+{
+    if (!s || !rate || n != s->n) return fail(MGC_ERR_INVALID, "rate array must hold n_neurons entries");
+    CK(cudaSetDevice(s->device));
+    CK(cudaMemcpyAsync(const_cast<float*>(s->a.rate), rate, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+    return MGC_OK;
+}
+
+mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int64_t counts_cap, int32_t* ids,
+                           int64_t ids_cap, int64_t* n_steps, int64_t* n_ids)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->a.record) return fail(MGC_ERR_INVALID, "raster recording is off for this handle");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    int64_t step = 0, step0 = 0, pos = 0;
+    int32_t status = 0;
+    CK(cudaMemcpy(&step, s->a.step, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&step0, s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&pos, s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&status, s->a.status, 4, cudaMemcpyDeviceToHost));
+    const int64_t ns = std::min(step - step0, s->raster_steps_cap);
+    const int64_t ni = std::min(pos, s->raster_ids_cap);
+    std::vector<int32_t> c32(ns);
+    if (ns) CK(cudaMemcpy(c32.data(), s->a.raster_counts, 4 * ns, cudaMemcpyDeviceToHost));
+    std::vector<int32_t> hid(ni);
+    if (ni) CK(cudaMemcpy(hid.data(), s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
+    bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
+    int64_t off = 0;
+    for (int64_t i = 0; i < ns; ++i) {
+        const int64_t c = c32[i];
+        if (off + c <= ni) std::sort(hid.begin() + off, hid.begin() + off + c);
+        if (counts && i < counts_cap) counts[i] = c;
+        off += c;
+    }
+    if (ids) memcpy(ids, hid.data(), 4 * std::min(ni, ids_cap));
+    if (first_step) *first_step = step0;
+    if (n_steps) *n_steps = std::min(ns, counts_cap);
+    if (n_ids) *n_ids = std::min(ni, ids_cap);
+    // clear
+    const int64_t zero = 0;
+    const int32_t zero32 = 0;
+    CK(cudaMemcpy(s->a.raster_step0, &step, 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->a.raster_pos, &zero, 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->a.status, &zero32, 4, cudaMemcpyHostToDevice));
+    if (truncated) return fail(MGC_ERR_OVERFLOW, "raster truncated (device status %d)", status);
+    return MGC_OK;
+}
+
+mgc_status mgc_read_state(mgc_sim* s, float* v, float* i_exc, float* i_inh, int32_t* refrac, int32_t* last_fired,
+                          int32_t* fire_cnt)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    const size_t n = s->n;
+    if (v) CK(cudaMemcpy(v, s->a.V, 4 * n, cudaMemcpyDeviceToHost));
+    if (i_exc) CK(cudaMemcpy(i_exc, s->a.Iexc, 4 * n, cudaMemcpyDeviceToHost));
+    if (i_inh) CK(cudaMemcpy(i_inh, s->a.Iinh, 4 * n, cudaMemcpyDeviceToHost));
+    if (refrac) CK(cudaMemcpy(refrac, s->a.refrac, 4 * n, cudaMemcpyDeviceToHost));
+    if (last_fired) CK(cudaMemcpy(last_fired, s->a.last_fired, 4 * n, cudaMemcpyDeviceToHost));
+    if (fire_cnt) CK(cudaMemcpy(fire_cnt, s->a.fire_cnt, 4 * n, cudaMemcpyDeviceToHost));
+    return MGC_OK;
+}
+
+mgc_status mgc_read_weights(mgc_sim* s, float* weight)
+{
+    if (!s || !weight) return fail(MGC_ERR_INVALID, "null argument");
+    if (!s->csr_syn64) return fail(MGC_ERR_INVALID, "procedural networks have no synapse-list order");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    std::vector<uint2> syn(s->S);
+    std::vector<int64_t> idx(s->S);
+    if (s->S) {
+        CK(cudaMemcpy(syn.data(), s->a.syn, 8 * s->S, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(idx.data(), s->csr_syn64, 8 * s->S, cudaMemcpyDeviceToHost));
+    }
+    for (int64_t p = 0; p < s->S; ++p) {
+        uint32_t b = syn[p].y;
+        memcpy(&weight[idx[p]], &b, 4);
+    }
+    return MGC_OK;
+}
+
+mgc_status mgc_export_csr(mgc_sim* s, int64_t* row_ptr, int32_t* tgt, float* weight, int32_t* delay)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    if (row_ptr) CK(cudaMemcpy(row_ptr, s->a.row_ptr, 8 * ((size_t)s->n + 1), cudaMemcpyDeviceToHost));
+    if (tgt || weight || delay) {
+        std::vector<uint2> syn(s->S);
+        if (s->S) CK(cudaMemcpy(syn.data(), s->a.syn, 8 * s->S, cudaMemcpyDeviceToHost));
+        for (int64_t p = 0; p < s->S; ++p) {
+            if (tgt) tgt[p] = (int32_t)(syn[p].x & s->a.tmask);
+            if (delay) delay[p] = (int32_t)(syn[p].x >> s->a.tbits);
+            if (weight) memcpy(&weight[p], &syn[p].y, 4);
+        }
+    }
+    return MGC_OK;
+}
+
+mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
+{
+    if (!s || !info) return fail(MGC_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    memset(info, 0, sizeof(*info));
+    info->n_neurons = s->n;
+    info->ring_len = s->M;
+    info->min_delay = s->dmin;
+    info->max_delay = s->dmax;
+    info->n_synapses = s->S;
+    CK(cudaMemcpy(&info->step, s->a.step, 8, cudaMemcpyDeviceToHost));
+    unsigned long long ev = 0;
+    CK(cudaMemcpy(&ev, s->a.events, 8, cudaMemcpyDeviceToHost));
+    info->events = (int64_t)ev;
+    info->mode = s->mode;
+    info->graph_steps = s->graph_steps ? s->graph_steps : kGraphSteps;
+    info->device_bytes = (int64_t)s->bytes;
+    return MGC_OK;
+}
+
+mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
+{
+    if (!s || !ms || steps < 0) return fail(MGC_ERR_INVALID, "bad profile arguments");
+    CK(cudaSetDevice(s->device));
+    constexpr int kBatch = 64;
+    std::vector<cudaEvent_t> ev(4 * kBatch);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    double acc[3] = {0, 0, 0};
+    mgc_status st = MGC_OK;
+    for (int64_t done = 0; done < steps && st == MGC_OK;) {
+        const int b = (int)std::min<int64_t>(kBatch, steps - done);
+        for (int i = 0; i < b; ++i) {
+            cudaEvent_t* e = &ev[4 * i];
+            cudaEventRecord(e[0], s->stream);
+            k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+            cudaEventRecord(e[1], s->stream);
+            k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+            cudaEventRecord(e[2], s->stream);
+            s->launches += 2;
+            if (s->stdp) {
+                k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+                s->launches += 1;
+            }
+            cudaEventRecord(e[3], s->stream);
+        }
+        cudaError_t err = cudaStreamSynchronize(s->stream);
+        if (err != cudaSuccess) {
+            st = fail(MGC_ERR_CUDA, "profile: %s", cudaGetErrorString(err));
+            break;
+        }
+        for (int i = 0; i < b; ++i) {
+            float t;
+            cudaEvent_t* e = &ev[4 * i];
+            cudaEventElapsedTime(&t, e[0], e[1]);
+            acc[0] += t;
+            cudaEventElapsedTime(&t, e[1], e[2]);
+            acc[1] += t;
+            cudaEventElapsedTime(&t, e[2], e[3]);
+            acc[2] += t;
+        }
+        done += b;
+        s->host_step += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 3; ++k) ms[k] = (float)acc[k];
+    return st;
+}
+
+mgc_status mgc_get_stream(mgc_sim* s, void** stream)
+{
+    if (!s || !stream) return fail(MGC_ERR_INVALID, "null argument");
+    *stream = (void*)s->stream;
+    return MGC_OK;
+}
+
+int64_t mgc_effective_steps(int64_t steps, int32_t min_delay)
+{
+    if (min_delay < 1 || steps < 0) return -1;
+    const int64_t cycles = steps / min_delay + (steps % min_delay == 0 ? 1 : 0);
+    return std::min(steps, cycles * (int64_t)min_delay);
+}
+
+void mgc_destroy(mgc_sim* s) { delete s; }
+
+const char* mgc_last_error(void) { return g_last_error.c_str(); }
+
+int64_t mgc_kernel_launches(mgc_sim* s) { return s ? s->launches : 0; }
+
+}  // extern "C"
