@@ -1,0 +1,223 @@
+// MGBrain C++ API: Config storage, Model, NetGen.
+#include <chrono>
+#include <cstdlib>
+
+#include "mgbrain/constgen.h"
+#include "mgbrain/netgen.h"
+
+namespace MGBrain {
+
+// Defaults of src/macro.cpp:3-14, plus the additions.
+real Config::STEP = 0.001f;
+real Config::DT = 0.001f;
+real Config::DW = 0.01f;
+bool Config::STDP = false;
+bool Config::SINGLE_GPU = false;
+bool Config::PEER_ACCESS = true;
+bool Config::SHUFFLE_GEN = false;
+bool Config::FIRE_CHECK = false;
+bool Config::DENSE_SPIKE = false;
+bool Config::STAGGERED = false;
+float Config::MIN_GPUMEM = 3.0f;
+bool Config::SEQUENCE = false;
+long long Config::SEED = -1;
+long long Config::NETGEN_SEED = -1;
+int Config::DEVICE = 0;
+bool Config::THROW_ON_ERROR = false;
+bool Config::STDP_BY_TYPE = false;
+
+Model::Model() { indexer = 0; }
+
+void Model::set_lif_const(std::array<real, 30> c)
+{
+    nlifconst = true;
+    lifconst = c;
+}
+
+void Model::set_stdp_const(std::array<real, 6> c)
+{
+    nstdpconst = true;
+    stdpconst = c;
+}
+
+Population& Model::create_pop(int num, NeuronType type, bool isSource)
+{
+    pops.emplace_back(indexer++, num, isSource, type);
+    return pops.back();
+}
+
+// src/model/model.cpp:86-111: a one-to-one projection needs equal sizes; a
+// repeated (src, tar) pair replaces the last matching projection only when
+// that projection is not the first one (index > 0), else it is appended.
+bool Model::connect(Population& src, Population tar, std::array<real, 2> w, std::array<real, 2> d, float ctype,
+                    SynapseType stype)
+{
+    if (ctype == 0.0 && src.num != tar.num) return false;
+    int last = -1;
+    for (int i = 0; i < (int)pros.size(); ++i)
+        if (pros[i].src == src.id && pros[i].tar == tar.id) last = i;
+    if (last > 0) {
+        pros[last].wrange = w;
+        pros[last].drange = d;
+        pros[last].ctype = ctype;
+        pros[last].stype = stype;
+    } else {
+        pros.emplace_back(src.id, tar.id, w, d, ctype, stype);
+    }
+    return true;
+}
+
+bool Model::connect(Population& src, Population tar, real weight, real delay, float ctype, SynapseType stype)
+{
+    return connect(src, tar, {weight, weight}, {delay, delay}, ctype, stype);
+}
+
+bool Model::connect(Population& src, Population tar, std::array<real, 2> w, std::array<real, 2> d, float ctype)
+{
+    return connect(src, tar, w, d, ctype, SynapseType::STATIC);
+}
+
+bool Model::connect(Population& src, Population tar, real weight, real delay, float ctype)
+{
+    return connect(src, tar, {weight, weight}, {delay, delay}, ctype, SynapseType::STATIC);
+}
+
+// ---------------------------------------------------------------------------
+// NetGen: the reference's generation algorithm (src/model/netgen.cpp),
+// consuming std::mt19937 and glibc rand() in the same order.
+// ---------------------------------------------------------------------------
+void NetGen::rand_vector(std::vector<bool>& list, int gen_num, int max_num)
+{
+    list.assign(max_num, false);
+    for (int i = 0; i < max_num && i < gen_num; ++i) list[i] = true;
+    for (int index = max_num - 1; index > 0; --index) {
+        const int j = rand() % max_num;
+        const bool t = list[index];
+        list[index] = list[j];
+        list[j] = t;
+    }
+}
+
+// Weights come in steps of Config::DW; for a range whose floor is >= 0 the
+// steps go downwards from the floor (netgen.cpp:26-29).
+real NetGen::rand_weight(real floor, real ceil)
+{
+    if (ceil == floor) return floor;
+    const int range = (int)((ceil - floor) / Config::DW) + 1;
+    const real step = (rand() % range) * Config::DW;
+    return floor < 0 ? floor + step : floor - step;
+}
+
+real NetGen::rand_delay(real floor, real ceil)
+{
+    if (ceil == floor) return floor;
+    const int range = (int)((ceil - floor) / Config::DT) + 1;
+    return floor + (rand() % range) * Config::DT;
+}
+
+namespace {
+
+void add_synapse(Network& net, int src, int tar, real w, real d, SynapseType stype)
+{
+    net.synapses.emplace_back(src, tar, w, d);
+    net.neurons[src].nxt.push_back(tar);
+    net.neurons[tar].pre.push_back(src);
+    net.neurons[src].syns.push_back(net.synapses.size());
+    net.plastic.push_back(stype == SynapseType::STDP ? 1 : 0);
+}
+
+}  // namespace
+
+void NetGen::gen_net(Network& net, Model& model)
+{
+    const unsigned long seed = Config::NETGEN_SEED >= 0
+                                   ? (unsigned long)Config::NETGEN_SEED
+                                   : (unsigned long)std::chrono::system_clock::now().time_since_epoch().count();
+    std::mt19937 rng(seed);
+    net.nlifconst = model.nlifconst;
+    net.nstdpconst = model.nstdpconst;
+    net.lifconst = model.lifconst;
+    net.stdpconst = model.stdpconst;
+    // neurons: population after population, ids in creation order
+    net.pops.reserve(net.pops.size() + model.pops.size());
+    int next_id = 0;
+    for (const Population& p : model.pops) {
+        net.pops.emplace_back(p.id, p.num, p.source, p.type);
+        net.neurons.reserve(net.neurons.size() + p.num);
+        for (int j = 0; j < p.num; ++j) {
+            net.pops.back().neurons[j] = next_id;
+            net.neurons.emplace_back(next_id, p.source, p.type);
+            ++next_id;
+        }
+    }
+    model.indexer = next_id;
+
+    for (const Projection& pr : model.pros) {
+        const Pop& sp = net.pops[pr.src];
+        const Pop& tp = net.pops[pr.tar];
+        const int sn = sp.num, tn = tp.num;
+        const real w0 = pr.wrange[0], w1 = pr.wrange[1], d0 = pr.drange[0], d1 = pr.drange[1];
+        if (pr.ctype == 1.0) {
+            net.synapses.reserve(net.synapses.size() + (size_t)sn * tn);
+            for (int m = 0; m < sn; ++m)
+                for (int n = 0; n < tn; ++n) {
+                    const real w = rand_weight(w0, w1);
+                    const real d = rand_delay(d0, d1);
+                    add_synapse(net, sp.neurons[m], tp.neurons[n], w, d, pr.stype);
+                }
+        } else if (pr.ctype == 0.0) {
+            for (int k = 0; k < sn; ++k) {
+                const real w = rand_weight(w0, w1);
+                const real d = rand_delay(d0, d1);
+                add_synapse(net, sp.neurons[k], tp.neurons[k], w, d, pr.stype);
+            }
+        } else if (pr.ctype > 0.0 && pr.ctype < 1.0) {
+            if (Config::SHUFFLE_GEN) {
+                // exactly round(sn*tn*p) pairs placed by a rand()-driven
+                // shuffle (std::random_shuffle in libstdc++: position i swaps
+                // with rand() % (i+1))
+                const size_t len = (size_t)(int)(sn * tn);
+                const size_t gen_num = (size_t)std::round(len * pr.ctype);
+                std::vector<bool> chosen(len);
+                for (size_t k = 0; k < len; ++k) chosen[k] = k < gen_num;
+                for (size_t k = 1; k < len; ++k) {
+                    const size_t j = (size_t)((long)rand() % (long)(k + 1));
+                    if (j != k) {
+                        const bool t = chosen[k];
+                        chosen[k] = chosen[j];
+                        chosen[j] = t;
+                    }
+                }
+                for (int m = 0; m < sn; ++m)
+                    for (int n = 0; n < tn; ++n)
+                        if (chosen[(size_t)m * tn + n]) {
+                            const real w = rand_weight(w0, w1);
+                            const real d = rand_delay(d0, d1);
+                            add_synapse(net, sp.neurons[m], tp.neurons[n], w, d, pr.stype);
+                        }
+            } else {
+                // Each pair in row-major order is taken with probability
+                // 1.1 p while fewer than round(sn*tn*p) are taken; the
+                // remaining slots of the list stay pair (0, 0).
+                const size_t max_num = (size_t)sn * (size_t)tn;
+                const size_t gen_num = static_cast<size_t>(std::round(max_num * pr.ctype));
+                const double limit = gen_num * 1.1;
+                std::vector<size_t> picked(gen_num, 0);
+                size_t count = 0;
+                for (size_t m = 0; m < (size_t)sn; ++m)
+                    for (size_t n = 0; n < (size_t)tn; ++n)
+                        if (count < gen_num && (double)(rng() % max_num) < limit) picked[count++] = m * tn + n;
+                net.synapses.reserve(net.synapses.size() + gen_num);
+                for (size_t t = 0; t < gen_num; ++t) {
+                    const int m = (int)(picked[t] / tn);
+                    const int n = (int)(picked[t] % tn);
+                    const real w = rand_weight(w0, w1);
+                    const real d = rand_delay(d0, d1);
+                    add_synapse(net, sp.neurons[m], tp.neurons[n], w, d, pr.stype);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace MGBrain

