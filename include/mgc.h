@@ -30,10 +30,16 @@ typedef enum mgc_status {
 /* NeuronType values, src/macro.h:40-48. */
 enum { MGC_RAW = 0, MGC_LIF0 = 1, MGC_POISSON = 2, MGC_LIF = 3, MGC_LIFE = 4, MGC_LIFB = 5 };
 
-/* Propagation method. */
+/* Event delivery method.  Both give every neuron the same input sum. */
 enum {
-    MGC_MODE_AUTO = 0,   /* core picks */
-    MGC_MODE_PUSH = 1    /* event push from spiking rows into the delay ring */
+    MGC_MODE_AUTO = 0,     /* DEFERRED when the network allows it, else PUSH */
+    MGC_MODE_PUSH = 1,     /* push from spiking rows into the M-slot delay ring at
+                              the emission step (mgcore.cu:271-305); required
+                              when weights are plastic */
+    MGC_MODE_DEFERRED = 2  /* rows bucketed by delay; at step s the spikes of
+                              step s-d push their delay-d bucket into one
+                              L2-resident accumulator per neuron (static
+                              weights, < 2^32 synapses, <= 2048 delay values) */
 };
 
 typedef struct mgc_sim mgc_sim;

@@ -1,9 +1,20 @@
 // Device kernels of the simulation core (sm_100a).
 //
-// One simulation step is two or three launches on the handle's stream:
-//   k_neuron  neuron update of every neuron + spike compaction
-//   k_push    event delivery from the spiking rows into the delay ring
+// Two delivery methods compute the same input currents:
+//  ring (immediate push; needed when weights are plastic):
+//   k_neuron  neuron update reading ring slot s % M, spike compaction
+//   k_push    event push from the spiking rows into ring slots (s+d) % M
 //   k_stdp    (Config::STDP) weight update over the spikers' rows
+//  deferred (static weights):
+//   k_deliver events whose arrival step is s: for every delay d, the
+//             spikes of step s-d push their delay-d row segment (rows are
+//             bucketed by delay) into one accumulator per neuron, which
+//             stays resident in L2 instead of an M-slot ring in HBM
+//   k_neuron  neuron update reading and clearing the accumulators; spikes
+//             go to the history slot s % H.
+// A ring slot receives exactly the events whose arrival step is that of the
+// slot (delays are 1..M-1), so both methods hand every neuron the same sum;
+// with equal weights per sign the fp32 sums are identical in any order.
 // The step number lives in device memory and the last block of the step's
 // last kernel advances it, so the launch sequence of every step is
 // identical and a run of steps can be captured once as a CUDA graph and
@@ -28,6 +39,7 @@ enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2 };
 constexpr int kNeuronBlock = 256;
 constexpr int kPushBlock = 256;
 constexpr int kChunk = 128;           // synapses per warp task (4 per lane)
+constexpr int kMaxBuckets = 2048;     // delay values the deferred method handles
 
 struct StepArgs {
     int32_t n;            // neurons
@@ -42,6 +54,16 @@ struct StepArgs {
     int32_t chunks_per_spike;
     int32_t stdp;
     int32_t record;       // raster recording on
+    int32_t deferred;     // deferred delivery (else ring)
+    int32_t dmin;         // deferred: delay of bucket 0
+    int32_t D;            //   number of delay buckets per row
+    int32_t H;            //   history slots (>= dmax + 1)
+    int32_t bucket_chunks;//   kChunk tasks per bucket (longest bucket)
+    int32_t* hist_ids;    //   [H][n] spike ids per step
+    int32_t* hist_cnt;    //   [H]
+    const uint32_t* bucket;  // [n*D + 1] CSR position of (source, bucket)
+    float* acc_e;         //   [n] input arriving this step
+    float* acc_i;
     // neuron state
     const int8_t* type;
     const float* rate;
@@ -63,7 +85,8 @@ struct StepArgs {
     // step bookkeeping
     int32_t* spk;             // spike ids of the current step
     int32_t* spk_count;
-    int64_t* step;
+    int64_t* step;            // steps done; step[1] packs the slots below
+    int32_t* slots;           // [0] = step % M (ring slot), [1] = step % H (history slot)
     unsigned int* done;       // blocks finished in the step's last kernel
     unsigned long long* events;
     int32_t* raster_ids;
@@ -94,12 +117,23 @@ __device__ __forceinline__ bool last_block(unsigned int* done)
     return is_last;
 }
 
+__device__ __forceinline__ int32_t* step_count(const StepArgs& a, int32_t hslot)
+{
+    return a.deferred ? a.hist_cnt + hslot : a.spk_count;
+}
+
+__device__ __forceinline__ int32_t* step_ids(const StepArgs& a, int32_t hslot)
+{
+    return a.deferred ? a.hist_ids + (size_t)hslot * (size_t)a.n : a.spk;
+}
+
 __device__ __forceinline__ void step_epilogue(const StepArgs& a)
 {
     if (threadIdx.x != 0) return;
     __threadfence();
     const int64_t s = *a.step;
-    const int32_t nspk = *(volatile int32_t*)a.spk_count;
+    const int32_t slot = a.slots[0], hslot = a.slots[1];
+    const int32_t nspk = *(volatile int32_t*)step_count(a, hslot);
     if (a.record) {
         const int64_t idx = s - *a.raster_step0;
         if (idx < a.raster_steps_cap)
@@ -110,8 +144,14 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
         if (pos + nspk > a.raster_ids_cap) atomicOr(a.status, kStatusRasterIds);
         *a.raster_pos = pos + nspk;
     }
-    *a.spk_count = 0;
+    const int32_t next_h = hslot + 1 == a.H ? 0 : hslot + 1;
+    if (a.deferred)
+        a.hist_cnt[next_h] = 0;  // held step s+1-H, no longer read
+    else
+        *a.spk_count = 0;
     *a.done = 0;
+    a.slots[0] = slot + 1 == a.M ? 0 : slot + 1;
+    a.slots[1] = next_h;
     __threadfence();
     *a.step = s + 1;
 }
@@ -124,6 +164,7 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
 {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *a.step;
+    const int32_t slot = a.slots[0], hslot = a.slots[1];
     bool fired = false;
     if (i < a.n) {
         const int t = a.type[i];
@@ -136,13 +177,22 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
                 a.last_fired[i] = (int32_t)s;
             }
         } else if (t == kLIF || t == kLIFB || t == kLIFE) {
-            const int32_t slot = (int32_t)(s % a.M);
-            const size_t loc = (size_t)slot * (size_t)a.n + (size_t)i;
-            const float re = a.ring_e[loc];
-            const float ri = a.ring_i[loc];
-            // every LIF-family path clears slot s%M (getInput/clearInput, :94-103)
-            a.ring_e[loc] = 0.0f;
-            a.ring_i[loc] = 0.0f;
+            // every LIF-family path reads and clears this step's input
+            // (getInput/clearInput, :94-103)
+            float* pe;
+            float* pi;
+            if (a.deferred) {
+                pe = a.acc_e + i;
+                pi = a.acc_i + i;
+            } else {
+                const size_t loc = (size_t)slot * (size_t)a.n + (size_t)i;
+                pe = a.ring_e + loc;
+                pi = a.ring_i + loc;
+            }
+            const float re = *pe;
+            const float ri = *pi;
+            *pe = 0.0f;
+            *pi = 0.0f;
             int32_t rf = a.refrac[i];
             float v = a.V[i];
             if (t == kLIFB) {
@@ -215,10 +265,97 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
     if (m) {
         const int lane = threadIdx.x & 31;
         int32_t base = 0;
-        if (lane == 0) base = atomicAdd(a.spk_count, __popc(m));
+        if (lane == 0) base = atomicAdd(step_count(a, hslot), __popc(m));
         base = __shfl_sync(0xffffffffu, base, 0);
-        if (fired) a.spk[base + __popc(m & ((1u << lane) - 1u))] = i;
+        if (fired) {
+            const int32_t pos = base + __popc(m & ((1u << lane) - 1u));
+            step_ids(a, hslot)[pos] = i;
+            if (a.deferred && a.record) {
+                // nothing runs after this kernel in the step: record here
+                const int64_t rp = *a.raster_pos + pos;
+                if (rp < a.raster_ids_cap) a.raster_ids[rp] = i;
+            }
+        }
     }
+    if (a.deferred) {
+        if (last_block(a.done)) step_epilogue(a);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deferred delivery: the events that arrive at step s.  For each delay d of
+// the buckets, the spikes of step s-d send the delay-d segment of their
+// row; task f enumerates (d, spike, 128-synapse chunk) through a prefix sum
+// over the per-delay spike counts kept in shared memory.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    const int64_t s = *a.step;
+    const int32_t hslot = a.slots[1];
+    const int D = a.D;
+    const int CH = a.bucket_chunks;
+    // pre[k] = tasks of buckets < k; bucket k holds delay dmin + k
+    if (threadIdx.x < 32) {
+        int64_t carry = 0;
+        const int lane = threadIdx.x;
+        if (lane == 0) pre[0] = 0;
+        for (int base = 0; base < D; base += 32) {
+            const int k = base + lane;
+            int64_t c = 0;
+            if (k < D && s - (a.dmin + k) >= 0) {
+                int32_t h = hslot - (a.dmin + k);  // slot of step s - d, d < H
+                if (h < 0) h += a.H;
+                c = (int64_t)a.hist_cnt[h] * CH;
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t v = __shfl_up_sync(0xffffffffu, c, o);
+                if (lane >= o) c += v;
+            }
+            if (k < D) pre[k + 1] = carry + c;
+            carry += __shfl_sync(0xffffffffu, c, 31);
+        }
+    }
+    __syncthreads();
+    const int64_t total = pre[D];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long ev = 0;
+    for (int64_t f = warp; f < total; f += nwarps) {
+        int lo = 0, hi = D - 1;  // last k with pre[k] <= f
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+        }
+        const int k = lo;
+        const int64_t local = f - pre[k];
+        const int32_t j = (int32_t)(local / CH);
+        const int32_t c = (int32_t)(local - (int64_t)j * CH);
+        int32_t h = hslot - (a.dmin + k);
+        if (h < 0) h += a.H;
+        const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
+        const uint32_t* bk = a.bucket + (size_t)src * D + k;
+        const int64_t sb = bk[0], se = bk[1];
+        const int64_t b = sb + (int64_t)c * kChunk;
+        if (b >= se) continue;
+        const int64_t e = min(se, b + (int64_t)kChunk);
+        if (lane == 0) ev += (unsigned long long)(e - b);
+        uint2 w[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t q = b + lane + 32 * u;
+            w[u] = q < e ? __ldcs(a.syn + q) : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (b + lane + 32 * u >= e) continue;
+            const float wt = as_f(w[u].y);
+            atomicAdd((wt > 0.0f ? a.acc_e : a.acc_i) + (w[u].x & a.tmask), wt);
+        }
+    }
+    if (lane == 0 && ev) atomicAdd(a.events, ev);
 }
 
 // ---------------------------------------------------------------------------
@@ -229,9 +366,8 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
 {
-    const int64_t s = *a.step;
     const int32_t cnt = *(volatile int32_t*)a.spk_count;
-    const int32_t slot0 = (int32_t)(s % a.M);
+    const int32_t slot0 = a.slots[0];
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;

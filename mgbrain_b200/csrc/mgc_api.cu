@@ -32,27 +32,28 @@ mgc_status fail(mgc_status st, const char* fmt, ...)
     return st;
 }
 
-#define CK(expr)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (expr);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            if (e_ == cudaErrorMemoryAllocation) {                                            \
-                cudaGetLastError();                                                           \
-                return fail(MGC_ERR_NOMEM, "%s: %s", #expr, cudaGetErrorString(e_));          \
-            }                                                                                 \
+#define CK(expr)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess) {                                                                  \
+            if (e_ == cudaErrorMemoryAllocation) {                                                \
+                cudaGetLastError();                                                               \
+                return fail(MGC_ERR_NOMEM, "%s: %s", #expr, cudaGetErrorString(e_));              \
+            }                                                                                     \
             return fail(MGC_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
-                        __LINE__);                                                            \
-        }                                                                                     \
+                        __LINE__);                                                                \
+        }                                                                                         \
     } while (0)
 
-#define CKS(expr)                        \
-    do {                                 \
-        mgc_status s_ = (expr);          \
-        if (s_ != MGC_OK) return s_;     \
+#define CKS(expr)                    \
+    do {                             \
+        mgc_status s_ = (expr);      \
+        if (s_ != MGC_OK) return s_; \
     } while (0)
 
 constexpr int64_t kDefaultRasterSteps = 1 << 16;
 constexpr int kGraphSteps = 64;
+constexpr size_t kMaxBucketBytes = size_t(16) << 30;  // deferred bucket table budget
 
 int bits_for(int64_t n)
 {
@@ -71,11 +72,10 @@ struct mgc_sim {
     int64_t S = 0;
     int mode = MGC_MODE_PUSH;
     bool stdp = false;
-    int neuron_grid = 1, push_grid = 1, stdp_grid = 1;
+    int neuron_grid = 1, push_grid = 1, stdp_grid = 1, deliver_grid = 1;
     std::vector<void*> allocs;
     size_t bytes = 0;
-    int64_t* csr_syn64 = nullptr;     // synapse-list index of each CSR position (explicit nets)
-    int64_t host_step = 0;            // steps enqueued
+    int64_t* csr_syn64 = nullptr;  // synapse-list index of each CSR position (explicit nets)
     int64_t launches = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -110,15 +110,6 @@ struct mgc_sim {
         if (host && count) CK(cudaMemcpyAsync(*p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
         return MGC_OK;
     }
-
-    void release(void* p)
-    {
-        auto it = std::find(allocs.begin(), allocs.end(), p);
-        if (it != allocs.end()) {
-            allocs.erase(it);
-            cudaFree(p);
-        }
-    }
 };
 
 namespace {
@@ -140,51 +131,83 @@ mgc_status tmp_alloc(DevTmp& t, T** p, size_t count)
     return MGC_OK;
 }
 
-__global__ void k_iota32(uint32_t* v, int64_t n)
+#define GRID_STRIDE(i, n) \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); i += (int64_t)gridDim.x * blockDim.x)
+
+__global__ void k_count_rows(const uint32_t* key, int64_t S, int kshift, int64_t* deg)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        v[i] = (uint32_t)i;
+    GRID_STRIDE(k, S) atomicAdd(reinterpret_cast<unsigned long long*>(deg + (key[k] >> kshift)), 1ull);
 }
 
-__global__ void k_count_rows(const int32_t* key, int64_t S, int64_t* deg)
+// Synapse count of every (source, delay bucket) from the sorted keys.
+__global__ void k_count_buckets(const uint32_t* key, int64_t S, int dbits, int D, uint32_t* cnt)
 {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < S; k += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(reinterpret_cast<unsigned long long*>(deg + key[k]), 1ull);
+    GRID_STRIDE(k, S)
+    {
+        const uint32_t src = key[k] >> dbits, b = key[k] & ((1u << dbits) - 1u);
+        atomicAdd(cnt + (size_t)src * D + b, 1u);
+    }
+}
+
+__global__ void k_max_gap(const uint32_t* off, int64_t count, unsigned int* out)
+{
+    GRID_STRIDE(i, count) atomicMax(out, off[i + 1] - off[i]);
 }
 
 __global__ void k_validate(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int32_t n,
                            int32_t dlim, int32_t* bad)
 {
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < S; k += (int64_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(k, S)
+    {
         if (src[k] < 0 || src[k] >= n || tar[k] < 0 || tar[k] >= n || delay[k] < 1 || delay[k] >= dlim)
             atomicOr(bad, 1);
     }
 }
 
-// CSR words from an explicit synapse list gathered in sorted order.
-__global__ void k_gather_explicit(const uint32_t* order, const int32_t* keys, const int32_t* tar, const float* w,
-                                  const int32_t* delay, const uint8_t* plastic_in, int64_t S, int tbits,
-                                  uint2* syn, int64_t* csr_syn, int32_t* csr_src, uint8_t* plastic_out)
+// Sort key of a synapse: source, then (deferred) delay bucket.
+__global__ void k_explicit_keys(const int32_t* src, const int32_t* delay, int64_t S, int dbits, int dmin,
+                                uint32_t* keys, uint32_t* vals)
 {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(k, S)
+    {
+        keys[k] = ((uint32_t)src[k] << dbits) | (uint32_t)(dbits ? delay[k] - dmin : 0);
+        vals[k] = (uint32_t)k;
+    }
+}
+
+// CSR words from an explicit synapse list gathered in sorted order.
+__global__ void k_gather_explicit(const uint32_t* order, const uint32_t* keys, int kshift, const int32_t* tar,
+                                  const float* w, const int32_t* delay, const uint8_t* plastic_in, int64_t S,
+                                  int tbits, uint2* syn, int64_t* csr_syn, int32_t* csr_src, uint8_t* plastic_out)
+{
+    GRID_STRIDE(p, S)
+    {
         const uint32_t k = order[p];
         syn[p] = make_uint2((uint32_t)tar[k] | ((uint32_t)delay[k] << tbits), __float_as_uint(w[k]));
         csr_syn[p] = k;
-        if (csr_src) csr_src[p] = keys[p];
+        if (csr_src) csr_src[p] = (int32_t)(keys[p] >> kshift);
         if (plastic_out) plastic_out[p] = plastic_in ? (plastic_in[k] != 0) : 1;
     }
 }
 
 __global__ void k_inverse(const int64_t* csr_syn, int64_t S, uint32_t* pos_of)
 {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x)
-        pos_of[csr_syn[p]] = (uint32_t)p;
+    GRID_STRIDE(p, S) pos_of[csr_syn[p]] = (uint32_t)p;
 }
 
 __global__ void k_widen(const uint32_t* in, int64_t S, int64_t* out)
 {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x)
-        out[p] = in[p];
+    GRID_STRIDE(p, S) out[p] = in[p];
+}
+
+__global__ void k_iota(uint32_t* v, int64_t S)
+{
+    GRID_STRIDE(p, S) v[p] = (uint32_t)p;
+}
+
+__global__ void k_cast_keys(const int32_t* in, int64_t S, uint32_t* out)
+{
+    GRID_STRIDE(p, S) out[p] = (uint32_t)in[p];
 }
 
 // Fixed in-degree generator (see mgc_fixed_indegree_desc): synapse index
@@ -211,21 +234,22 @@ __device__ __forceinline__ void fid_decode(const ProjTable& pt, uint64_t seed, i
     w = pt.w[r];
 }
 
-__global__ void k_fid_keys(ProjTable pt, uint64_t seed, int64_t S, int32_t* keys, uint32_t* vals, int64_t* deg)
+__global__ void k_fid_keys(ProjTable pt, uint64_t seed, int64_t S, int dbits, int dmin, uint32_t* keys, uint32_t* vals)
 {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < S; i += (int64_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(i, S)
+    {
         int32_t src, tar, d;
         float w;
         fid_decode(pt, seed, i, src, tar, d, w);
-        keys[i] = src;
+        keys[i] = ((uint32_t)src << dbits) | (uint32_t)(dbits ? d - dmin : 0);
         vals[i] = (uint32_t)i;
-        atomicAdd(reinterpret_cast<unsigned long long*>(deg + src), 1ull);
     }
 }
 
 __global__ void k_fid_gather(ProjTable pt, uint64_t seed, const uint32_t* order, int64_t S, int tbits, uint2* syn)
 {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < S; p += (int64_t)gridDim.x * blockDim.x) {
+    GRID_STRIDE(p, S)
+    {
         int32_t src, tar, d;
         float w;
         fid_decode(pt, seed, order[p], src, tar, d, w);
@@ -240,30 +264,29 @@ int grid_for(int64_t n, int block = 256)
 }
 
 // Stable radix sort of (key, value) pairs by key; keys < 2^key_bits.
-mgc_status sort_pairs(const int32_t* keys_in, int32_t* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
+mgc_status sort_pairs(const uint32_t* keys_in, uint32_t* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
                       int64_t S, int key_bits, cudaStream_t st)
 {
-    // CUB takes item counts as int per call: sort in one call when it fits.
     if (S > (int64_t)0x7fffffff) return fail(MGC_ERR_INVALID, "more than 2^31-1 synapses in one sort");
     size_t tb = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
     DevTmp t;
-    void* tp = nullptr;
     CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
-    tp = t.p;
-    CK(cub::DeviceRadixSort::SortPairs(tp, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
+    CK(cub::DeviceRadixSort::SortPairs(t.p, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
     CK(cudaStreamSynchronize(st));
     return MGC_OK;
 }
 
-mgc_status exclusive_scan(int64_t* deg_then_ptr, int32_t n, cudaStream_t st)
+// In-place exclusive scan of count+1 entries (the last entry becomes the total).
+template <class T>
+mgc_status exclusive_scan(T* v, int64_t count, cudaStream_t st)
 {
-    // deg has n+1 entries; turns deg[0..n) into row offsets row_ptr[0..n].
+    if (count + 1 > (int64_t)0x7fffffff) return fail(MGC_ERR_INVALID, "scan too long");
     size_t tb = 0;
-    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, deg_then_ptr, deg_then_ptr, n + 1, st));
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, v, v, (int)(count + 1), st));
     DevTmp t;
     CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
-    CK(cub::DeviceScan::ExclusiveSum(t.p, tb, deg_then_ptr, deg_then_ptr, n + 1, st));
+    CK(cub::DeviceScan::ExclusiveSum(t.p, tb, v, v, (int)(count + 1), st));
     return MGC_OK;
 }
 
@@ -322,9 +345,9 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     CKS(s->alloc(&a.refrac, n));
     CKS(s->alloc(&a.last_fired, n));
     CKS(s->alloc(&a.fire_cnt, n));
-    CKS(s->alloc(&a.spk, n));
     CKS(s->alloc(&a.spk_count, 1));
-    CKS(s->alloc(&a.step, 1));
+    CKS(s->alloc(&a.step, 2));  // step, then the two slot counters
+    a.slots = reinterpret_cast<int32_t*>(a.step + 1);
     CKS(s->alloc(&a.done, 1));
     CKS(s->alloc(&a.events, 1));
     CKS(s->alloc(&a.status, 1));
@@ -345,34 +368,104 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     return MGC_OK;
 }
 
-mgc_status init_ring_and_launch(mgc_sim* s, int64_t max_row_len)
+// Delivery method for this network; fills the layout fields of s->a.
+mgc_status choose_mode(mgc_sim* s, int requested)
 {
     StepArgs& a = s->a;
-    a.M = s->M;
-    CKS(s->alloc(&a.ring_e, (size_t)s->M * s->n));
-    CKS(s->alloc(&a.ring_i, (size_t)s->M * s->n));
-    a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_row_len + kChunk - 1) / kChunk);
+    const int D = s->dmax - s->dmin + 1;
+    const int dbits = D > 1 ? bits_for(D) : 0;
+    const bool deferred_ok = !s->stdp && s->S > 0 && s->S < (int64_t(1) << 32) && D <= kMaxBuckets &&
+                             a.tbits + dbits <= 32 &&
+                             ((size_t)s->n * (size_t)D + 1) * sizeof(uint32_t) <= kMaxBucketBytes;
+    if (requested == MGC_MODE_DEFERRED && !deferred_ok)
+        return fail(MGC_ERR_INVALID, "deferred delivery needs static weights, < 2^32 synapses and <= %d delays",
+                    kMaxBuckets);
+    if (requested == MGC_MODE_PUSH || !deferred_ok) {
+        s->mode = MGC_MODE_PUSH;
+        a.deferred = 0;
+        a.D = 1;
+        a.H = 1;
+    } else {
+        s->mode = MGC_MODE_DEFERRED;
+        a.deferred = 1;
+        a.D = D;
+        a.dmin = s->dmin;
+        a.H = s->dmax + 1;
+    }
+    return MGC_OK;
+}
+
+int sort_dbits(const mgc_sim* s) { return s->a.deferred && s->a.D > 1 ? bits_for(s->a.D) : 0; }
+
+// Shared tail of both builders: row offsets, delay buckets, method buffers
+// and launch shapes.  keys are the sorted CSR keys.
+mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
+{
+    StepArgs& a = s->a;
+    const int dbits = sort_dbits(s);
+    int64_t* row_ptr = const_cast<int64_t*>(a.row_ptr);
+    int64_t max_len = 0;
+    if (s->S > 0) {
+        k_count_rows<<<grid_for(s->S), 256, 0, s->stream>>>(keys, s->S, dbits, row_ptr);
+        CKS(exclusive_scan(row_ptr, s->n, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        CKS(max_row(row_ptr, s->n, &max_len));
+    }
+    a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_len + kChunk - 1) / kChunk);
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, s->device));
     int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push, kPushBlock, 0));
-    s->push_grid = prop.multiProcessorCount * std::max(1, occ);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stdp, kPushBlock, 0));
-    s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
+    if (a.deferred) {
+        const int64_t nb = (int64_t)s->n * a.D;
+        uint32_t* bucket;
+        CKS(s->alloc(&bucket, nb + 1));
+        k_count_buckets<<<grid_for(s->S), 256, 0, s->stream>>>(keys, s->S, dbits, a.D, bucket);
+        CKS(exclusive_scan(bucket, nb, s->stream));
+        DevTmp t;
+        unsigned int* dmax_gap;
+        CKS(tmp_alloc(t, &dmax_gap, 1));
+        CK(cudaMemsetAsync(dmax_gap, 0, 4, s->stream));
+        k_max_gap<<<grid_for(nb), 256, 0, s->stream>>>(bucket, nb, dmax_gap);
+        unsigned int gap = 0;
+        CK(cudaMemcpyAsync(&gap, dmax_gap, 4, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        a.bucket = bucket;
+        a.bucket_chunks = (int32_t)std::max<int64_t>(1, ((int64_t)gap + kChunk - 1) / kChunk);
+        CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
+        CKS(s->alloc(&a.hist_cnt, a.H));
+        CKS(s->alloc(&a.acc_e, s->n));
+        CKS(s->alloc(&a.acc_i, s->n));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_deliver, kPushBlock, 0));
+        s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
+    } else {
+        a.M = s->M;
+        CKS(s->alloc(&a.ring_e, (size_t)s->M * s->n));
+        CKS(s->alloc(&a.ring_i, (size_t)s->M * s->n));
+        CKS(s->alloc(&a.spk, s->n));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push, kPushBlock, 0));
+        s->push_grid = prop.multiProcessorCount * std::max(1, occ);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stdp, kPushBlock, 0));
+        s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
+    }
+    a.M = s->M;
     s->neuron_grid = (s->n + kNeuronBlock - 1) / kNeuronBlock;
     CK(cudaStreamSynchronize(s->stream));
     return MGC_OK;
 }
 
+int kernels_per_step(const mgc_sim* s) { return s->a.deferred ? 2 : (s->stdp ? 3 : 2); }
+
 mgc_status enqueue_step(mgc_sim* s)
 {
-    k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-    k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
-    s->launches += 2;
-    if (s->stdp) {
-        k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
-        s->launches += 1;
+    if (s->a.deferred) {
+        k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+        k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+    } else {
+        k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+        k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+        if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
     }
+    s->launches += kernels_per_step(s);
     CK(cudaGetLastError());
     return MGC_OK;
 }
@@ -399,6 +492,16 @@ mgc_status build_graph(mgc_sim* s)
     return MGC_OK;
 }
 
+mgc_status check_tbits(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    a.tbits = bits_for(s->n);
+    a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
+    if (a.tbits + bits_for((int64_t)s->dmax + 1) > 32)
+        return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", s->dmax, s->n);
+    return MGC_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -410,7 +513,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     if (d->n_neurons <= 0 || !d->type) return fail(MGC_ERR_INVALID, "network needs neurons and types");
     if (d->n_synapses < 0 || (d->n_synapses > 0 && (!d->syn_src || !d->syn_tar || !d->syn_weight || !d->syn_delay)))
         return fail(MGC_ERR_INVALID, "synapse arrays missing");
-    if (d->mode != MGC_MODE_AUTO && d->mode != MGC_MODE_PUSH) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
+    if (d->mode < MGC_MODE_AUTO || d->mode > MGC_MODE_DEFERRED) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
     CKS(pick_device(d->device));
     std::unique_ptr<mgc_sim> s(new mgc_sim);
     s->device = d->device;
@@ -418,7 +521,6 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     s->n = d->n_neurons;
     s->S = d->n_synapses;
     s->stdp = d->stdp != 0;
-    s->mode = MGC_MODE_PUSH;
     CKS(init_common(s.get(), s->n, d->type, d->rate, d->v_init, d->lifconst, d->stdpconst, d->seed,
                     d->raster_steps, d->raster_ids));
     StepArgs& a = s->a;
@@ -435,10 +537,9 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     s->dmin = dmin;
     s->dmax = dmax;
     s->M = dmax + 1;
-    a.tbits = bits_for(s->n);
-    a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
-    if (a.tbits + bits_for((int64_t)dmax + 1) > 32)
-        return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", dmax, s->n);
+    CKS(check_tbits(s.get()));
+    CKS(choose_mode(s.get(), d->mode));
+    const int dbits = sort_dbits(s.get());
 
     int64_t* row_ptr;
     CKS(s->alloc(&row_ptr, (size_t)s->n + 1));
@@ -447,13 +548,14 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     CKS(s->alloc(&syn, S, false));
     a.syn = syn;
     CKS(s->alloc(&s->csr_syn64, S, false));
-    int64_t max_len = 0;
+    DevTmp t_keys2;
+    uint32_t* keys2 = nullptr;
     if (S > 0) {
         DevTmp t_src, t_tar, t_w, t_d, t_pl, t_keys, t_vals, t_order, t_bad;
-        int32_t *src, *tar, *dl, *keys, *bad;
+        int32_t *src, *tar, *dl, *bad;
         float* w;
         uint8_t* pl = nullptr;
-        uint32_t *vals, *order;
+        uint32_t *keys, *vals, *order;
         CKS(tmp_alloc(t_src, &src, S));
         CKS(tmp_alloc(t_tar, &tar, S));
         CKS(tmp_alloc(t_w, &w, S));
@@ -473,21 +575,20 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
         CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         if (hbad) return fail(MGC_ERR_INVALID, "synapse with out-of-range source, target or delay");
-        // CSR by source, synapse-list order inside a row (stable sort)
-        k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(src, S, row_ptr);
-        CKS(exclusive_scan(row_ptr, s->n, s->stream));
+        // CSR by source (and delay bucket), synapse-list order inside (stable)
         CKS(tmp_alloc(t_keys, &keys, S));
         CKS(tmp_alloc(t_vals, &vals, S));
         CKS(tmp_alloc(t_order, &order, S));
-        k_iota32<<<grid_for(S), 256, 0, s->stream>>>(vals, S);
-        CKS(sort_pairs(src, keys, vals, order, S, a.tbits, s->stream));
+        CKS(tmp_alloc(t_keys2, &keys2, S));
+        k_explicit_keys<<<grid_for(S), 256, 0, s->stream>>>(src, dl, S, dbits, s->dmin, keys, vals);
+        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits + dbits, s->stream));
         int32_t* csr_src = nullptr;
         uint8_t* plastic = nullptr;
         if (s->stdp) {
             CKS(s->alloc(&csr_src, S, false));
             if (d->syn_plastic) CKS(s->alloc(&plastic, S, false));
         }
-        k_gather_explicit<<<grid_for(S), 256, 0, s->stream>>>(order, keys, tar, w, dl, pl, S, a.tbits, syn,
+        k_gather_explicit<<<grid_for(S), 256, 0, s->stream>>>(order, keys2, dbits, tar, w, dl, pl, S, a.tbits, syn,
                                                                s->csr_syn64, csr_src, plastic);
         a.csr_src = csr_src;
         a.plastic = plastic;
@@ -497,19 +598,20 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
             int64_t* dend_pos;
             CKS(s->alloc(&dend_off, (size_t)s->n + 1));
             CKS(s->alloc(&dend_pos, S, false));
-            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(tar, S, dend_off);
+            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, keys);
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(keys, S, 0, dend_off);
             CKS(exclusive_scan(dend_off, s->n, s->stream));
             k_inverse<<<grid_for(S), 256, 0, s->stream>>>(s->csr_syn64, S, vals);  // vals := pos_of
-            CKS(sort_pairs(tar, keys, vals, order, S, a.tbits, s->stream));
+            uint32_t* keys_out = reinterpret_cast<uint32_t*>(src);  // src is no longer needed
+            CKS(sort_pairs(keys, keys_out, vals, order, S, a.tbits, s->stream));
             k_widen<<<grid_for(S), 256, 0, s->stream>>>(order, S, dend_pos);
             a.dend_off = dend_off;
             a.dend_pos = dend_pos;
         }
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s->stream));
-        CKS(max_row(row_ptr, s->n, &max_len));
     }
-    CKS(init_ring_and_launch(s.get(), max_len));
+    CKS(finish_build(s.get(), keys2));
     *out = s.release();
     return MGC_OK;
 }
@@ -520,6 +622,7 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim**
     *out = nullptr;
     if (d->n_pops <= 0 || d->n_proj < 0 || d->n_proj > 16)
         return fail(MGC_ERR_INVALID, "need 1+ populations and at most 16 projections");
+    if (d->mode < MGC_MODE_AUTO || d->mode > MGC_MODE_DEFERRED) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
     CKS(pick_device(d->device));
     int32_t n = 0;
     for (int p = 0; p < d->n_pops; ++p) {
@@ -535,8 +638,8 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim**
     int32_t dmin = 0x7fffffff, dmax = 0;
     for (int r = 0; r < d->n_proj; ++r) {
         const int sp = d->pr_src[r], tp = d->pr_tar[r];
-        if (sp < 0 || sp >= d->n_pops || tp < 0 || tp >= d->n_pops || d->pr_k[r] < 0 ||
-            d->pr_dmin[r] < 1 || d->pr_dmax[r] < d->pr_dmin[r] || (d->pr_k[r] > 0 && d->pop_num[sp] == 0))
+        if (sp < 0 || sp >= d->n_pops || tp < 0 || tp >= d->n_pops || d->pr_k[r] < 0 || d->pr_dmin[r] < 1 ||
+            d->pr_dmax[r] < d->pr_dmin[r] || (d->pr_k[r] > 0 && d->pop_num[sp] == 0))
             return fail(MGC_ERR_INVALID, "bad projection %d", r);
         pt.base[r] = S;
         pt.src_start[r] = d->pop_start[sp];
@@ -560,7 +663,6 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim**
     s->n = n;
     s->S = S;
     s->stdp = false;
-    s->mode = MGC_MODE_PUSH;
     float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
     CKS(init_common(s.get(), n, type.data(), d->rate, d->v_init, d->lifconst, stdpc, d->seed, d->raster_steps,
                     d->raster_ids));
@@ -568,34 +670,31 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim**
     s->dmin = dmin;
     s->dmax = dmax;
     s->M = dmax + 1;
-    a.tbits = bits_for(n);
-    a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
-    if (a.tbits + bits_for((int64_t)dmax + 1) > 32)
-        return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", dmax, n);
+    CKS(check_tbits(s.get()));
+    CKS(choose_mode(s.get(), d->mode));
+    const int dbits = sort_dbits(s.get());
     int64_t* row_ptr;
     CKS(s->alloc(&row_ptr, (size_t)n + 1));
     a.row_ptr = row_ptr;
     uint2* syn;
     CKS(s->alloc(&syn, S, false));
     a.syn = syn;
-    int64_t max_len = 0;
+    DevTmp t_keys2;
+    uint32_t* keys2 = nullptr;
     if (S > 0) {
-        DevTmp t_keys, t_vals, t_k2, t_order;
-        int32_t *keys, *keys2;
-        uint32_t *vals, *order;
+        DevTmp t_keys, t_vals, t_order;
+        uint32_t *keys, *vals, *order;
         CKS(tmp_alloc(t_keys, &keys, S));
         CKS(tmp_alloc(t_vals, &vals, S));
-        k_fid_keys<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, S, keys, vals, row_ptr);
-        CKS(exclusive_scan(row_ptr, n, s->stream));
-        CKS(tmp_alloc(t_k2, &keys2, S));
+        k_fid_keys<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, S, dbits, s->dmin, keys, vals);
+        CKS(tmp_alloc(t_keys2, &keys2, S));
         CKS(tmp_alloc(t_order, &order, S));
-        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits, s->stream));
+        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits + dbits, s->stream));
         k_fid_gather<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, order, S, a.tbits, syn);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s->stream));
-        CKS(max_row(row_ptr, n, &max_len));
     }
-    CKS(init_ring_and_launch(s.get(), max_len));
+    CKS(finish_build(s.get(), keys2));
     *out = s.release();
     return MGC_OK;
 }
@@ -609,12 +708,11 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         if (!s->graph) CKS(build_graph(s));
         while (left >= s->graph_steps) {
             CK(cudaGraphLaunch(s->graph, s->stream));
-            s->launches += (int64_t)s->graph_steps * (s->stdp ? 3 : 2);
+            s->launches += (int64_t)s->graph_steps * kernels_per_step(s);
             left -= s->graph_steps;
         }
     }
     for (; left > 0; --left) CKS(enqueue_step(s));
-    s->host_step += steps;
     return MGC_OK;
 }
 
@@ -656,7 +754,7 @@ mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int
     if (ns) CK(cudaMemcpy(c32.data(), s->a.raster_counts, 4 * ns, cudaMemcpyDeviceToHost));
     std::vector<int32_t> hid(ni);
     if (ni) CK(cudaMemcpy(hid.data(), s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
-    bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
+    const bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
     int64_t off = 0;
     for (int64_t i = 0; i < ns; ++i) {
         const int64_t c = c32[i];
@@ -668,7 +766,6 @@ mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int
     if (first_step) *first_step = step0;
     if (n_steps) *n_steps = std::min(ns, counts_cap);
     if (n_ids) *n_ids = std::min(ni, ids_cap);
-    // clear
     const int64_t zero = 0;
     const int32_t zero32 = 0;
     CK(cudaMemcpy(s->a.raster_step0, &step, 8, cudaMemcpyHostToDevice));
@@ -706,10 +803,7 @@ mgc_status mgc_read_weights(mgc_sim* s, float* weight)
         CK(cudaMemcpy(syn.data(), s->a.syn, 8 * s->S, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(idx.data(), s->csr_syn64, 8 * s->S, cudaMemcpyDeviceToHost));
     }
-    for (int64_t p = 0; p < s->S; ++p) {
-        uint32_t b = syn[p].y;
-        memcpy(&weight[idx[p]], &b, 4);
-    }
+    for (int64_t p = 0; p < s->S; ++p) memcpy(&weight[idx[p]], &syn[p].y, 4);
     return MGC_OK;
 }
 
@@ -720,12 +814,17 @@ mgc_status mgc_export_csr(mgc_sim* s, int64_t* row_ptr, int32_t* tgt, float* wei
     CK(cudaStreamSynchronize(s->stream));
     if (row_ptr) CK(cudaMemcpy(row_ptr, s->a.row_ptr, 8 * ((size_t)s->n + 1), cudaMemcpyDeviceToHost));
     if (tgt || weight || delay) {
-        std::vector<uint2> syn(s->S);
-        if (s->S) CK(cudaMemcpy(syn.data(), s->a.syn, 8 * s->S, cudaMemcpyDeviceToHost));
-        for (int64_t p = 0; p < s->S; ++p) {
-            if (tgt) tgt[p] = (int32_t)(syn[p].x & s->a.tmask);
-            if (delay) delay[p] = (int32_t)(syn[p].x >> s->a.tbits);
-            if (weight) memcpy(&weight[p], &syn[p].y, 4);
+        // in pieces, so a large CSR needs no second full-size host copy
+        const int64_t piece = int64_t(1) << 24;
+        std::vector<uint2> buf((size_t)std::min<int64_t>(piece, std::max<int64_t>(s->S, 1)));
+        for (int64_t p0 = 0; p0 < s->S; p0 += piece) {
+            const int64_t c = std::min(piece, s->S - p0);
+            CK(cudaMemcpy(buf.data(), s->a.syn + p0, 8 * c, cudaMemcpyDeviceToHost));
+            for (int64_t q = 0; q < c; ++q) {
+                if (tgt) tgt[p0 + q] = (int32_t)(buf[q].x & s->a.tmask);
+                if (delay) delay[p0 + q] = (int32_t)(buf[q].x >> s->a.tbits);
+                if (weight) memcpy(&weight[p0 + q], &buf[q].y, 4);
+            }
         }
     }
     return MGC_OK;
@@ -765,17 +864,24 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
         const int b = (int)std::min<int64_t>(kBatch, steps - done);
         for (int i = 0; i < b; ++i) {
             cudaEvent_t* e = &ev[4 * i];
-            cudaEventRecord(e[0], s->stream);
-            k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-            cudaEventRecord(e[1], s->stream);
-            k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
-            cudaEventRecord(e[2], s->stream);
-            s->launches += 2;
-            if (s->stdp) {
-                k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
-                s->launches += 1;
+            // ms[0] neuron update, ms[1] event delivery (push or deferred), ms[2] STDP
+            if (s->a.deferred) {
+                cudaEventRecord(e[0], s->stream);
+                k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[1], s->stream);
+                k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[2], s->stream);
+                cudaEventRecord(e[3], s->stream);
+            } else {
+                cudaEventRecord(e[0], s->stream);
+                k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[1], s->stream);
+                k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[2], s->stream);
+                if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[3], s->stream);
             }
-            cudaEventRecord(e[3], s->stream);
+            s->launches += kernels_per_step(s);
         }
         cudaError_t err = cudaStreamSynchronize(s->stream);
         if (err != cudaSuccess) {
@@ -783,17 +889,21 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             break;
         }
         for (int i = 0; i < b; ++i) {
-            float t;
+            float t0, t1, t2;
             cudaEvent_t* e = &ev[4 * i];
-            cudaEventElapsedTime(&t, e[0], e[1]);
-            acc[0] += t;
-            cudaEventElapsedTime(&t, e[1], e[2]);
-            acc[1] += t;
-            cudaEventElapsedTime(&t, e[2], e[3]);
-            acc[2] += t;
+            cudaEventElapsedTime(&t0, e[0], e[1]);
+            cudaEventElapsedTime(&t1, e[1], e[2]);
+            cudaEventElapsedTime(&t2, e[2], e[3]);
+            if (s->a.deferred) {
+                acc[1] += t0;
+                acc[0] += t1;
+            } else {
+                acc[0] += t0;
+                acc[1] += t1;
+                acc[2] += t2;
+            }
         }
         done += b;
-        s->host_step += b;
     }
     for (auto& e : ev) cudaEventDestroy(e);
     for (int k = 0; k < 3; ++k) ms[k] = (float)acc[k];
