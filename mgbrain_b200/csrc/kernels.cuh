@@ -43,6 +43,8 @@ constexpr int kMaxBuckets = 2048;     // delay values the deferred method handle
 
 struct StepArgs {
     int32_t n;            // neurons
+    int32_t ns;           // neuron arrays' length: n rounded up to a multiple of 4
+    int32_t deliver_blocks;  // fused step kernel: blocks that deliver
     int32_t M;            // ring slots = max_delay + 1
     int32_t tbits;        // target bits in a packed CSR word
     uint32_t tmask;
@@ -157,145 +159,180 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
 }
 
 // ---------------------------------------------------------------------------
-// Neuron update, mgsim_neus_core (mgcore.cu:116-234), plus compaction of
-// the spiking ids (warp ballot, one atomic per warp).
+// Neuron update, mgsim_neus_core (mgcore.cu:116-234).  One thread updates a
+// group of 4 consecutive neurons with 16-byte loads and stores (arrays are
+// padded to a multiple of 4 with RAW neurons, which never change); spiking
+// ids are compacted in neuron order within a warp, one atomic per warp.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, int64_t s, float& v, int32_t& rf,
+                                           float re, float ri)
+{
+    bool fired = false;
+    if (t == kPOISSON) {
+        // mgcore.cu:121-131: fires when the per-step probability beats the draw
+        fired = __ldg(a.rate + i) > poisson_uniform(a.seed, i, s);
+    } else if (t == kLIFB) {
+        // mgcore.cu:164-196: threshold on the old V, then leak + input
+        if (rf > 0) {
+            --rf;
+        } else if (v >= a.C[4]) {
+            fired = true;
+            v = a.C[3];
+            rf = a.refrac_steps;
+        } else {
+            const float in = __fadd_rn(re, ri);
+            const float lk = __fmul_rn(a.lifb_leak, v);
+            v = __fadd_rn(v, __fsub_rn(in, lk));
+        }
+    } else if (t == kLIF) {
+        // mgcore.cu:132-163: exponential integration, then threshold
+        if (rf > 0) {
+            --rf;
+        } else {
+            float ie = a.Iexc[i], ii = a.Iinh[i];
+            float nv = __fmul_rn(a.C[17], v);
+            nv = __fadd_rn(nv, a.C[14]);
+            nv = __fadd_rn(nv, __fmul_rn(ie, a.C[12]));
+            nv = __fadd_rn(nv, __fmul_rn(ii, a.C[13]));
+            ie = __fmul_rn(ie, a.C[15]);
+            ii = __fmul_rn(ii, a.C[16]);
+            if (nv >= a.C[4]) {
+                fired = true;
+                nv = a.C[3];
+                rf = a.refrac_steps;
+            } else {
+                ie = __fadd_rn(ie, re);
+                ii = __fadd_rn(ii, ri);
+            }
+            v = nv;
+            a.Iexc[i] = ie;
+            a.Iinh[i] = ii;
+        }
+    } else if (t == kLIFE) {
+        // mgcore.cu:197-233: conductances decay every step
+        const float ie = __fadd_rn(re, __fmul_rn(a.Iexc[i], 0.98f));
+        const float ii = __fadd_rn(-ri, __fmul_rn(a.Iinh[i], 0.99f));
+        a.Iexc[i] = ie;
+        a.Iinh[i] = ii;
+        if (rf > 0) {
+            --rf;
+        } else if (v >= a.C[4]) {
+            fired = true;
+            v = a.C[3];
+            rf = a.refrac_steps;
+        } else {
+            float sum = __fsub_rn(-0.06f, v);
+            sum = __fadd_rn(sum, __fmul_rn(ie, __fsub_rn(0.0f, v)));
+            sum = __fadd_rn(sum, __fmul_rn(ii, __fsub_rn(-0.08f, v)));
+            sum = __fadd_rn(sum, 0.02f);
+            v = __fadd_rn(v, __fmul_rn(sum, 0.005f));
+        }
+    }
+    // RAW and LIF0 have no branch in the reference: never update, never fire.
+    if (fired) {
+        a.fire_cnt[i] += 1;
+        a.last_fired[i] = (int32_t)s;
+    }
+    return fired;
+}
+
+// Updates neuron groups [first warp group .. ) with a warp-strided loop;
+// `warp`/`nwarps` index the warps taking part.  Input of this step is read
+// from (and cleared in) in_e/in_i, which point at the ring slot or the
+// accumulator buffer.
+__device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
+                                              int64_t warp, int64_t nwarps)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t ngroups = a.ns >> 2;
+    int32_t* ids = step_ids(a, hslot);
+    int32_t* cnt = step_count(a, hslot);
+    const int64_t rbase = (a.deferred && a.record) ? *a.raster_pos : 0;
+    for (int64_t gb = warp * 32; gb < ngroups; gb += nwarps * 32) {
+        const int64_t g = gb + lane;
+        unsigned fmask = 0;
+        if (g < ngroups) {
+            const char4 t4 = __ldg(reinterpret_cast<const char4*>(a.type) + g);
+            float4 v4 = reinterpret_cast<float4*>(a.V)[g];
+            int4 r4 = reinterpret_cast<int4*>(a.refrac)[g];
+            const float4 e4 = reinterpret_cast<float4*>(in_e)[g];
+            const float4 i4 = reinterpret_cast<float4*>(in_i)[g];
+            reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            const int32_t i0 = (int32_t)(g << 2);
+            fmask |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e4.x, i4.x) ? 1u : 0u;
+            fmask |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e4.y, i4.y) ? 2u : 0u;
+            fmask |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e4.z, i4.z) ? 4u : 0u;
+            fmask |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e4.w, i4.w) ? 8u : 0u;
+            reinterpret_cast<float4*>(a.V)[g] = v4;
+            reinterpret_cast<int4*>(a.refrac)[g] = r4;
+        }
+        // compaction in neuron order: warp-inclusive scan of spike counts
+        const int c = __popc(fmask);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total) {
+            int32_t base = 0;
+            if (lane == 31) base = atomicAdd(cnt, total);
+            base = __shfl_sync(0xffffffffu, base, 31);
+            int32_t pos = base + incl - c;
+            const int32_t i0 = (int32_t)(g << 2);
+            for (int k = 0; k < 4; ++k) {
+                if (fmask & (1u << k)) {
+                    ids[pos] = i0 + k;
+                    if (a.deferred && a.record && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
+                    ++pos;
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float* acc_buf(const StepArgs& a, float* base, int64_t s)
+{
+    return base + (size_t)(s & 1) * (size_t)a.ns;
+}
+
 __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
 {
-    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t s = *a.step;
     const int32_t slot = a.slots[0], hslot = a.slots[1];
-    bool fired = false;
-    if (i < a.n) {
-        const int t = a.type[i];
-        if (t == kPOISSON) {
-            // mgcore.cu:121-131
-            const float u = poisson_uniform(a.seed, i, s);
-            fired = a.rate[i] > u;
-            if (fired) {
-                a.fire_cnt[i] += 1;
-                a.last_fired[i] = (int32_t)s;
-            }
-        } else if (t == kLIF || t == kLIFB || t == kLIFE) {
-            // every LIF-family path reads and clears this step's input
-            // (getInput/clearInput, :94-103)
-            float* pe;
-            float* pi;
-            if (a.deferred) {
-                pe = a.acc_e + i;
-                pi = a.acc_i + i;
-            } else {
-                const size_t loc = (size_t)slot * (size_t)a.n + (size_t)i;
-                pe = a.ring_e + loc;
-                pi = a.ring_i + loc;
-            }
-            const float re = *pe;
-            const float ri = *pi;
-            *pe = 0.0f;
-            *pi = 0.0f;
-            int32_t rf = a.refrac[i];
-            float v = a.V[i];
-            if (t == kLIFB) {
-                // mgcore.cu:164-196: threshold on the old V, then leak + input
-                if (rf > 0) {
-                    --rf;
-                } else if (v >= a.C[4]) {
-                    fired = true;
-                    v = a.C[3];
-                    rf = a.refrac_steps;
-                } else {
-                    const float in = __fadd_rn(re, ri);
-                    const float lk = __fmul_rn(a.lifb_leak, v);
-                    v = __fadd_rn(v, __fsub_rn(in, lk));
-                }
-            } else if (t == kLIF) {
-                // mgcore.cu:132-163: exponential integration, then threshold
-                if (rf > 0) {
-                    --rf;
-                } else {
-                    float ie = a.Iexc[i], ii = a.Iinh[i];
-                    float nv = __fmul_rn(a.C[17], v);
-                    nv = __fadd_rn(nv, a.C[14]);
-                    nv = __fadd_rn(nv, __fmul_rn(ie, a.C[12]));
-                    nv = __fadd_rn(nv, __fmul_rn(ii, a.C[13]));
-                    ie = __fmul_rn(ie, a.C[15]);
-                    ii = __fmul_rn(ii, a.C[16]);
-                    if (nv >= a.C[4]) {
-                        fired = true;
-                        nv = a.C[3];
-                        rf = a.refrac_steps;
-                    } else {
-                        ie = __fadd_rn(ie, re);
-                        ii = __fadd_rn(ii, ri);
-                    }
-                    v = nv;
-                    a.Iexc[i] = ie;
-                    a.Iinh[i] = ii;
-                }
-            } else {
-                // LIFE, mgcore.cu:197-233: conductances decay every step
-                const float ie = __fadd_rn(re, __fmul_rn(a.Iexc[i], 0.98f));
-                const float ii = __fadd_rn(-ri, __fmul_rn(a.Iinh[i], 0.99f));
-                a.Iexc[i] = ie;
-                a.Iinh[i] = ii;
-                if (rf > 0) {
-                    --rf;
-                } else if (v >= a.C[4]) {
-                    fired = true;
-                    v = a.C[3];
-                    rf = a.refrac_steps;
-                } else {
-                    float sum = __fsub_rn(-0.06f, v);
-                    sum = __fadd_rn(sum, __fmul_rn(ie, __fsub_rn(0.0f, v)));
-                    sum = __fadd_rn(sum, __fmul_rn(ii, __fsub_rn(-0.08f, v)));
-                    sum = __fadd_rn(sum, 0.02f);
-                    v = __fadd_rn(v, __fmul_rn(sum, 0.005f));
-                }
-            }
-            if (fired) {
-                a.fire_cnt[i] += 1;
-                a.last_fired[i] = (int32_t)s;
-            }
-            a.V[i] = v;
-            a.refrac[i] = rf;
-        }
-        // RAW and LIF0 have no branch in the reference: never update, never fire.
+    float *in_e, *in_i;
+    if (a.deferred) {
+        in_e = acc_buf(a, a.acc_e, s);
+        in_i = acc_buf(a, a.acc_i, s);
+    } else {
+        in_e = a.ring_e + (size_t)slot * (size_t)a.ns;
+        in_i = a.ring_i + (size_t)slot * (size_t)a.ns;
     }
-    const unsigned int m = __ballot_sync(0xffffffffu, fired);
-    if (m) {
-        const int lane = threadIdx.x & 31;
-        int32_t base = 0;
-        if (lane == 0) base = atomicAdd(step_count(a, hslot), __popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (fired) {
-            const int32_t pos = base + __popc(m & ((1u << lane) - 1u));
-            step_ids(a, hslot)[pos] = i;
-            if (a.deferred && a.record) {
-                // nothing runs after this kernel in the step: record here
-                const int64_t rp = *a.raster_pos + pos;
-                if (rp < a.raster_ids_cap) a.raster_ids[rp] = i;
-            }
-        }
-    }
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    neuron_groups(a, s, hslot, in_e, in_i, warp, nwarps);
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Deferred delivery: the events that arrive at step s.  For each delay d of
-// the buckets, the spikes of step s-d send the delay-d segment of their
-// row; task f enumerates (d, spike, 128-synapse chunk) through a prefix sum
-// over the per-delay spike counts kept in shared memory.
+// Deferred delivery of the events that arrive at step sa: for each delay d
+// of the buckets, the spikes of step sa-d send the delay-d segment of their
+// row into the accumulator of step sa.  Task f enumerates (d, spike,
+// 128-synapse chunk) through a prefix sum over the per-delay spike counts
+// held in shared memory.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
+__device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
+                                                 int64_t nwarps)
 {
-    __shared__ int64_t pre[kMaxBuckets + 1];
-    const int64_t s = *a.step;
-    const int32_t hslot = a.slots[1];
     const int D = a.D;
     const int CH = a.bucket_chunks;
-    // pre[k] = tasks of buckets < k; bucket k holds delay dmin + k
+    // history slot of step sa: the current slot advanced by (sa - s)
+    int32_t hs = a.slots[1] + (int32_t)(sa - *a.step);
+    if (hs >= a.H) hs -= a.H;
     if (threadIdx.x < 32) {
         int64_t carry = 0;
         const int lane = threadIdx.x;
@@ -303,8 +340,8 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
         for (int base = 0; base < D; base += 32) {
             const int k = base + lane;
             int64_t c = 0;
-            if (k < D && s - (a.dmin + k) >= 0) {
-                int32_t h = hslot - (a.dmin + k);  // slot of step s - d, d < H
+            if (k < D && sa - (a.dmin + k) >= 0) {
+                int32_t h = hs - (a.dmin + k);  // slot of step sa - d, d < H
                 if (h < 0) h += a.H;
                 c = (int64_t)a.hist_cnt[h] * CH;
             }
@@ -319,9 +356,9 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
     }
     __syncthreads();
     const int64_t total = pre[D];
+    float* acc_e = acc_buf(a, a.acc_e, sa);
+    float* acc_i = acc_buf(a, a.acc_i, sa);
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long ev = 0;
     for (int64_t f = warp; f < total; f += nwarps) {
         int lo = 0, hi = D - 1;  // last k with pre[k] <= f
@@ -333,11 +370,11 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
         const int64_t local = f - pre[k];
         const int32_t j = (int32_t)(local / CH);
         const int32_t c = (int32_t)(local - (int64_t)j * CH);
-        int32_t h = hslot - (a.dmin + k);
+        int32_t h = hs - (a.dmin + k);
         if (h < 0) h += a.H;
         const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
-        const uint32_t* bk = a.bucket + (size_t)src * D + k;
-        const int64_t sb = bk[0], se = bk[1];
+        const uint32_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
+        const int64_t sb = __ldg(bk), se = __ldg(bk + 1);
         const int64_t b = sb + (int64_t)c * kChunk;
         if (b >= se) continue;
         const int64_t e = min(se, b + (int64_t)kChunk);
@@ -352,10 +389,35 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
         for (int u = 0; u < 4; ++u) {
             if (b + lane + 32 * u >= e) continue;
             const float wt = as_f(w[u].y);
-            atomicAdd((wt > 0.0f ? a.acc_e : a.acc_i) + (w[u].x & a.tmask), wt);
+            atomicAdd((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
         }
     }
     if (lane == 0 && ev) atomicAdd(a.events, ev);
+}
+
+// Arrivals of the current step (used when the minimum delay is one step).
+__global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    deliver_arrivals(a, *a.step, pre, warp, nwarps);
+}
+
+// One launch per step when the minimum delay is >= 2: the arrivals of step
+// s+1 depend only on spikes of steps <= s-1, so every warp first delivers
+// its share of them into the other accumulator buffer and then updates its
+// share of the neurons for step s; the two memory-latency chains of
+// different warps overlap on each SM.
+__global__ void __launch_bounds__(kPushBlock, 6) k_fused(StepArgs a)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    const int64_t s = *a.step;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    deliver_arrivals(a, s + 1, pre, warp, nwarps);
+    neuron_groups(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
+    if (last_block(a.done)) step_epilogue(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -398,7 +460,7 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
             if (slot >= a.M) slot -= a.M;
             const float wt = as_f(w[u].y);
             float* ring = wt > 0.0f ? a.ring_e : a.ring_i;
-            atomicAdd(ring + (size_t)slot * (size_t)a.n + tgt, wt);
+            atomicAdd(ring + (size_t)slot * (size_t)a.ns + tgt, wt);
         }
     }
     if (lane == 0 && ev) atomicAdd(a.events, ev);

@@ -72,7 +72,9 @@ struct mgc_sim {
     int64_t S = 0;
     int mode = MGC_MODE_PUSH;
     bool stdp = false;
-    int neuron_grid = 1, push_grid = 1, stdp_grid = 1, deliver_grid = 1;
+    int neuron_grid = 1, push_grid = 1, stdp_grid = 1, deliver_grid = 1, fused_grid = 1;
+    bool fused = false;  // one launch per step (deferred, min delay >= 2)
+    bool ahead = true;   // arrivals of the current device step are already delivered
     std::vector<void*> allocs;
     size_t bytes = 0;
     int64_t* csr_syn64 = nullptr;  // synapse-list index of each CSR position (explicit nets)
@@ -325,6 +327,8 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
 {
     StepArgs& a = s->a;
     a.n = n;
+    a.ns = (n + 3) & ~3;  // neuron arrays padded with RAW neurons for 16-byte access
+    const size_t ns = a.ns;
     a.seed = seed;
     memcpy(a.C, lifc, sizeof(a.C));
     if (stdpc) memcpy(a.P, stdpc, sizeof(a.P));
@@ -332,19 +336,21 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     a.refrac_steps = (int32_t)roundf(lifc[8] / lifc[0]) - 1;  // mgcore.cu:184
     a.lifb_leak = lifc[9] != 0.0f ? lifc[9] : 0.005f;          // mgcore.cu:190
     int8_t* d_type;
-    CKS(s->upload(&d_type, type, n));
+    CKS(s->alloc(&d_type, ns));
+    CK(cudaMemcpyAsync(d_type, type, n, cudaMemcpyHostToDevice, s->stream));
     a.type = d_type;
     float* d_rate;
-    CKS(s->upload(&d_rate, rate, n));
+    CKS(s->alloc(&d_rate, ns));
+    if (rate) CK(cudaMemcpyAsync(d_rate, rate, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
     a.rate = d_rate;
-    std::vector<float> v0(n);
+    std::vector<float> v0(ns, 0.0f);
     for (int32_t i = 0; i < n; ++i) v0[i] = v_init ? v_init[i] : lifc[1];  // mgsim.cpp:97
-    CKS(s->upload(&a.V, v0.data(), n));
-    CKS(s->alloc(&a.Iexc, n));
-    CKS(s->alloc(&a.Iinh, n));
-    CKS(s->alloc(&a.refrac, n));
-    CKS(s->alloc(&a.last_fired, n));
-    CKS(s->alloc(&a.fire_cnt, n));
+    CKS(s->upload(&a.V, v0.data(), ns));
+    CKS(s->alloc(&a.Iexc, ns));
+    CKS(s->alloc(&a.Iinh, ns));
+    CKS(s->alloc(&a.refrac, ns));
+    CKS(s->alloc(&a.last_fired, ns));
+    CKS(s->alloc(&a.fire_cnt, ns));
     CKS(s->alloc(&a.spk_count, 1));
     CKS(s->alloc(&a.step, 2));  // step, then the two slot counters
     a.slots = reinterpret_cast<int32_t*>(a.step + 1);
@@ -433,14 +439,18 @@ mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
         a.bucket_chunks = (int32_t)std::max<int64_t>(1, ((int64_t)gap + kChunk - 1) / kChunk);
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
-        CKS(s->alloc(&a.acc_e, s->n));
-        CKS(s->alloc(&a.acc_i, s->n));
+        CKS(s->alloc(&a.acc_e, 2 * (size_t)a.ns));  // two step buffers
+        CKS(s->alloc(&a.acc_i, 2 * (size_t)a.ns));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_deliver, kPushBlock, 0));
         s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
+        // fused step kernel: one resident wave, every warp delivers then updates
+        s->fused = s->dmin >= 2;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused, kPushBlock, 0));
+        s->fused_grid = prop.multiProcessorCount * std::max(1, occ);
     } else {
         a.M = s->M;
-        CKS(s->alloc(&a.ring_e, (size_t)s->M * s->n));
-        CKS(s->alloc(&a.ring_i, (size_t)s->M * s->n));
+        CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns));
+        CKS(s->alloc(&a.ring_i, (size_t)s->M * a.ns));
         CKS(s->alloc(&a.spk, s->n));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_push, kPushBlock, 0));
         s->push_grid = prop.multiProcessorCount * std::max(1, occ);
@@ -448,30 +458,47 @@ mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
         s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
     }
     a.M = s->M;
-    s->neuron_grid = (s->n + kNeuronBlock - 1) / kNeuronBlock;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_neuron, kNeuronBlock, 0));
+    s->neuron_grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((int64_t)prop.multiProcessorCount * std::max(1, occ),
+                             (a.ns / 4 + kNeuronBlock - 1) / kNeuronBlock));
     CK(cudaStreamSynchronize(s->stream));
     return MGC_OK;
 }
 
-int kernels_per_step(const mgc_sim* s) { return s->a.deferred ? 2 : (s->stdp ? 3 : 2); }
+int kernels_per_step(const mgc_sim* s) { return s->a.deferred ? (s->fused ? 1 : 2) : (s->stdp ? 3 : 2); }
 
 mgc_status enqueue_step(mgc_sim* s)
 {
     if (s->a.deferred) {
-        k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
-        k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+        if (s->fused) {
+            if (!s->ahead) {  // arrivals of this step not yet delivered
+                k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+                s->launches += 1;
+            }
+            k_fused<<<s->fused_grid, kPushBlock, 0, s->stream>>>(s->a);
+            s->ahead = true;
+            s->launches += 1;
+        } else {
+            k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+            k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+            s->launches += 2;
+        }
     } else {
         k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
         k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
         if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+        s->launches += kernels_per_step(s);
     }
-    s->launches += kernels_per_step(s);
     CK(cudaGetLastError());
     return MGC_OK;
 }
 
 mgc_status build_graph(mgc_sim* s)
 {
+    // every captured step must start in the same delivery state: for the
+    // fused method that is "arrivals already delivered", which the step
+    // before the graph establishes (mgc_run brings it about first)
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     const int64_t before = s->launches;
@@ -704,6 +731,10 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
     if (!s || steps < 0) return fail(MGC_ERR_INVALID, "bad run arguments");
     CK(cudaSetDevice(s->device));
     int64_t left = steps;
+    if (s->a.deferred && s->fused && !s->ahead && left > 0) {
+        CKS(enqueue_step(s));  // catches up the delivery, leaves ahead = true
+        --left;
+    }
     if (left >= kGraphSteps) {
         if (!s->graph) CKS(build_graph(s));
         while (left >= s->graph_steps) {
@@ -865,7 +896,20 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
         for (int i = 0; i < b; ++i) {
             cudaEvent_t* e = &ev[4 * i];
             // ms[0] neuron update, ms[1] event delivery (push or deferred), ms[2] STDP
-            if (s->a.deferred) {
+            if (s->a.deferred && s->fused) {
+                // the fused step timed as its two parts: neuron update of
+                // step s, then delivery of the arrivals of step s+1
+                if (!s->ahead) {
+                    k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+                    s->ahead = true;
+                }
+                cudaEventRecord(e[0], s->stream);
+                k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[1], s->stream);
+                k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+                cudaEventRecord(e[2], s->stream);
+                cudaEventRecord(e[3], s->stream);
+            } else if (s->a.deferred) {
                 cudaEventRecord(e[0], s->stream);
                 k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
                 cudaEventRecord(e[1], s->stream);
@@ -881,7 +925,7 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
                 if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
                 cudaEventRecord(e[3], s->stream);
             }
-            s->launches += kernels_per_step(s);
+            s->launches += s->a.deferred ? 2 : kernels_per_step(s);
         }
         cudaError_t err = cudaStreamSynchronize(s->stream);
         if (err != cudaSuccess) {
@@ -894,7 +938,10 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             cudaEventElapsedTime(&t0, e[0], e[1]);
             cudaEventElapsedTime(&t1, e[1], e[2]);
             cudaEventElapsedTime(&t2, e[2], e[3]);
-            if (s->a.deferred) {
+            if (s->a.deferred && s->fused) {
+                acc[0] += t0;
+                acc[1] += t1;
+            } else if (s->a.deferred) {
                 acc[1] += t0;
                 acc[0] += t1;
             } else {
