@@ -36,10 +36,16 @@ enum {
     MGC_MODE_PUSH = 1,     /* push from spiking rows into the M-slot delay ring at
                               the emission step (mgcore.cu:271-305); required
                               when weights are plastic */
-    MGC_MODE_DEFERRED = 2  /* rows bucketed by delay; at step s the spikes of
+    MGC_MODE_DEFERRED = 2, /* rows bucketed by delay; at step s the spikes of
                               step s-d push their delay-d bucket into one
                               L2-resident accumulator per neuron (static
                               weights, < 2^32 synapses, <= 2048 delay values) */
+    MGC_MODE_PULL = 3      /* one pass per target over its incoming synapses
+                              each step, adding spiking sources in a fixed
+                              order (deterministic for any weights) with STDP
+                              fused in; cost grows with all synapses, so AUTO
+                              takes it only for plastic networks of <= 2^26
+                              synapses (explicit networks only) */
 };
 
 typedef struct mgc_sim mgc_sim;

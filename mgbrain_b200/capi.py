@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libm
 
 MGC_OK, MGC_ERR_INVALID, MGC_ERR_CUDA, MGC_ERR_NOMEM, MGC_ERR_OVERFLOW, MGC_ERR_NODEVICE = range(6)
 RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)
-MODE_AUTO, MODE_PUSH, MODE_DEFERRED = 0, 1, 2
+MODE_AUTO, MODE_PUSH, MODE_DEFERRED, MODE_PULL = 0, 1, 2, 3
 
 EXPORTED = (
     "mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",

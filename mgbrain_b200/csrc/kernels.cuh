@@ -60,12 +60,19 @@ struct StepArgs {
     int32_t dmin;         // deferred: delay of bucket 0
     int32_t D;            //   number of delay buckets per row
     int32_t H;            //   history slots (>= dmax + 1)
-    int32_t bucket_chunks;//   kChunk tasks per bucket (longest bucket)
+    int32_t bucket_chunks;//   tasks per bucket (longest bucket / (task_lanes * 4))
+    int32_t task_lanes;   //   lanes per delivery task: 8 or 32
     int32_t* hist_ids;    //   [H][n] spike ids per step
     int32_t* hist_cnt;    //   [H]
     const uint32_t* bucket;  // [n*D + 1] CSR position of (source, bucket)
-    float* acc_e;         //   [n] input arriving this step
+    float* acc_e;         //   [2][ns] input arriving at steps of each parity
     float* acc_i;
+    int32_t pull;         // pull method (per-target pass at emission, STDP fused)
+    uint32_t* fired_bits; //   [ns/32] spikes of the current step
+    const int64_t* in_ptr;//   [n+1] incoming rows (by target)
+    uint2* in_ent;        //   [S] {source | delay << tbits, weight bits}, rows sorted by
+                          //   (delay, source, synapse-list order)
+    const uint8_t* in_plastic;  // [S] or null
     // neuron state
     const int8_t* type;
     const float* rate;
@@ -247,7 +254,8 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     const int64_t ngroups = a.ns >> 2;
     int32_t* ids = step_ids(a, hslot);
     int32_t* cnt = step_count(a, hslot);
-    const int64_t rbase = (a.deferred && a.record) ? *a.raster_pos : 0;
+    const bool rec = (a.deferred || a.pull) && a.record;  // no push kernel to record
+    const int64_t rbase = rec ? *a.raster_pos : 0;
     for (int64_t gb = warp * 32; gb < ngroups; gb += nwarps * 32) {
         const int64_t g = gb + lane;
         unsigned fmask = 0;
@@ -267,6 +275,14 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             reinterpret_cast<float4*>(a.V)[g] = v4;
             reinterpret_cast<int4*>(a.refrac)[g] = r4;
         }
+        if (a.pull) {
+            // bitmap of this step's spikes: 8 lanes (32 neurons) per word
+            unsigned wv = fmask << (4 * (lane & 7));
+            wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
+            wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
+            wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
+            if ((lane & 7) == 0) a.fired_bits[(gb >> 3) + (lane >> 3)] = wv;
+        }
         // compaction in neuron order: warp-inclusive scan of spike counts
         const int c = __popc(fmask);
         int incl = c;
@@ -285,7 +301,7 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             for (int k = 0; k < 4; ++k) {
                 if (fmask & (1u << k)) {
                     ids[pos] = i0 + k;
-                    if (a.deferred && a.record && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
+                    if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
                     ++pos;
                 }
             }
@@ -316,6 +332,111 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
+}
+
+// stdp_cal_weight, mgcore.cu:346-364 (dt in steps, nearest-spike pairing).
+__device__ __forceinline__ float stdp_weight(int32_t dt, float w, const float* P)
+{
+    float dw = 0.0f;
+    if (dt < 0)
+        dw = __fmul_rn(P[0], expf(__fdiv_rn((float)dt, P[2])));
+    else if (dt > 0)
+        dw = __fmul_rn(P[1], expf(__fdiv_rn((float)(-dt), P[3])));
+    float nw = __fadd_rn(w, dw);
+    nw = (nw > P[4]) ? P[4] : ((nw < P[5]) ? P[5] : nw);
+    return nw;
+}
+
+__device__ __forceinline__ bool bit_of(const uint32_t* bits, int32_t i) { return (bits[i >> 5] >> (i & 31)) & 1u; }
+
+// ---------------------------------------------------------------------------
+// Pull method, after k_neuron of step s: one warp per target walks its
+// incoming row.  Synapses whose source spiked at s add their (pre-update)
+// weight to ring slot (s + delay) % M of the target, in the order the
+// reference's push visits them for one slot (source ascending, then
+// synapse-list order), so sums are the same fp32 sequence whatever the
+// weights; the same pass applies the reference's STDP (mgcore.cu:365-412):
+// dt = s - last_fired[target] when the source spiked, dt = last_fired[source]
+// - s when the target spiked (both: dt = 0 twice).  No atomics: the warp owns
+// the target's ring entries and incoming weights.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
+{
+    const int64_t s = *a.step;
+    const int32_t slot0 = a.slots[0];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long ev = 0;
+    for (int64_t T = warp; T < a.n; T += nwarps) {
+        const int64_t rb = a.in_ptr[T], re = a.in_ptr[T + 1];
+        if (rb == re) continue;
+        const bool post = bit_of(a.fired_bits, (int32_t)T);
+        const int32_t lfT = a.last_fired[T];
+        // lane 0 keeps the running sums of the ring entries of one delay
+        int32_t cur_d = -1;
+        float ce = 0.0f, ci = 0.0f;
+        bool te = false, ti = false;
+        for (int64_t q0 = rb; q0 < re; q0 += 32) {
+            const int64_t q = q0 + lane;
+            const bool ok = q < re;
+            const uint2 e = ok ? a.in_ent[q] : make_uint2(0u, 0u);
+            const int32_t src = (int32_t)(e.x & a.tmask);
+            const int32_t d = (int32_t)(e.x >> a.tbits);
+            const float w = as_f(e.y);
+            const bool pre = ok && bit_of(a.fired_bits, src);
+            const unsigned m = __ballot_sync(0xffffffffu, pre);
+            unsigned mm = m;
+            while (mm) {  // spiking sources in row order
+                const int l = __ffs(mm) - 1;
+                mm &= mm - 1;
+                const int32_t dl = __shfl_sync(0xffffffffu, d, l);
+                const float wl = __shfl_sync(0xffffffffu, w, l);
+                if (lane == 0) {
+                    if (dl != cur_d) {
+                        if (cur_d >= 0) {
+                            int32_t sl = slot0 + cur_d;
+                            if (sl >= a.M) sl -= a.M;
+                            if (te) a.ring_e[(size_t)sl * a.ns + T] = ce;
+                            if (ti) a.ring_i[(size_t)sl * a.ns + T] = ci;
+                        }
+                        cur_d = dl;
+                        te = ti = false;
+                    }
+                    int32_t sl = slot0 + dl;
+                    if (sl >= a.M) sl -= a.M;
+                    if (wl > 0.0f) {
+                        if (!te) {
+                            ce = a.ring_e[(size_t)sl * a.ns + T];
+                            te = true;
+                        }
+                        ce = __fadd_rn(ce, wl);
+                    } else {
+                        if (!ti) {
+                            ci = a.ring_i[(size_t)sl * a.ns + T];
+                            ti = true;
+                        }
+                        ci = __fadd_rn(ci, wl);
+                    }
+                }
+            }
+            if (lane == 0) ev += (unsigned long long)__popc(m);
+            if (a.stdp && ok && (pre || post) && (!a.in_plastic || a.in_plastic[q])) {
+                float nw = w;
+                if (pre) nw = stdp_weight((int32_t)s - lfT, nw, a.P);
+                if (post) nw = stdp_weight(a.last_fired[src] - (int32_t)s, nw, a.P);
+                a.in_ent[q].y = as_u(nw);
+            }
+        }
+        if (lane == 0 && cur_d >= 0) {
+            int32_t sl = slot0 + cur_d;
+            if (sl >= a.M) sl -= a.M;
+            if (te) a.ring_e[(size_t)sl * a.ns + T] = ce;
+            if (ti) a.ring_i[(size_t)sl * a.ns + T] = ci;
+        }
+    }
+    if (lane == 0 && ev) atomicAdd(a.events, ev);
+    if (last_block(a.done)) step_epilogue(a);
 }
 
 // ---------------------------------------------------------------------------
@@ -358,9 +479,17 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
     const int64_t total = pre[D];
     float* acc_e = acc_buf(a, a.acc_e, sa);
     float* acc_i = acc_buf(a, a.acc_i, sa);
+    // Lane groups of G lanes each take one task (a chunk of G*4 synapses of
+    // one bucket), so a warp keeps 32/G independent chains in flight.
+    const int G = a.task_lanes;
+    const int per_warp = 32 / G;
     const int lane = threadIdx.x & 31;
+    const int gi = lane / G, li = lane - gi * G;
+    const int span = G * 4;
     unsigned long long ev = 0;
-    for (int64_t f = warp; f < total; f += nwarps) {
+    for (int64_t fb = warp * per_warp; fb < total; fb += nwarps * per_warp) {
+        const int64_t f = fb + gi;
+        if (f >= total) continue;
         int lo = 0, hi = D - 1;  // last k with pre[k] <= f
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
@@ -375,24 +504,24 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
         const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
         const uint32_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
         const int64_t sb = __ldg(bk), se = __ldg(bk + 1);
-        const int64_t b = sb + (int64_t)c * kChunk;
+        const int64_t b = sb + (int64_t)c * span;
         if (b >= se) continue;
-        const int64_t e = min(se, b + (int64_t)kChunk);
-        if (lane == 0) ev += (unsigned long long)(e - b);
+        const int64_t e = min(se, b + (int64_t)span);
+        if (li == 0) ev += (unsigned long long)(e - b);
         uint2 w[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int64_t q = b + lane + 32 * u;
+            const int64_t q = b + li + G * u;
             w[u] = q < e ? __ldcs(a.syn + q) : make_uint2(0u, 0u);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            if (b + lane + 32 * u >= e) continue;
+            if (b + li + G * u >= e) continue;
             const float wt = as_f(w[u].y);
             atomicAdd((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
         }
     }
-    if (lane == 0 && ev) atomicAdd(a.events, ev);
+    if (ev) atomicAdd(a.events, ev);
 }
 
 // Arrivals of the current step (used when the minimum delay is one step).
@@ -469,18 +598,6 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
     }
 }
 
-// stdp_cal_weight, mgcore.cu:346-364 (dt in steps, nearest-spike pairing).
-__device__ __forceinline__ float stdp_weight(int32_t dt, float w, const float* P)
-{
-    float dw = 0.0f;
-    if (dt < 0)
-        dw = __fmul_rn(P[0], expf(__fdiv_rn((float)dt, P[2])));
-    else if (dt > 0)
-        dw = __fmul_rn(P[1], expf(__fdiv_rn((float)(-dt), P[3])));
-    float nw = __fadd_rn(w, dw);
-    nw = (nw > P[4]) ? P[4] : ((nw < P[5]) ? P[5] : nw);
-    return nw;
-}
 
 // ---------------------------------------------------------------------------
 // STDP, mgsim_stdp_core (mgcore.cu:365-412): for each spiking neuron its

@@ -74,6 +74,9 @@ struct mgc_sim {
     bool stdp = false;
     int neuron_grid = 1, push_grid = 1, stdp_grid = 1, deliver_grid = 1, fused_grid = 1;
     bool fused = false;  // one launch per step (deferred, min delay >= 2)
+    bool explicit_net = false;  // built from a synapse list (mgc_create)
+    int pull_grid = 1;
+    int64_t* in_syn64 = nullptr;  // synapse-list index of each incoming-row position (pull)
     bool ahead = true;   // arrivals of the current device step are already delivered
     std::vector<void*> allocs;
     size_t bytes = 0;
@@ -212,6 +215,31 @@ __global__ void k_cast_keys(const int32_t* in, int64_t S, uint32_t* out)
     GRID_STRIDE(p, S) out[p] = (uint32_t)in[p];
 }
 
+// Incoming rows for the pull method: target, then delay, then source, then
+// synapse-list order (the sort is stable).
+__global__ void k_pull_keys(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int tb, int db,
+                            int dmin, uint64_t* keys, uint32_t* vals)
+{
+    GRID_STRIDE(k, S)
+    {
+        keys[k] = ((uint64_t)tar[k] << (db + tb)) | ((uint64_t)(delay[k] - dmin) << tb) | (uint64_t)src[k];
+        vals[k] = (uint32_t)k;
+    }
+}
+
+__global__ void k_gather_pull(const uint32_t* order, const int32_t* src, const float* w, const int32_t* delay,
+                              const uint8_t* plastic_in, int64_t S, int tbits, uint2* ent, int64_t* ent_syn,
+                              uint8_t* plastic_out)
+{
+    GRID_STRIDE(p, S)
+    {
+        const uint32_t k = order[p];
+        ent[p] = make_uint2((uint32_t)src[k] | ((uint32_t)delay[k] << tbits), __float_as_uint(w[k]));
+        ent_syn[p] = k;
+        if (plastic_out) plastic_out[p] = plastic_in ? (plastic_in[k] != 0) : 1;
+    }
+}
+
 // Fixed in-degree generator (see mgc_fixed_indegree_desc): synapse index
 // i -> projection r (by prefix), target t, draw k.
 struct ProjTable {
@@ -266,8 +294,9 @@ int grid_for(int64_t n, int block = 256)
 }
 
 // Stable radix sort of (key, value) pairs by key; keys < 2^key_bits.
-mgc_status sort_pairs(const uint32_t* keys_in, uint32_t* keys_out, const uint32_t* vals_in, uint32_t* vals_out,
-                      int64_t S, int key_bits, cudaStream_t st)
+template <class K>
+mgc_status sort_pairs(const K* keys_in, K* keys_out, const uint32_t* vals_in, uint32_t* vals_out, int64_t S,
+                      int key_bits, cudaStream_t st)
 {
     if (S > (int64_t)0x7fffffff) return fail(MGC_ERR_INVALID, "more than 2^31-1 synapses in one sort");
     size_t tb = 0;
@@ -386,6 +415,21 @@ mgc_status choose_mode(mgc_sim* s, int requested)
     if (requested == MGC_MODE_DEFERRED && !deferred_ok)
         return fail(MGC_ERR_INVALID, "deferred delivery needs static weights, < 2^32 synapses and <= %d delays",
                     kMaxBuckets);
+    // pull: explicit networks whose per-step pass over all synapses is
+    // cheap; AUTO takes it for plastic networks of up to 2^26 synapses
+    const bool pull_ok = s->explicit_net && s->S < (int64_t(1) << 32) && a.tbits + dbits <= 32;
+    if (requested == MGC_MODE_PULL && !pull_ok)
+        return fail(MGC_ERR_INVALID, "the pull method needs an explicit synapse list of < 2^32 synapses");
+    if (requested == MGC_MODE_PULL ||
+        (requested == MGC_MODE_AUTO && s->stdp && pull_ok && s->S <= (int64_t(1) << 26))) {
+        s->mode = MGC_MODE_PULL;
+        a.pull = 1;
+        a.deferred = 0;
+        a.D = D;
+        a.dmin = s->dmin;
+        a.H = 1;
+        return MGC_OK;
+    }
     if (requested == MGC_MODE_PUSH || !deferred_ok) {
         s->mode = MGC_MODE_PUSH;
         a.deferred = 0;
@@ -436,7 +480,12 @@ mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
         CK(cudaMemcpyAsync(&gap, dmax_gap, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         a.bucket = bucket;
-        a.bucket_chunks = (int32_t)std::max<int64_t>(1, ((int64_t)gap + kChunk - 1) / kChunk);
+        // short buckets (the common case of many delays): 8 or 16 lanes per
+        // task, several tasks per warp; long buckets: a whole warp per task
+        const double mean_bucket = (double)s->S / std::max<double>(1.0, (double)s->n * a.D);
+        a.task_lanes = mean_bucket <= 16.0 ? 8 : (mean_bucket <= 48.0 ? 16 : 32);
+        const int64_t span = (int64_t)a.task_lanes * 4;
+        a.bucket_chunks = (int32_t)std::max<int64_t>(1, ((int64_t)gap + span - 1) / span);
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
         CKS(s->alloc(&a.acc_e, 2 * (size_t)a.ns));  // two step buffers
@@ -456,6 +505,12 @@ mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
         s->push_grid = prop.multiProcessorCount * std::max(1, occ);
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stdp, kPushBlock, 0));
         s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
+        if (a.pull) {
+            const int64_t groups = a.ns / 4;
+            CKS(s->alloc(&a.fired_bits, (size_t)((groups + 31) / 32) * 4));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pull, kPushBlock, 0));
+            s->pull_grid = prop.multiProcessorCount * std::max(1, occ);
+        }
     }
     a.M = s->M;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_neuron, kNeuronBlock, 0));
@@ -466,7 +521,12 @@ mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
     return MGC_OK;
 }
 
-int kernels_per_step(const mgc_sim* s) { return s->a.deferred ? (s->fused ? 1 : 2) : (s->stdp ? 3 : 2); }
+int kernels_per_step(const mgc_sim* s)
+{
+    if (s->a.deferred) return s->fused ? 1 : 2;
+    if (s->a.pull) return 2;
+    return s->stdp ? 3 : 2;
+}
 
 mgc_status enqueue_step(mgc_sim* s)
 {
@@ -486,8 +546,12 @@ mgc_status enqueue_step(mgc_sim* s)
         }
     } else {
         k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-        k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
-        if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+        if (s->a.pull) {
+            k_pull<<<s->pull_grid, kPushBlock, 0, s->stream>>>(s->a);
+        } else {
+            k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+            if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+        }
         s->launches += kernels_per_step(s);
     }
     CK(cudaGetLastError());
@@ -540,7 +604,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     if (d->n_neurons <= 0 || !d->type) return fail(MGC_ERR_INVALID, "network needs neurons and types");
     if (d->n_synapses < 0 || (d->n_synapses > 0 && (!d->syn_src || !d->syn_tar || !d->syn_weight || !d->syn_delay)))
         return fail(MGC_ERR_INVALID, "synapse arrays missing");
-    if (d->mode < MGC_MODE_AUTO || d->mode > MGC_MODE_DEFERRED) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
+    if (d->mode < MGC_MODE_AUTO || d->mode > MGC_MODE_PULL) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
     CKS(pick_device(d->device));
     std::unique_ptr<mgc_sim> s(new mgc_sim);
     s->device = d->device;
@@ -548,6 +612,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     s->n = d->n_neurons;
     s->S = d->n_synapses;
     s->stdp = d->stdp != 0;
+    s->explicit_net = true;
     CKS(init_common(s.get(), s->n, d->type, d->rate, d->v_init, d->lifconst, d->stdpconst, d->seed,
                     d->raster_steps, d->raster_ids));
     StepArgs& a = s->a;
@@ -602,6 +667,35 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
         CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         if (hbad) return fail(MGC_ERR_INVALID, "synapse with out-of-range source, target or delay");
+        if (a.pull) {
+            const int db = s->dmax > s->dmin ? bits_for(s->dmax - s->dmin + 1) : 0;
+            DevTmp t_k64a, t_k64b, t_v, t_o;
+            uint64_t *k64a, *k64b;
+            uint32_t *pv, *po;
+            CKS(tmp_alloc(t_k64a, &k64a, S));
+            CKS(tmp_alloc(t_k64b, &k64b, S));
+            CKS(tmp_alloc(t_v, &pv, S));
+            CKS(tmp_alloc(t_o, &po, S));
+            k_pull_keys<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, a.tbits, db, s->dmin, k64a, pv);
+            CKS(sort_pairs(k64a, k64b, pv, po, S, 2 * a.tbits + db, s->stream));
+            int64_t* in_ptr;
+            uint2* in_ent;
+            uint8_t* in_pl = nullptr;
+            CKS(s->alloc(&in_ptr, (size_t)s->n + 1));
+            CKS(s->alloc(&in_ent, S, false));
+            CKS(s->alloc(&s->in_syn64, S, false));
+            if (s->stdp && d->syn_plastic) CKS(s->alloc(&in_pl, S, false));
+            k_gather_pull<<<grid_for(S), 256, 0, s->stream>>>(po, src, w, dl, pl, S, a.tbits, in_ent, s->in_syn64,
+                                                               in_pl);
+            uint32_t* tkeys = reinterpret_cast<uint32_t*>(pv);
+            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, tkeys);
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(tkeys, S, 0, in_ptr);
+            CKS(exclusive_scan(in_ptr, s->n, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+            a.in_ptr = in_ptr;
+            a.in_ent = in_ent;
+            a.in_plastic = in_pl;
+        }
         // CSR by source (and delay bucket), synapse-list order inside (stable)
         CKS(tmp_alloc(t_keys, &keys, S));
         CKS(tmp_alloc(t_vals, &vals, S));
@@ -611,7 +705,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
         CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits + dbits, s->stream));
         int32_t* csr_src = nullptr;
         uint8_t* plastic = nullptr;
-        if (s->stdp) {
+        if (s->stdp && !a.pull) {
             CKS(s->alloc(&csr_src, S, false));
             if (d->syn_plastic) CKS(s->alloc(&plastic, S, false));
         }
@@ -619,7 +713,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
                                                                s->csr_syn64, csr_src, plastic);
         a.csr_src = csr_src;
         a.plastic = plastic;
-        if (s->stdp) {
+        if (s->stdp && !a.pull) {
             // incoming lists: CSR positions sorted by target, synapse-list order
             int64_t* dend_off;
             int64_t* dend_pos;
@@ -830,9 +924,12 @@ mgc_status mgc_read_weights(mgc_sim* s, float* weight)
     CK(cudaStreamSynchronize(s->stream));
     std::vector<uint2> syn(s->S);
     std::vector<int64_t> idx(s->S);
+    // the pull method keeps the live weights in its incoming rows
+    const uint2* src_words = s->a.pull ? s->a.in_ent : s->a.syn;
+    const int64_t* src_idx = s->a.pull ? s->in_syn64 : s->csr_syn64;
     if (s->S) {
-        CK(cudaMemcpy(syn.data(), s->a.syn, 8 * s->S, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(idx.data(), s->csr_syn64, 8 * s->S, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(syn.data(), src_words, 8 * s->S, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(idx.data(), src_idx, 8 * s->S, cudaMemcpyDeviceToHost));
     }
     for (int64_t p = 0; p < s->S; ++p) memcpy(&weight[idx[p]], &syn[p].y, 4);
     return MGC_OK;
@@ -920,9 +1017,13 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
                 cudaEventRecord(e[0], s->stream);
                 k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
                 cudaEventRecord(e[1], s->stream);
-                k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+                if (s->a.pull) {
+                    k_pull<<<s->pull_grid, kPushBlock, 0, s->stream>>>(s->a);  // delivery + STDP
+                } else {
+                    k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
+                }
                 cudaEventRecord(e[2], s->stream);
-                if (s->stdp) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
+                if (s->stdp && !s->a.pull) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
                 cudaEventRecord(e[3], s->stream);
             }
             s->launches += s->a.deferred ? 2 : kernels_per_step(s);

@@ -43,13 +43,15 @@ def test_stdp_net_fp32_vs_fp64():
 
 
 @pytest.mark.gpu
-def test_stdp_net_cuda_matches_oracle():
+@pytest.mark.parametrize("mode", ["push", "pull"])
+def test_stdp_net_cuda_matches_oracle(mode):
     net = stdp_net.build(n_in=784, n_exc=400)
     oc, oi, ost = run_oracle(net, 2)
+    m = {"push": mgb.MODE_PUSH, "pull": mgb.MODE_PULL}[mode]
     g = mgb.Simulator.from_arrays(net["n"], net["type"], net["src"], net["tar"], net["weight"],
                                   net["delay"], net["lifconst"], net["stdpconst"], stdp=True,
-                                  plastic=net["plastic"], seed=11)
-    assert g.info()["mode"] == mgb.MODE_PUSH
+                                  plastic=net["plastic"], seed=11, mode=m)
+    assert g.info()["mode"] == m
     for ep in range(2):
         g.set_rates(stdp_net.rates(net, ep))
         g.run(stdp_net.REDRAW_STEPS)
