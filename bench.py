@@ -183,7 +183,7 @@ def oracle_sim(w, threads):
             arr([r[4] for r in R], np.int32), arr([r[5] for r in R], np.int32)]
     h = L.mgbo_create_fixed_indegree(*[T._p(k) for k in keep[:3]], len(P),
                                      *[T._p(k) for k in keep[3:]], len(R), T._p(w["rate"]),
-                                     T._p(w["v0"]), T._p(w["lif"]), 1, 1, threads)
+                                     T._p(w["v0"]), T._p(w["lif"]), 1, 1, threads, 0, 0)
     if not h:
         raise MemoryError("oracle could not allocate the network")
     return L, h, T
@@ -419,10 +419,20 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
+    ap.add_argument("--kernel-profile", choices=["quiet", "driven"],
+                    help="only build the network at --scale, run --warmup bench steps and 300 "
+                         "profiled steps (separate kernels); for ncu captures")
     a = ap.parse_args()
     ws, rank, local = dist_init()
     try:
-        if a.impl == "reference":
+        if a.kernel_profile:
+            w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
+            sim = make_sim(w, local, seed=1, record=False)
+            sim.run(CHUNK * a.warmup)
+            ms = sim.profile(300)
+            print(json.dumps({"kernel_profile": a.kernel_profile, "scale": a.scale,
+                              "ms_per_300_steps": ms, "info": sim.info()}))
+        elif a.impl == "reference":
             run_reference(a, ws, rank)
         else:
             run_ours(a, ws, rank, local)

@@ -74,6 +74,8 @@ typedef struct mgc_net_desc {
     int32_t device;            /* CUDA device ordinal */
     int64_t raster_steps;      /* steps the raster holds between reads (0: default) */
     int64_t raster_ids;        /* spike ids it holds between reads (0: default, <0: off) */
+    int32_t id_offset;         /* added to neuron ids in the POISSON draws (a network
+                                  simulated as part of a larger one draws as there) */
 } mgc_net_desc;
 
 /* Procedural fixed in-degree network built on the device.  Population p
@@ -81,7 +83,9 @@ typedef struct mgc_net_desc {
  * r gives every neuron of pop pr_tar[r] exactly pr_k[r] synapses whose
  * sources are drawn uniformly, with replacement, from pop pr_src[r], with
  * weight pr_w[r] and delay uniform in [pr_dmin[r], pr_dmax[r]] steps,
- * from Philox4x32-10 keyed by conn_seed. */
+ * from Philox4x32-10 keyed by conn_seed with counter (target + id_offset, k,
+ * r + proj_offset): a block of a larger network given the offsets it has
+ * there generates the same synapses and POISSON draws as inside it. */
 typedef struct mgc_fixed_indegree_desc {
     int32_t n_pops;
     const int32_t* pop_start;
@@ -103,6 +107,8 @@ typedef struct mgc_fixed_indegree_desc {
     int32_t device;
     int64_t raster_steps;
     int64_t raster_ids;
+    int32_t id_offset;
+    int32_t proj_offset;
 } mgc_fixed_indegree_desc;
 
 typedef struct mgc_info {
@@ -128,6 +134,17 @@ mgc_status mgc_create(const mgc_net_desc* desc, mgc_sim** out);
  * host; no reference counterpart (netgen.cpp:39-229 is host-only and
  * cannot express a fixed in-degree). */
 mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* desc, mgc_sim** out);
+
+/* Many independent fixed in-degree networks advanced together in one
+ * handle (a parameter sweep).  Block b's neurons occupy ids
+ * [start_b, start_b + n_b), start_b = sizes of the blocks before it; its
+ * populations are given relative to start_b.  Block b generates the
+ * synapses it would generate alone with id_offset = start_b and
+ * proj_offset = projections of the earlier blocks, and with the batch's
+ * POISSON seed (blocks[0].seed) its raster equals that lone run's.  All
+ * blocks share blocks[0]'s LIF constants, mode, device and raster sizes.
+ * No reference counterpart (the reference simulates one network). */
+mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, mgc_sim** out);
 
 /* Enqueues `steps` steps on the handle's stream and returns without
  * waiting.  Replaces the step loop of MGSimulator::simulate_sparse

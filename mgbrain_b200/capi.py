@@ -21,7 +21,7 @@ EXPORTED = (
     "mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
-    "mgc_kernel_launches", "mgc_profile_steps",
+    "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch",
 )
 
 
@@ -38,7 +38,7 @@ class NetDesc(C.Structure):
         ("syn_tar", C.c_void_p), ("syn_weight", C.c_void_p), ("syn_delay", C.c_void_p),
         ("syn_plastic", C.c_void_p), ("lifconst", C.c_float * 30), ("stdpconst", C.c_float * 6),
         ("stdp", C.c_int32), ("mode", C.c_int32), ("seed", C.c_uint64), ("device", C.c_int32),
-        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64),
+        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64), ("id_offset", C.c_int32),
     ]
 
 
@@ -50,7 +50,8 @@ class FixedInDegreeDesc(C.Structure):
         ("pr_dmin", C.c_void_p), ("pr_dmax", C.c_void_p), ("rate", C.c_void_p),
         ("v_init", C.c_void_p), ("lifconst", C.c_float * 30), ("conn_seed", C.c_uint64),
         ("seed", C.c_uint64), ("mode", C.c_int32), ("device", C.c_int32),
-        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64),
+        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64), ("id_offset", C.c_int32),
+        ("proj_offset", C.c_int32),
     ]
 
 
@@ -79,6 +80,7 @@ def lib():
     vp, i32, i64 = C.c_void_p, C.c_int32, C.c_int64
     L.mgc_create.argtypes = [C.POINTER(NetDesc), C.POINTER(vp)]
     L.mgc_create_fixed_indegree.argtypes = [C.POINTER(FixedInDegreeDesc), C.POINTER(vp)]
+    L.mgc_create_batch.argtypes = [C.POINTER(FixedInDegreeDesc), i32, C.POINTER(vp)]
     L.mgc_run.argtypes = [vp, i64]
     L.mgc_sync.argtypes = [vp]
     L.mgc_set_rates.argtypes = [vp, vp, i32]
@@ -96,7 +98,7 @@ def lib():
     L.mgc_last_error.restype = C.c_char_p
     L.mgc_kernel_launches.argtypes = [vp]
     L.mgc_kernel_launches.restype = i64
-    for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
+    for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_create_batch", "mgc_run", "mgc_sync", "mgc_set_rates",
                  "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
                  "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
         getattr(L, name).restype = C.c_int
@@ -157,11 +159,10 @@ class Simulator:
         check(L.mgc_create(C.byref(d), C.byref(h)))
         return cls(h.value, int(n), d.n_synapses)
 
-    @classmethod
-    def fixed_indegree(cls, pops, projs, lifconst, rate=None, v_init=None, conn_seed=1, seed=1,
-                       device=0, mode=MODE_AUTO, raster_steps=0, raster_ids=0):
-        """pops: list of (start, num, type); projs: (src_pop, tar_pop, k, w, dmin, dmax)."""
-        L = lib()
+    @staticmethod
+    def _block_desc(pops, projs, lifconst, rate=None, v_init=None, conn_seed=1, seed=1, device=0,
+                    mode=MODE_AUTO, raster_steps=0, raster_ids=0, id_offset=0, proj_offset=0):
+        """A FixedInDegreeDesc plus the arrays it points into (keep both alive)."""
         P = np.asarray(pops, np.int64).reshape(-1, 3)
         R = list(projs)
         a = dict(
@@ -183,10 +184,39 @@ class Simulator:
         d.lifconst[:] = [float(x) for x in np.asarray(lifconst, np.float32)]
         d.conn_seed, d.seed, d.mode, d.device = int(conn_seed), int(seed), int(mode), int(device)
         d.raster_steps, d.raster_ids = int(raster_steps), int(raster_ids)
-        h = C.c_void_p()
-        check(L.mgc_create_fixed_indegree(C.byref(d), C.byref(h)))
+        d.id_offset, d.proj_offset = int(id_offset), int(proj_offset)
         n = int((P[:, 0] + P[:, 1]).max())
         S = int(sum(int(P[r[1], 1]) * int(r[2]) for r in R))
+        return d, a, n, S
+
+    @classmethod
+    def fixed_indegree(cls, pops, projs, lifconst, **kw):
+        """pops: list of (start, num, type); projs: (src_pop, tar_pop, k, w, dmin, dmax);
+        keywords: rate, v_init, conn_seed, seed, device, mode, raster_steps, raster_ids,
+        id_offset, proj_offset."""
+        d, keep, n, S = cls._block_desc(pops, projs, lifconst, **kw)
+        h = C.c_void_p()
+        check(lib().mgc_create_fixed_indegree(C.byref(d), C.byref(h)))
+        return cls(h.value, n, S)
+
+    @classmethod
+    def batch(cls, blocks, lifconst, seed=1, device=0, mode=MODE_AUTO, raster_steps=0, raster_ids=0):
+        """Independent networks side by side in one handle.  blocks: dicts with
+        pops, projs and optional rate, v_init, conn_seed (populations relative
+        to the block)."""
+        descs, keep, n, S = [], [], 0, 0
+        for b in blocks:
+            d, a, nb, sb = cls._block_desc(b["pops"], b["projs"], lifconst, rate=b.get("rate"),
+                                           v_init=b.get("v_init"), conn_seed=b.get("conn_seed", 1),
+                                           seed=seed, device=device, mode=mode,
+                                           raster_steps=raster_steps, raster_ids=raster_ids)
+            descs.append(d)
+            keep.append(a)
+            n += nb
+            S += sb
+        arr = (FixedInDegreeDesc * len(descs))(*descs)
+        h = C.c_void_p()
+        check(lib().mgc_create_batch(arr, len(descs), C.byref(h)))
         return cls(h.value, n, S)
 
     # ---- stepping -------------------------------------------------------

@@ -49,6 +49,7 @@ struct StepArgs {
     int32_t tbits;        // target bits in a packed CSR word
     uint32_t tmask;
     uint64_t seed;        // POISSON draw key
+    int32_t id_offset;    // added to neuron ids in the POISSON draws
     int32_t refrac_steps; // round(t_ref/DT) - 1, mgcore.cu:184
     float lifb_leak;      // 0.005f (mgcore.cu:190) unless lifconst[9] != 0
     float C[30];          // LIFECONSTS
@@ -64,7 +65,7 @@ struct StepArgs {
     int32_t task_lanes;   //   lanes per delivery task: 8 or 32
     int32_t* hist_ids;    //   [H][n] spike ids per step
     int32_t* hist_cnt;    //   [H]
-    const uint32_t* bucket;  // [n*D + 1] CSR position of (source, bucket)
+    const int64_t* bucket;   // [n*D + 1] CSR position of (source, bucket)
     float* acc_e;         //   [2][ns] input arriving at steps of each parity
     float* acc_i;
     int32_t pull;         // pull method (per-target pass at emission, STDP fused)
@@ -177,7 +178,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
     bool fired = false;
     if (t == kPOISSON) {
         // mgcore.cu:121-131: fires when the per-step probability beats the draw
-        fired = __ldg(a.rate + i) > poisson_uniform(a.seed, i, s);
+        fired = __ldg(a.rate + i) > poisson_uniform(a.seed, (int64_t)i + a.id_offset, s);
     } else if (t == kLIFB) {
         // mgcore.cu:164-196: threshold on the old V, then leak + input
         if (rf > 0) {
@@ -502,7 +503,7 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
         int32_t h = hs - (a.dmin + k);
         if (h < 0) h += a.H;
         const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
-        const uint32_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
+        const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
         const int64_t sb = __ldg(bk), se = __ldg(bk + 1);
         const int64_t b = sb + (int64_t)c * span;
         if (b >= se) continue;

@@ -145,18 +145,18 @@ __global__ void k_count_rows(const uint32_t* key, int64_t S, int kshift, int64_t
 }
 
 // Synapse count of every (source, delay bucket) from the sorted keys.
-__global__ void k_count_buckets(const uint32_t* key, int64_t S, int dbits, int D, uint32_t* cnt)
+__global__ void k_count_buckets(const uint32_t* key, int64_t S, int dbits, int D, int64_t* cnt)
 {
     GRID_STRIDE(k, S)
     {
         const uint32_t src = key[k] >> dbits, b = key[k] & ((1u << dbits) - 1u);
-        atomicAdd(cnt + (size_t)src * D + b, 1u);
+        atomicAdd(reinterpret_cast<unsigned long long*>(cnt + (size_t)src * D + b), 1ull);
     }
 }
 
-__global__ void k_max_gap(const uint32_t* off, int64_t count, unsigned int* out)
+__global__ void k_max_gap(const int64_t* off, int64_t count, unsigned long long* out)
 {
-    GRID_STRIDE(i, count) atomicMax(out, off[i + 1] - off[i]);
+    GRID_STRIDE(i, count) atomicMax(out, (unsigned long long)(off[i + 1] - off[i]));
 }
 
 __global__ void k_validate(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int32_t n,
@@ -241,48 +241,59 @@ __global__ void k_gather_pull(const uint32_t* order, const int32_t* src, const f
 }
 
 // Fixed in-degree generator (see mgc_fixed_indegree_desc): synapse index
-// i -> projection r (by prefix), target t, draw k.
-struct ProjTable {
-    int32_t n;
-    int64_t base[17];
-    int32_t src_start[16], src_num[16], tar_start[16], k[16], dmin[16], dspan[16];
-    float w[16];
+// i -> projection r (binary search over the block's table), target t, draw k.
+struct ProjEntry {
+    int64_t base;  // first synapse index of the projection
+    uint64_t seed; // conn_seed of its block
+    int32_t src_start, src_num, tar_start, k, dmin, dspan;
+    float w;
+    int32_t rid;     // projection index in the draws
+    int32_t id_off;  // added to target ids in the draws
+    int32_t pad;
 };
 
-__device__ __forceinline__ void fid_decode(const ProjTable& pt, uint64_t seed, int64_t i, int32_t& src, int32_t& tar,
+__device__ __forceinline__ void fid_decode(const ProjEntry* pt, int32_t npr, int64_t i, int32_t& src, int32_t& tar,
                                            int32_t& delay, float& w)
 {
-    int r = 0;
-    while (r + 1 < pt.n && i >= pt.base[r + 1]) ++r;
-    const int64_t loc = i - pt.base[r];
-    const int32_t tl = (int32_t)(loc / pt.k[r]);
-    const int32_t k = (int32_t)(loc - (int64_t)tl * pt.k[r]);
-    tar = pt.tar_start[r] + tl;
-    const U32x4 x = conn_draw(seed, (uint32_t)tar, (uint32_t)k, (uint32_t)r);
-    src = pt.src_start[r] + (int32_t)scale_u32(x.x, (uint32_t)pt.src_num[r]);
-    delay = pt.dmin[r] + (int32_t)scale_u32(x.y, (uint32_t)pt.dspan[r]);
-    w = pt.w[r];
+    int lo = 0, hi = npr - 1;  // last r with base <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pt[mid].base <= i) lo = mid; else hi = mid - 1;
+    }
+    const ProjEntry& e = pt[lo];
+    const int64_t loc = i - e.base;
+    const int32_t tl = (int32_t)(loc / e.k);
+    const int32_t k = (int32_t)(loc - (int64_t)tl * e.k);
+    tar = e.tar_start + tl;
+    const U32x4 x = conn_draw(e.seed, (uint32_t)(tar + e.id_off), (uint32_t)k, (uint32_t)e.rid);
+    src = e.src_start + (int32_t)scale_u32(x.x, (uint32_t)e.src_num);
+    delay = e.dmin + (int32_t)scale_u32(x.y, (uint32_t)e.dspan);
+    w = e.w;
 }
 
-__global__ void k_fid_keys(ProjTable pt, uint64_t seed, int64_t S, int dbits, int dmin, uint32_t* keys, uint32_t* vals)
+// Keys of synapses [base, base + count) of one block; values are offsets
+// from base.
+__global__ void k_fid_keys(const ProjEntry* pt, int32_t npr, int64_t base, int64_t count, int dbits, int dmin,
+                           uint32_t* keys, uint32_t* vals)
 {
-    GRID_STRIDE(i, S)
+    GRID_STRIDE(j, count)
     {
         int32_t src, tar, d;
         float w;
-        fid_decode(pt, seed, i, src, tar, d, w);
-        keys[i] = ((uint32_t)src << dbits) | (uint32_t)(dbits ? d - dmin : 0);
-        vals[i] = (uint32_t)i;
+        fid_decode(pt, npr, base + j, src, tar, d, w);
+        keys[j] = ((uint32_t)src << dbits) | (uint32_t)(dbits ? d - dmin : 0);
+        vals[j] = (uint32_t)j;
     }
 }
 
-__global__ void k_fid_gather(ProjTable pt, uint64_t seed, const uint32_t* order, int64_t S, int tbits, uint2* syn)
+__global__ void k_fid_gather(const ProjEntry* pt, int32_t npr, int64_t base, const uint32_t* order, int64_t count,
+                             int tbits, uint2* syn)
 {
-    GRID_STRIDE(p, S)
+    GRID_STRIDE(p, count)
     {
         int32_t src, tar, d;
         float w;
-        fid_decode(pt, seed, order[p], src, tar, d, w);
+        fid_decode(pt, npr, base + order[p], src, tar, d, w);
         syn[p] = make_uint2((uint32_t)tar | ((uint32_t)d << tbits), __float_as_uint(w));
     }
 }
@@ -409,12 +420,11 @@ mgc_status choose_mode(mgc_sim* s, int requested)
     StepArgs& a = s->a;
     const int D = s->dmax - s->dmin + 1;
     const int dbits = D > 1 ? bits_for(D) : 0;
-    const bool deferred_ok = !s->stdp && s->S > 0 && s->S < (int64_t(1) << 32) && D <= kMaxBuckets &&
+    const bool deferred_ok = !s->stdp && s->S > 0 && D <= kMaxBuckets &&
                              a.tbits + dbits <= 32 &&
                              ((size_t)s->n * (size_t)D + 1) * sizeof(uint32_t) <= kMaxBucketBytes;
     if (requested == MGC_MODE_DEFERRED && !deferred_ok)
-        return fail(MGC_ERR_INVALID, "deferred delivery needs static weights, < 2^32 synapses and <= %d delays",
-                    kMaxBuckets);
+        return fail(MGC_ERR_INVALID, "deferred delivery needs static weights and <= %d delays", kMaxBuckets);
     // pull: explicit networks whose per-step pass over all synapses is
     // cheap; AUTO takes it for plastic networks of up to 2^26 synapses
     const bool pull_ok = s->explicit_net && s->S < (int64_t(1) << 32) && a.tbits + dbits <= 32;
@@ -447,39 +457,57 @@ mgc_status choose_mode(mgc_sim* s, int requested)
 
 int sort_dbits(const mgc_sim* s) { return s->a.deferred && s->a.D > 1 ? bits_for(s->a.D) : 0; }
 
-// Shared tail of both builders: row offsets, delay buckets, method buffers
-// and launch shapes.  keys are the sorted CSR keys.
-mgc_status finish_build(mgc_sim* s, const uint32_t* keys)
+// Row and bucket counts are accumulated from sorted keys (one call per
+// sorted block), then turned into offsets by finish_build.
+mgc_status begin_layout(mgc_sim* s)
 {
     StepArgs& a = s->a;
+    int64_t* row_ptr;
+    CKS(s->alloc(&row_ptr, (size_t)s->n + 1));
+    a.row_ptr = row_ptr;
+    if (a.deferred) {
+        int64_t* bucket;
+        CKS(s->alloc(&bucket, (size_t)s->n * a.D + 1));
+        a.bucket = bucket;
+    }
+    return MGC_OK;
+}
+
+void count_keys(mgc_sim* s, const uint32_t* keys, int64_t count)
+{
+    if (count <= 0) return;
     const int dbits = sort_dbits(s);
+    k_count_rows<<<grid_for(count), 256, 0, s->stream>>>(keys, count, dbits, const_cast<int64_t*>(s->a.row_ptr));
+    if (s->a.deferred)
+        k_count_buckets<<<grid_for(count), 256, 0, s->stream>>>(keys, count, dbits, s->a.D,
+                                                                 const_cast<int64_t*>(s->a.bucket));
+}
+
+// Shared tail of the builders: offsets, method buffers and launch shapes.
+mgc_status finish_build(mgc_sim* s)
+{
+    StepArgs& a = s->a;
     int64_t* row_ptr = const_cast<int64_t*>(a.row_ptr);
     int64_t max_len = 0;
-    if (s->S > 0) {
-        k_count_rows<<<grid_for(s->S), 256, 0, s->stream>>>(keys, s->S, dbits, row_ptr);
-        CKS(exclusive_scan(row_ptr, s->n, s->stream));
-        CK(cudaStreamSynchronize(s->stream));
-        CKS(max_row(row_ptr, s->n, &max_len));
-    }
+    CKS(exclusive_scan(row_ptr, s->n, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (s->S > 0) CKS(max_row(row_ptr, s->n, &max_len));
     a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_len + kChunk - 1) / kChunk);
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, s->device));
     int occ = 0;
     if (a.deferred) {
         const int64_t nb = (int64_t)s->n * a.D;
-        uint32_t* bucket;
-        CKS(s->alloc(&bucket, nb + 1));
-        k_count_buckets<<<grid_for(s->S), 256, 0, s->stream>>>(keys, s->S, dbits, a.D, bucket);
+        int64_t* bucket = const_cast<int64_t*>(a.bucket);
         CKS(exclusive_scan(bucket, nb, s->stream));
         DevTmp t;
-        unsigned int* dmax_gap;
+        unsigned long long* dmax_gap;
         CKS(tmp_alloc(t, &dmax_gap, 1));
-        CK(cudaMemsetAsync(dmax_gap, 0, 4, s->stream));
+        CK(cudaMemsetAsync(dmax_gap, 0, 8, s->stream));
         k_max_gap<<<grid_for(nb), 256, 0, s->stream>>>(bucket, nb, dmax_gap);
-        unsigned int gap = 0;
-        CK(cudaMemcpyAsync(&gap, dmax_gap, 4, cudaMemcpyDeviceToHost, s->stream));
+        unsigned long long gap = 0;
+        CK(cudaMemcpyAsync(&gap, dmax_gap, 8, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        a.bucket = bucket;
         // short buckets (the common case of many delays): 8 or 16 lanes per
         // task, several tasks per warp; long buckets: a whole warp per task
         const double mean_bucket = (double)s->S / std::max<double>(1.0, (double)s->n * a.D);
@@ -617,6 +645,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
                     d->raster_steps, d->raster_ids));
     StepArgs& a = s->a;
     a.stdp = s->stdp;
+    a.id_offset = d->id_offset;
     const int64_t S = s->S;
     // delay range (mgsim.cpp:42-51); M = max_delay + 1 (:71)
     int32_t dmin = 0x7fffffff, dmax = 0;
@@ -632,10 +661,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     CKS(check_tbits(s.get()));
     CKS(choose_mode(s.get(), d->mode));
     const int dbits = sort_dbits(s.get());
-
-    int64_t* row_ptr;
-    CKS(s->alloc(&row_ptr, (size_t)s->n + 1));
-    a.row_ptr = row_ptr;
+    CKS(begin_layout(s.get()));
     uint2* syn;
     CKS(s->alloc(&syn, S, false));
     a.syn = syn;
@@ -729,95 +755,144 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
             a.dend_off = dend_off;
             a.dend_pos = dend_pos;
         }
+        count_keys(s.get(), keys2, S);
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(s->stream));
     }
-    CKS(finish_build(s.get(), keys2));
+    CKS(finish_build(s.get()));
+    *out = s.release();
+    return MGC_OK;
+}
+
+// Independent fixed in-degree networks ("blocks") laid side by side in one
+// handle: block b's neurons get ids [start_b, start_b + n_b) with start_b
+// the sum of the earlier blocks' sizes, its populations are relative to
+// start_b, and its synapses and draws are those it would generate alone with
+// id_offset = start_b and proj_offset = the number of earlier projections.
+// Each block is generated and sorted separately (a block's synapses occupy
+// one contiguous CSR range), so the total may exceed what one sort takes.
+mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, mgc_sim** out)
+{
+    if (!blocks || !out || n_blocks <= 0) return fail(MGC_ERR_INVALID, "null argument or no blocks");
+    *out = nullptr;
+    const mgc_fixed_indegree_desc& d0 = blocks[0];
+    if (d0.mode < MGC_MODE_AUTO || d0.mode > MGC_MODE_DEFERRED)
+        return fail(MGC_ERR_INVALID, "unknown mode %d", d0.mode);
+    CKS(pick_device(d0.device));
+    std::vector<int64_t> start(n_blocks + 1, 0), pbase(n_blocks + 1, 0), sbase(n_blocks + 1, 0);
+    std::vector<ProjEntry> pt;
+    int32_t dmin = 0x7fffffff, dmax = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        const mgc_fixed_indegree_desc& d = blocks[b];
+        if (d.n_pops <= 0 || d.n_proj < 0) return fail(MGC_ERR_INVALID, "block %d: need 1+ populations", b);
+        if (memcmp(d.lifconst, d0.lifconst, sizeof(d0.lifconst)) != 0)
+            return fail(MGC_ERR_INVALID, "block %d: blocks share one LIF constant set", b);
+        int64_t nb = 0;
+        for (int p = 0; p < d.n_pops; ++p) {
+            if (d.pop_start[p] < 0 || d.pop_num[p] < 0) return fail(MGC_ERR_INVALID, "block %d: bad population %d", b, p);
+            nb = std::max<int64_t>(nb, (int64_t)d.pop_start[p] + d.pop_num[p]);
+        }
+        start[b + 1] = start[b] + nb;
+        int64_t S = sbase[b];
+        for (int r = 0; r < d.n_proj; ++r) {
+            const int sp = d.pr_src[r], tp = d.pr_tar[r];
+            if (sp < 0 || sp >= d.n_pops || tp < 0 || tp >= d.n_pops || d.pr_k[r] < 0 || d.pr_dmin[r] < 1 ||
+                d.pr_dmax[r] < d.pr_dmin[r] || (d.pr_k[r] > 0 && d.pop_num[sp] == 0))
+                return fail(MGC_ERR_INVALID, "block %d: bad projection %d", b, r);
+            ProjEntry e{};
+            e.base = S;
+            e.src_start = (int32_t)start[b] + d.pop_start[sp];
+            e.src_num = d.pop_num[sp];
+            e.tar_start = (int32_t)start[b] + d.pop_start[tp];
+            e.k = std::max(1, d.pr_k[r]);
+            e.dmin = d.pr_dmin[r];
+            e.dspan = d.pr_dmax[r] - d.pr_dmin[r] + 1;
+            e.w = d.pr_w[r];
+            e.seed = d.conn_seed;
+            e.rid = (int32_t)(pbase[b] + r + d.proj_offset);
+            e.id_off = d.id_offset;  // block-local ids are already shifted by start_b
+            pt.push_back(e);
+            const int64_t sr = (int64_t)d.pop_num[tp] * d.pr_k[r];
+            S += sr;
+            if (sr > 0) {
+                dmin = std::min(dmin, d.pr_dmin[r]);
+                dmax = std::max(dmax, d.pr_dmax[r]);
+            }
+        }
+        sbase[b + 1] = S;
+        pbase[b + 1] = pbase[b] + d.n_proj;
+        if (S - sbase[b] > (int64_t)0x7fffffff)
+            return fail(MGC_ERR_INVALID, "block %d has more than 2^31-1 synapses; split it", b);
+    }
+    if (start[n_blocks] > 0x7fffffff) return fail(MGC_ERR_INVALID, "more than 2^31-1 neurons");
+    const int32_t n = (int32_t)start[n_blocks];
+    const int64_t S = sbase[n_blocks];
+    if (S == 0) dmin = dmax = 1;
+    std::vector<int8_t> type(n, (int8_t)MGC_RAW);
+    std::vector<float> rate(n, 0.0f), v0(n, d0.lifconst[1]);
+    for (int b = 0; b < n_blocks; ++b) {
+        const mgc_fixed_indegree_desc& d = blocks[b];
+        const int64_t nb = start[b + 1] - start[b];
+        for (int p = 0; p < d.n_pops; ++p)
+            for (int32_t i = 0; i < d.pop_num[p]; ++i) type[start[b] + d.pop_start[p] + i] = (int8_t)d.pop_type[p];
+        if (d.rate) memcpy(rate.data() + start[b], d.rate, 4 * nb);
+        if (d.v_init) memcpy(v0.data() + start[b], d.v_init, 4 * nb);
+    }
+    std::unique_ptr<mgc_sim> s(new mgc_sim);
+    s->device = d0.device;
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->n = n;
+    s->S = S;
+    s->stdp = false;
+    float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
+    CKS(init_common(s.get(), n, type.data(), rate.data(), v0.data(), d0.lifconst, stdpc, d0.seed, d0.raster_steps,
+                    d0.raster_ids));
+    StepArgs& a = s->a;
+    a.id_offset = d0.id_offset;
+    s->dmin = dmin;
+    s->dmax = dmax;
+    s->M = dmax + 1;
+    CKS(check_tbits(s.get()));
+    CKS(choose_mode(s.get(), d0.mode));
+    const int dbits = sort_dbits(s.get());
+    CKS(begin_layout(s.get()));
+    uint2* syn;
+    CKS(s->alloc(&syn, S, false));
+    a.syn = syn;
+    if (S > 0) {
+        DevTmp t_pt;
+        ProjEntry* dpt;
+        CKS(tmp_alloc(t_pt, &dpt, pt.size()));
+        CK(cudaMemcpyAsync(dpt, pt.data(), sizeof(ProjEntry) * pt.size(), cudaMemcpyHostToDevice, s->stream));
+        int64_t maxS = 0;
+        for (int b = 0; b < n_blocks; ++b) maxS = std::max(maxS, sbase[b + 1] - sbase[b]);
+        DevTmp t_keys, t_vals, t_keys2, t_order;
+        uint32_t *keys, *vals, *keys2, *order;
+        CKS(tmp_alloc(t_keys, &keys, maxS));
+        CKS(tmp_alloc(t_vals, &vals, maxS));
+        CKS(tmp_alloc(t_keys2, &keys2, maxS));
+        CKS(tmp_alloc(t_order, &order, maxS));
+        for (int b = 0; b < n_blocks; ++b) {
+            const int64_t Sb = sbase[b + 1] - sbase[b];
+            if (Sb == 0) continue;
+            const ProjEntry* bpt = dpt + pbase[b];
+            const int npr = (int)(pbase[b + 1] - pbase[b]);
+            k_fid_keys<<<grid_for(Sb), 256, 0, s->stream>>>(bpt, npr, sbase[b], Sb, dbits, s->dmin, keys, vals);
+            CKS(sort_pairs(keys, keys2, vals, order, Sb, a.tbits + dbits, s->stream));
+            k_fid_gather<<<grid_for(Sb), 256, 0, s->stream>>>(bpt, npr, sbase[b], order, Sb, a.tbits, syn + sbase[b]);
+            count_keys(s.get(), keys2, Sb);
+            CK(cudaGetLastError());
+        }
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    CKS(finish_build(s.get()));
     *out = s.release();
     return MGC_OK;
 }
 
 mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim** out)
 {
-    if (!d || !out) return fail(MGC_ERR_INVALID, "null argument");
-    *out = nullptr;
-    if (d->n_pops <= 0 || d->n_proj < 0 || d->n_proj > 16)
-        return fail(MGC_ERR_INVALID, "need 1+ populations and at most 16 projections");
-    if (d->mode < MGC_MODE_AUTO || d->mode > MGC_MODE_DEFERRED) return fail(MGC_ERR_INVALID, "unknown mode %d", d->mode);
-    CKS(pick_device(d->device));
-    int32_t n = 0;
-    for (int p = 0; p < d->n_pops; ++p) {
-        if (d->pop_start[p] < 0 || d->pop_num[p] < 0) return fail(MGC_ERR_INVALID, "bad population %d", p);
-        n = std::max(n, d->pop_start[p] + d->pop_num[p]);
-    }
-    std::vector<int8_t> type(n, (int8_t)MGC_RAW);
-    for (int p = 0; p < d->n_pops; ++p)
-        for (int32_t i = 0; i < d->pop_num[p]; ++i) type[d->pop_start[p] + i] = (int8_t)d->pop_type[p];
-    ProjTable pt{};
-    pt.n = d->n_proj;
-    int64_t S = 0;
-    int32_t dmin = 0x7fffffff, dmax = 0;
-    for (int r = 0; r < d->n_proj; ++r) {
-        const int sp = d->pr_src[r], tp = d->pr_tar[r];
-        if (sp < 0 || sp >= d->n_pops || tp < 0 || tp >= d->n_pops || d->pr_k[r] < 0 || d->pr_dmin[r] < 1 ||
-            d->pr_dmax[r] < d->pr_dmin[r] || (d->pr_k[r] > 0 && d->pop_num[sp] == 0))
-            return fail(MGC_ERR_INVALID, "bad projection %d", r);
-        pt.base[r] = S;
-        pt.src_start[r] = d->pop_start[sp];
-        pt.src_num[r] = d->pop_num[sp];
-        pt.tar_start[r] = d->pop_start[tp];
-        pt.k[r] = std::max(1, d->pr_k[r]);
-        pt.dmin[r] = d->pr_dmin[r];
-        pt.dspan[r] = d->pr_dmax[r] - d->pr_dmin[r] + 1;
-        pt.w[r] = d->pr_w[r];
-        S += (int64_t)d->pop_num[tp] * d->pr_k[r];
-        if (d->pr_k[r] > 0 && d->pop_num[tp] > 0) {
-            dmin = std::min(dmin, d->pr_dmin[r]);
-            dmax = std::max(dmax, d->pr_dmax[r]);
-        }
-    }
-    pt.base[d->n_proj] = S;
-    if (S == 0) dmin = dmax = 1;
-    std::unique_ptr<mgc_sim> s(new mgc_sim);
-    s->device = d->device;
-    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    s->n = n;
-    s->S = S;
-    s->stdp = false;
-    float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
-    CKS(init_common(s.get(), n, type.data(), d->rate, d->v_init, d->lifconst, stdpc, d->seed, d->raster_steps,
-                    d->raster_ids));
-    StepArgs& a = s->a;
-    s->dmin = dmin;
-    s->dmax = dmax;
-    s->M = dmax + 1;
-    CKS(check_tbits(s.get()));
-    CKS(choose_mode(s.get(), d->mode));
-    const int dbits = sort_dbits(s.get());
-    int64_t* row_ptr;
-    CKS(s->alloc(&row_ptr, (size_t)n + 1));
-    a.row_ptr = row_ptr;
-    uint2* syn;
-    CKS(s->alloc(&syn, S, false));
-    a.syn = syn;
-    DevTmp t_keys2;
-    uint32_t* keys2 = nullptr;
-    if (S > 0) {
-        DevTmp t_keys, t_vals, t_order;
-        uint32_t *keys, *vals, *order;
-        CKS(tmp_alloc(t_keys, &keys, S));
-        CKS(tmp_alloc(t_vals, &vals, S));
-        k_fid_keys<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, S, dbits, s->dmin, keys, vals);
-        CKS(tmp_alloc(t_keys2, &keys2, S));
-        CKS(tmp_alloc(t_order, &order, S));
-        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits + dbits, s->stream));
-        k_fid_gather<<<grid_for(S), 256, 0, s->stream>>>(pt, d->conn_seed, order, S, a.tbits, syn);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(s->stream));
-    }
-    CKS(finish_build(s.get(), keys2));
-    *out = s.release();
-    return MGC_OK;
+    return mgc_create_batch(d, 1, out);
 }
 
 mgc_status mgc_run(mgc_sim* s, int64_t steps)

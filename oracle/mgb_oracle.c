@@ -36,6 +36,7 @@ struct mgbo_sim {
     float lifb_leak;
     int stdp;
     uint64_t seed;
+    int32_t id_offset;
     int64_t step, events;
     int32_t* spk;
 };
@@ -405,7 +406,7 @@ mgbo_sim* mgbo_create(int32_t n, const int8_t* type, const float* rate, const fl
 /* Fixed in-degree generator shared with the CUDA core's device generator:
  * projection r gives every target t of pop pr_tar[r] exactly pr_k[r]
  * sources drawn uniformly (with replacement) from pop pr_src[r]:
- *   x = Philox4x32-10(key = conn_seed, counter = (t, k, r, "CONN"))
+ *   x = Philox4x32-10(key = conn_seed, counter = (t + id_offset, k, r + proj_offset, "CONN"))
  *   src   = start[pr_src] + (x0 * num[pr_src]) >> 32
  *   delay = dmin + (x1 * (dmax - dmin + 1)) >> 32   (steps)
  * Synapse-list order: r, then t, then k. */
@@ -417,7 +418,7 @@ mgbo_sim* mgbo_create_fixed_indegree(const int32_t* pop_start, const int32_t* po
                                      const int32_t* pr_dmin, const int32_t* pr_dmax,
                                      int32_t npr, const float* rate, const float* v0,
                                      const float* lifc, uint64_t conn_seed, uint64_t seed,
-                                     int32_t nthreads)
+                                     int32_t nthreads, int32_t id_offset, int32_t proj_offset)
 {
     int32_t n = 0;
     for (int p = 0; p < npop; ++p)
@@ -429,6 +430,7 @@ mgbo_sim* mgbo_create_fixed_indegree(const int32_t* pop_start, const int32_t* po
     free(type);
     if (!s) return NULL;
     s->seed = seed;
+    s->id_offset = id_offset;
     s->stdp = 0;
     int64_t S = 0;
     int32_t dmin = 2147483647, dmax = 0;
@@ -479,7 +481,7 @@ mgbo_sim* mgbo_create_fixed_indegree(const int32_t* pop_start, const int32_t* po
                     const int32_t hi = ts + (int32_t)((int64_t)tnum * (me + 1) / T);
                     for (int32_t t = lo; t < hi; ++t)
                         for (int32_t k = 0; k < pr_k[r]; ++k) {
-                            mgb_u32x4 x = mgb_philox4x32_10((uint32_t)t, (uint32_t)k, (uint32_t)r, MGB_TAG_CONN,
+                            mgb_u32x4 x = mgb_philox4x32_10((uint32_t)(t + id_offset), (uint32_t)k, (uint32_t)(r + proj_offset), MGB_TAG_CONN,
                                                             (uint32_t)conn_seed, (uint32_t)(conn_seed >> 32));
                             int32_t src = ss + (int32_t)(((uint64_t)x.v[0] * (uint64_t)snum) >> 32);
                             if (pass == 0) {
@@ -599,6 +601,8 @@ void mgbo_destroy(mgbo_sim* s)
     free(s->csr_syn); free(s->csr_plastic); free(s->dend_off); free(s->dend_pos); free(s->spk);
     free(s);
 }
+
+void mgbo_set_id_offset(mgbo_sim* s, int32_t id_offset) { s->id_offset = id_offset; }
 
 void mgbo_set_threads(mgbo_sim* s, int32_t nthreads)
 {

@@ -109,7 +109,7 @@ mgbo_sim* mgbo_create_fixed_indegree(const int32_t* pop_start, const int32_t* po
                                      const int32_t* pr_dmin, const int32_t* pr_dmax,
                                      int32_t npr, const float* rate, const float* v0,
                                      const float* lifc, uint64_t conn_seed, uint64_t seed,
-                                     int32_t nthreads);
+                                     int32_t nthreads, int32_t id_offset, int32_t proj_offset);
 
 /* Runs `steps` steps.  counts[steps] receives the spike count of each step
  * and ids the spiking neuron ids of each step in ascending order, capacity
@@ -119,6 +119,9 @@ int mgbo_run(mgbo_sim* s, int64_t steps, int64_t* counts, int32_t* ids, int64_t 
              int64_t* n_ids);
 void mgbo_set_rates(mgbo_sim* s, const float* rate);
 void mgbo_set_threads(mgbo_sim* s, int32_t nthreads);  /* threads of later runs */
+/* Neuron ids in the POISSON draws are offset by id_offset (a block of a
+ * larger network draws as it does there). */
+void mgbo_set_id_offset(mgbo_sim* s, int32_t id_offset);
 int64_t mgbo_events(const mgbo_sim* s);      /* synaptic events delivered so far */
 int64_t mgbo_step(const mgbo_sim* s);        /* steps simulated so far */
 int32_t mgbo_ring_len(const mgbo_sim* s);    /* M = max_delay + 1 */

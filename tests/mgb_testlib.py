@@ -72,7 +72,8 @@ def oracle():
     L.mgbo_create.argtypes = [i32, vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, i32, vp, u64, i32, i32]
     L.mgbo_create_fixed_indegree.restype = vp
     L.mgbo_create_fixed_indegree.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp,
-                                             vp, u64, u64, i32]
+                                             vp, u64, u64, i32, i32, i32]
+    L.mgbo_set_id_offset.argtypes = [vp, i32]
     L.mgbo_run.restype = C.c_int
     L.mgbo_run.argtypes = [vp, i64, vp, vp, i64, C.POINTER(i64)]
     L.mgbo_set_rates.argtypes = [vp, vp]

@@ -135,7 +135,7 @@ def test_fixed_indegree_matches_oracle(mode):
             arr([r[4] for r in R], np.int32), arr([r[5] for r in R], np.int32)]
     h = L.mgbo_create_fixed_indegree(*[T._p(k) for k in keep[:3]], len(P),
                                      *[T._p(k) for k in keep[3:]], len(R), T._p(rate), T._p(v0),
-                                     T._p(lif), 77, 5, 1)
+                                     T._p(lif), 77, 5, 1, 0, 0)
     try:
         S = L.mgbo_n_syn(h)
         orp = np.zeros(n + 1, np.int64)
