@@ -443,15 +443,20 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
 // ---------------------------------------------------------------------------
 // Deferred delivery of the events that arrive at step sa: for each delay d
 // of the buckets, the spikes of step sa-d send the delay-d segment of their
-// row into the accumulator of step sa.  Task f enumerates (d, spike,
-// 128-synapse chunk) through a prefix sum over the per-delay spike counts
-// held in shared memory.
+// row into the accumulator of step sa.  Task f enumerates (d, spike)
+// through a prefix sum over the per-delay spike counts held in shared
+// memory.  A warp takes 32 tasks at once: each lane fetches one segment
+// header, a warp scan lays the 32 segments end to end, and the lanes then
+// stride over the concatenated synapses (owner segment found by a 5-step
+// shuffle search), so all synapse loads of the batch are independent and
+// in flight together instead of one dependent chain per segment.
 // ---------------------------------------------------------------------------
+constexpr int kDeliverUnroll = 4;
+
 __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
                                                  int64_t nwarps)
 {
     const int D = a.D;
-    const int CH = a.bucket_chunks;
     // history slot of step sa: the current slot advanced by (sa - s)
     int32_t hs = a.slots[1] + (int32_t)(sa - *a.step);
     if (hs >= a.H) hs -= a.H;
@@ -465,7 +470,7 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
             if (k < D && sa - (a.dmin + k) >= 0) {
                 int32_t h = hs - (a.dmin + k);  // slot of step sa - d, d < H
                 if (h < 0) h += a.H;
-                c = (int64_t)a.hist_cnt[h] * CH;
+                c = (int64_t)a.hist_cnt[h];
             }
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -480,46 +485,60 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
     const int64_t total = pre[D];
     float* acc_e = acc_buf(a, a.acc_e, sa);
     float* acc_i = acc_buf(a, a.acc_i, sa);
-    // Lane groups of G lanes each take one task (a chunk of G*4 synapses of
-    // one bucket), so a warp keeps 32/G independent chains in flight.
-    const int G = a.task_lanes;
-    const int per_warp = 32 / G;
     const int lane = threadIdx.x & 31;
-    const int gi = lane / G, li = lane - gi * G;
-    const int span = G * 4;
     unsigned long long ev = 0;
-    for (int64_t fb = warp * per_warp; fb < total; fb += nwarps * per_warp) {
-        const int64_t f = fb + gi;
-        if (f >= total) continue;
-        int lo = 0, hi = D - 1;  // last k with pre[k] <= f
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+    for (int64_t fb = warp * 32; fb < total; fb += nwarps * 32) {
+        // 1. this lane's segment header
+        const int64_t f = fb + lane;
+        int64_t b = 0;
+        int32_t len = 0;
+        if (f < total) {
+            int lo = 0, hi = D - 1;  // last k with pre[k] <= f
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+            }
+            const int k = lo;
+            const int32_t j = (int32_t)(f - pre[k]);
+            int32_t h = hs - (a.dmin + k);
+            if (h < 0) h += a.H;
+            const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
+            const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
+            b = __ldg(bk);
+            len = (int32_t)(__ldg(bk + 1) - b);
         }
-        const int k = lo;
-        const int64_t local = f - pre[k];
-        const int32_t j = (int32_t)(local / CH);
-        const int32_t c = (int32_t)(local - (int64_t)j * CH);
-        int32_t h = hs - (a.dmin + k);
-        if (h < 0) h += a.H;
-        const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
-        const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
-        const int64_t sb = __ldg(bk), se = __ldg(bk + 1);
-        const int64_t b = sb + (int64_t)c * span;
-        if (b >= se) continue;
-        const int64_t e = min(se, b + (int64_t)span);
-        if (li == 0) ev += (unsigned long long)(e - b);
-        uint2 w[4];
+        // 2. segments end to end: exclusive offsets
+        int32_t incl = len;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int64_t q = b + li + G * u;
-            w[u] = q < e ? __ldcs(a.syn + q) : make_uint2(0u, 0u);
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
         }
+        const int32_t excl = incl - len;
+        const int32_t tot = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane == 0) ev += (unsigned long long)tot;
+        // 3. all lanes over the concatenated synapses
+        for (int32_t base = 0; base < tot; base += 32 * kDeliverUnroll) {
+            uint2 w[kDeliverUnroll];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            if (b + li + G * u >= e) continue;
-            const float wt = as_f(w[u].y);
-            atomicAdd((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
+            for (int u = 0; u < kDeliverUnroll; ++u) {
+                const int32_t idx = base + u * 32 + lane;
+                int L = 0;  // last lane whose segment starts at or before idx
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1) {
+                    const int32_t e = __shfl_sync(0xffffffffu, excl, L + st);
+                    if (e <= idx) L += st;
+                }
+                const int64_t bl = __shfl_sync(0xffffffffu, b, L);
+                const int32_t el = __shfl_sync(0xffffffffu, excl, L);
+                w[u] = idx < tot ? __ldcs(a.syn + bl + (idx - el)) : make_uint2(0u, 0u);
+            }
+#pragma unroll
+            for (int u = 0; u < kDeliverUnroll; ++u) {
+                if (base + u * 32 + lane >= tot) continue;
+                const float wt = as_f(w[u].y);
+                atomicAdd((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
+            }
         }
     }
     if (ev) atomicAdd(a.events, ev);
@@ -539,7 +558,7 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 // its share of them into the other accumulator buffer and then updates its
 // share of the neurons for step s; the two memory-latency chains of
 // different warps overlap on each SM.
-__global__ void __launch_bounds__(kPushBlock, 6) k_fused(StepArgs a)
+__global__ void __launch_bounds__(kPushBlock, 5) k_fused(StepArgs a)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
     const int64_t s = *a.step;
