@@ -184,9 +184,10 @@ mgc_status mgc_export_csr(mgc_sim* sim, int64_t* row_ptr, int32_t* tgt, float* w
 
 mgc_status mgc_get_info(mgc_sim* sim, mgc_info* info);
 
-/* Runs `steps` steps without graphs, timing each kernel class with CUDA
- * events on the handle's stream: ms[0] neuron update, ms[1] event push,
- * ms[2] STDP, summed over the steps.  No reference counterpart (the
+/* Runs `steps` steps with each kernel class bracketed by CUDA events (the
+ * steps and their event records are captured in batches of 64 as CUDA
+ * graphs, so the kernels run back to back as in mgc_run): ms[0] neuron
+ * update, ms[1] event delivery, ms[2] STDP, summed over the steps.  No reference counterpart (the
  * reference was profiled externally with nvprof, shell/single.sh:15). */
 mgc_status mgc_profile_steps(mgc_sim* sim, int64_t steps, float* ms);
 

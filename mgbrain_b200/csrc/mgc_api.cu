@@ -1063,18 +1063,25 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
     for (auto& e : ev) CK(cudaEventCreate(&e));
     double acc[3] = {0, 0, 0};
     mgc_status st = MGC_OK;
+    if (s->a.deferred && s->fused && !s->ahead) {
+        k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
+        s->ahead = true;
+    }
+    // Each batch of steps is captured with its event records as one CUDA
+    // graph and replayed, so kernels run back to back and the events time
+    // the GPU, not the host's launch rate.
     for (int64_t done = 0; done < steps && st == MGC_OK;) {
         const int b = (int)std::min<int64_t>(kBatch, steps - done);
+        if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            st = fail(MGC_ERR_CUDA, "profile: stream capture failed");
+            break;
+        }
         for (int i = 0; i < b; ++i) {
             cudaEvent_t* e = &ev[4 * i];
             // ms[0] neuron update, ms[1] event delivery (push or deferred), ms[2] STDP
             if (s->a.deferred && s->fused) {
                 // the fused step timed as its two parts: neuron update of
                 // step s, then delivery of the arrivals of step s+1
-                if (!s->ahead) {
-                    k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
-                    s->ahead = true;
-                }
                 cudaEventRecord(e[0], s->stream);
                 k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
                 cudaEventRecord(e[1], s->stream);
@@ -1103,7 +1110,14 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             }
             s->launches += s->a.deferred ? 2 : kernels_per_step(s);
         }
-        cudaError_t err = cudaStreamSynchronize(s->stream);
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        cudaError_t err = cudaStreamEndCapture(s->stream, &g);
+        if (err == cudaSuccess) err = cudaGraphInstantiate(&ge, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (err == cudaSuccess) err = cudaGraphLaunch(ge, s->stream);
+        if (err == cudaSuccess) err = cudaStreamSynchronize(s->stream);
+        if (ge) cudaGraphExecDestroy(ge);
         if (err != cudaSuccess) {
             st = fail(MGC_ERR_CUDA, "profile: %s", cudaGetErrorString(err));
             break;
