@@ -1062,6 +1062,9 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
     std::vector<cudaEvent_t> ev(4 * kBatch);
     for (auto& e : ev) CK(cudaEventCreate(&e));
     double acc[3] = {0, 0, 0};
+    // External records become event-record nodes of the captured graph (a
+    // plain record inside a capture only orders the capture's streams).
+    auto rec = [&](cudaEvent_t ev_) { cudaEventRecordWithFlags(ev_, s->stream, cudaEventRecordExternal); };
     mgc_status st = MGC_OK;
     if (s->a.deferred && s->fused && !s->ahead) {
         k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
@@ -1082,31 +1085,31 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             if (s->a.deferred && s->fused) {
                 // the fused step timed as its two parts: neuron update of
                 // step s, then delivery of the arrivals of step s+1
-                cudaEventRecord(e[0], s->stream);
+                rec(e[0]);
                 k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[1], s->stream);
+                rec(e[1]);
                 k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[2], s->stream);
-                cudaEventRecord(e[3], s->stream);
+                rec(e[2]);
+                rec(e[3]);
             } else if (s->a.deferred) {
-                cudaEventRecord(e[0], s->stream);
+                rec(e[0]);
                 k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[1], s->stream);
+                rec(e[1]);
                 k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[2], s->stream);
-                cudaEventRecord(e[3], s->stream);
+                rec(e[2]);
+                rec(e[3]);
             } else {
-                cudaEventRecord(e[0], s->stream);
+                rec(e[0]);
                 k_neuron<<<s->neuron_grid, kNeuronBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[1], s->stream);
+                rec(e[1]);
                 if (s->a.pull) {
                     k_pull<<<s->pull_grid, kPushBlock, 0, s->stream>>>(s->a);  // delivery + STDP
                 } else {
                     k_push<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
                 }
-                cudaEventRecord(e[2], s->stream);
+                rec(e[2]);
                 if (s->stdp && !s->a.pull) k_stdp<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
-                cudaEventRecord(e[3], s->stream);
+                rec(e[3]);
             }
             s->launches += s->a.deferred ? 2 : kernels_per_step(s);
         }
@@ -1123,11 +1126,15 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             break;
         }
         for (int i = 0; i < b; ++i) {
-            float t0, t1, t2;
+            float t0 = 0, t1 = 0, t2 = 0;
             cudaEvent_t* e = &ev[4 * i];
-            cudaEventElapsedTime(&t0, e[0], e[1]);
-            cudaEventElapsedTime(&t1, e[1], e[2]);
-            cudaEventElapsedTime(&t2, e[2], e[3]);
+            err = cudaEventElapsedTime(&t0, e[0], e[1]);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&t1, e[1], e[2]);
+            if (err == cudaSuccess) err = cudaEventElapsedTime(&t2, e[2], e[3]);
+            if (err != cudaSuccess) {
+                st = fail(MGC_ERR_CUDA, "profile: event time: %s", cudaGetErrorString(err));
+                break;
+            }
             if (s->a.deferred && s->fused) {
                 acc[0] += t0;
                 acc[1] += t1;
