@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
 // of the buckets, the spikes of step sa-d send the delay-d segment of their
 // row into the accumulator of step sa.  Task f enumerates (d, spike)
 // through a prefix sum over the per-delay spike counts held in shared
-// memory.  A warp takes 32 tasks at once: each lane fetches one segment
+// memory.  A warp takes up to 32 tasks at once: each lane fetches one segment
 // header, a warp scan lays the 32 segments end to end, and the lanes then
 // stride over the concatenated synapses (owner segment found by a 5-step
 // shuffle search), so all synapse loads of the batch are independent and
@@ -453,46 +453,61 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
 // ---------------------------------------------------------------------------
 constexpr int kDeliverUnroll = 4;
 
-__device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
-                                                 int64_t nwarps)
+// History slot of step sa: the current slot advanced by (sa - s).
+__device__ __forceinline__ int32_t hist_slot(const StepArgs& a, int64_t sa)
+{
+    int32_t hs = a.slots[1] + (int32_t)(sa - *a.step);
+    return hs >= a.H ? hs - a.H : hs;
+}
+
+// pre[k] = spikes of the delays before bucket k that arrive at step sa
+// (pre[D] = tasks in all); run by the block's first warp.
+__device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, int64_t* pre)
 {
     const int D = a.D;
-    // history slot of step sa: the current slot advanced by (sa - s)
-    int32_t hs = a.slots[1] + (int32_t)(sa - *a.step);
-    if (hs >= a.H) hs -= a.H;
-    if (threadIdx.x < 32) {
-        int64_t carry = 0;
-        const int lane = threadIdx.x;
-        if (lane == 0) pre[0] = 0;
-        for (int base = 0; base < D; base += 32) {
-            const int k = base + lane;
-            int64_t c = 0;
-            if (k < D && sa - (a.dmin + k) >= 0) {
-                int32_t h = hs - (a.dmin + k);  // slot of step sa - d, d < H
-                if (h < 0) h += a.H;
-                c = (int64_t)a.hist_cnt[h];
-            }
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int64_t v = __shfl_up_sync(0xffffffffu, c, o);
-                if (lane >= o) c += v;
-            }
-            if (k < D) pre[k + 1] = carry + c;
-            carry += __shfl_sync(0xffffffffu, c, 31);
+    const int32_t hs = hist_slot(a, sa);
+    const int lane = threadIdx.x;
+    int64_t carry = 0;
+    if (lane == 0) pre[0] = 0;
+    for (int base = 0; base < D; base += 32) {
+        const int k = base + lane;
+        int64_t c = 0;
+        if (k < D && sa - (a.dmin + k) >= 0) {
+            int32_t h = hs - (a.dmin + k);  // slot of step sa - d, d < H
+            if (h < 0) h += a.H;
+            c = (int64_t)a.hist_cnt[h];
         }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t v = __shfl_up_sync(0xffffffffu, c, o);
+            if (lane >= o) c += v;
+        }
+        if (k < D) pre[k + 1] = carry + c;
+        carry += __shfl_sync(0xffffffffu, c, 31);
     }
-    __syncthreads();
+}
+
+// The tasks themselves, after deliver_prefix and a block barrier.
+__device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, const int64_t* pre, int64_t warp,
+                                              int64_t nwarps)
+{
+    const int D = a.D;
+    const int32_t hs = hist_slot(a, sa);
     const int64_t total = pre[D];
     float* acc_e = acc_buf(a, a.acc_e, sa);
     float* acc_i = acc_buf(a, a.acc_i, sa);
     const int lane = threadIdx.x & 31;
     unsigned long long ev = 0;
-    for (int64_t fb = warp * 32; fb < total; fb += nwarps * 32) {
+    // tasks per warp: 32, or fewer when the grid has more lanes than tasks,
+    // so that a small step spreads over all warps instead of a few
+    const int64_t need = (total + nwarps - 1) / nwarps;
+    const int per = need >= 32 ? 32 : (need < 1 ? 1 : (int)need);
+    for (int64_t fb = warp * per; fb < total; fb += nwarps * per) {
         // 1. this lane's segment header
         const int64_t f = fb + lane;
         int64_t b = 0;
         int32_t len = 0;
-        if (f < total) {
+        if (lane < per && f < total) {
             int lo = 0, hi = D - 1;  // last k with pre[k] <= f
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -544,6 +559,14 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
     if (ev) atomicAdd(a.events, ev);
 }
 
+__device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
+                                                 int64_t nwarps)
+{
+    if (threadIdx.x < 32) deliver_prefix(a, sa, pre);
+    __syncthreads();
+    deliver_tasks(a, sa, pre, warp, nwarps);
+}
+
 // Arrivals of the current step (used when the minimum delay is one step).
 __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 {
@@ -554,9 +577,9 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 }
 
 // One launch per step when the minimum delay is >= 2: the arrivals of step
-// s+1 depend only on spikes of steps <= s-1, so every warp first delivers
-// its share of them into the other accumulator buffer and then updates its
-// share of the neurons for step s; the two memory-latency chains of
+// s+1 depend only on spikes of steps <= s-1, so every warp updates its
+// share of the neurons for step s and then delivers its share of those
+// arrivals into the other accumulator buffer; the memory-latency chains of
 // different warps overlap on each SM.
 __global__ void __launch_bounds__(kPushBlock, 5) k_fused(StepArgs a)
 {
@@ -564,8 +587,12 @@ __global__ void __launch_bounds__(kPushBlock, 5) k_fused(StepArgs a)
     const int64_t s = *a.step;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    deliver_arrivals(a, s + 1, pre, warp, nwarps);
+    // the first warp sums the spike counts per delay while all warps update
+    // their neurons; the barrier then publishes the sums for the delivery
+    if (threadIdx.x < 32) deliver_prefix(a, s + 1, pre);
     neuron_groups(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
+    __syncthreads();
+    deliver_tasks(a, s + 1, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);
 }
 

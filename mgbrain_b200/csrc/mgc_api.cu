@@ -1144,7 +1144,7 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
             } else {
                 acc[0] += t0;
                 acc[1] += t1;
-                acc[2] += t2;
+                if (s->stdp && !s->a.pull) acc[2] += t2;  // else no kernel between e[2] and e[3]
             }
         }
         done += b;
@@ -1175,3 +1175,4 @@ const char* mgc_last_error(void) { return g_last_error.c_str(); }
 int64_t mgc_kernel_launches(mgc_sim* s) { return s ? s->launches : 0; }
 
 }  // extern "C"
+

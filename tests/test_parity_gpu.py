@@ -59,7 +59,14 @@ def test_cuda_matches_oracle(name, mode):
         np.testing.assert_allclose(w, ost["weight32"], rtol=W_RTOL, atol=1e-9)
         np.testing.assert_allclose(gst["V"], ost["V32"], rtol=W_RTOL, atol=1e-8)
     else:
-        assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
+        wt = net["weight"]
+        if len(np.unique(wt[wt > 0])) <= 1 and len(np.unique(wt[wt <= 0])) <= 1:
+            # one weight per sign: every order of the fp32 input sums gives the same bits
+            assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
+        else:
+            # unequal weights of one sign: fp32 sums depend on the arrival order,
+            # which atomics (here and in the reference) leave open
+            np.testing.assert_allclose(gst["V"], ost["V32"], rtol=W_RTOL, atol=1e-8)
         assert np.array_equal(w, net["weight"])
     if gsim.info()["mode"] in (mgb.MODE_PUSH, mgb.MODE_PULL):
         assert gsim.info()["events"] == osim.events  # counted at emission
