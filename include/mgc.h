@@ -210,6 +210,32 @@ const char* mgc_last_error(void);
 /* Kernels this library launched on this handle so far. */
 int64_t mgc_kernel_launches(mgc_sim* sim);
 
+/* CSR row offsets of a synapse list held in DEVICE memory, computed without
+ * allocating anything: row_ptr[i] = synapses whose source is below i, for
+ * i = 0..n_neurons (row_ptr[n_neurons] = n_synapses) — the row_ptr that
+ * mgc_create builds and mgc_export_csr returns for the same list.  src
+ * (n_synapses int32) and row_ptr (n_neurons+1 int64) are device pointers on
+ * the current device; the work is enqueued on `stream` (a cudaStream_t, NULL
+ * for the legacy default stream) and the call waits for it before returning.
+ *
+ * For callers that cannot allocate device memory at this point: a caller whose
+ * memory pool owns the device (cudaMalloc can fail there although the pool
+ * has room), or a loop that rebuilds offsets while the simulation runs (every
+ * cudaFree synchronises the whole device).  mgc_create's own scan takes its
+ * scratch from cudaMalloc; this entry point uses a fixed 256 KB static device
+ * array instead, which limits it to n_neurons <= 134,217,727 (larger sizes
+ * return MGC_ERR_INVALID with the limit in mgc_last_error).  row_ptr needs no
+ * initial contents (the call zeroes it and its own counters).  The first call
+ * on a device does a one-time set-up (it looks up the scratch array's address,
+ * cudaGetSymbolAddress), so make that first call before any stream capture
+ * begins.  All calls on one device share the one scratch array, so calls that
+ * overlapped would race on it; the library serialises them with a lock per
+ * device.  Sources outside [0, n_neurons) are skipped and reported as
+ * MGC_ERR_INVALID.  No reference counterpart (the reference computes its row
+ * offsets, axon_offs, on the host: src/simulator/mgsim/adj/mgsim.cpp:115-122). */
+mgc_status mgc_row_offsets_static(const int32_t* src, int64_t n_synapses, int32_t n_neurons, int64_t* row_ptr,
+                                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,7 +21,7 @@ EXPORTED = (
     "mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
-    "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch",
+    "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
 )
 
 
@@ -98,6 +98,8 @@ def lib():
     L.mgc_last_error.restype = C.c_char_p
     L.mgc_kernel_launches.argtypes = [vp]
     L.mgc_kernel_launches.restype = i64
+    L.mgc_row_offsets_static.argtypes = [vp, i64, i32, vp, vp]
+    L.mgc_row_offsets_static.restype = C.c_int
     for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_create_batch", "mgc_run", "mgc_sync", "mgc_set_rates",
                  "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
                  "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
