@@ -210,6 +210,17 @@ const char* mgc_last_error(void);
 /* Kernels this library launched on this handle so far. */
 int64_t mgc_kernel_launches(mgc_sim* sim);
 
+/* Measures the two ceilings of event delivery on `device`: n_events scattered
+ * fp32 reductions (one per event, into n_targets accumulators, each fed by an
+ * 8-byte {target, weight} record streamed from device memory, the access
+ * pattern of the delivery kernels) and a plain stream of the same records.
+ * Records are generated on the device; best of `reps` timed runs after one
+ * warm-up, with CUDA events.  Allocates n_events*8 + n_targets*4 bytes for
+ * the call.  No reference counterpart (it measures the bound of the
+ * reference's event push, mgcore.cu:271-305, whose atomics set its rate). */
+mgc_status mgc_measure_scatter(int32_t device, int64_t n_events, int32_t n_targets, int32_t reps,
+                               double* red_events_per_s, double* read_bytes_per_s);
+
 /* CSR row offsets of a synapse list held in DEVICE memory, computed without
  * allocating anything: row_ptr[i] = synapses whose source is below i, for
  * i = 0..n_neurons (row_ptr[n_neurons] = n_synapses) — the row_ptr that

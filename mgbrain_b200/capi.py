@@ -22,6 +22,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
+    "mgc_measure_scatter",
 )
 
 
@@ -100,6 +101,8 @@ def lib():
     L.mgc_kernel_launches.restype = i64
     L.mgc_row_offsets_static.argtypes = [vp, i64, i32, vp, vp]
     L.mgc_row_offsets_static.restype = C.c_int
+    L.mgc_measure_scatter.argtypes = [i32, i64, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.mgc_measure_scatter.restype = C.c_int
     for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_create_batch", "mgc_run", "mgc_sync", "mgc_set_rates",
                  "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
                  "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
@@ -115,6 +118,14 @@ def check(status):
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def measure_scatter(device=0, n_events=100_000_000, n_targets=1 << 20, reps=3):
+    """(reductions/s, read bytes/s): the delivery ceilings of this device."""
+    red, rd = C.c_double(), C.c_double()
+    check(lib().mgc_measure_scatter(int(device), int(n_events), int(n_targets), int(reps), C.byref(red),
+                                    C.byref(rd)))
+    return red.value, rd.value
 
 
 def effective_steps(steps, min_delay):

@@ -109,6 +109,14 @@ struct StepArgs {
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
+
+// Fire-and-forget fp32 reduction into global memory (PTX red.add.f32: the
+// same rounding and subnormal flushing as atomicAdd, but no value comes back,
+// so the issuing warp never waits on it).
+__device__ __forceinline__ void red_add(float* p, float v)
+{
+    asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
 __device__ __forceinline__ uint32_t as_u(float f) { return __float_as_uint(f); }
 
 // ---------------------------------------------------------------------------
@@ -244,66 +252,95 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
     return fired;
 }
 
-// Updates neuron groups [first warp group .. ) with a warp-strided loop;
-// `warp`/`nwarps` index the warps taking part.  Input of this step is read
-// from (and cleared in) in_e/in_i, which point at the ring slot or the
-// accumulator buffer.
+// Updates the neuron groups with a warp-strided loop; `warp`/`nwarps` index
+// the warps taking part.  Each lane takes G groups per pass (groups
+// gb + h*32 + lane, h < G), all of whose loads are issued before the first
+// update, so a warp waits for memory once per pass.  Input of this step is
+// read from (and cleared in) in_e/in_i, which point at the ring slot or the
+// accumulator buffer.  Spiking ids are compacted in neuron order within the
+// pass, one atomic per warp.
+template <int G>
 __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
                                               int64_t warp, int64_t nwarps)
 {
+    static_assert(G == 1 || G == 2, "one or two groups per lane");
     const int lane = threadIdx.x & 31;
     const int64_t ngroups = a.ns >> 2;
     int32_t* ids = step_ids(a, hslot);
     int32_t* cnt = step_count(a, hslot);
     const bool rec = (a.deferred || a.pull) && a.record;  // no push kernel to record
     const int64_t rbase = rec ? *a.raster_pos : 0;
-    for (int64_t gb = warp * 32; gb < ngroups; gb += nwarps * 32) {
-        const int64_t g = gb + lane;
-        unsigned fmask = 0;
-        if (g < ngroups) {
-            const char4 t4 = __ldg(reinterpret_cast<const char4*>(a.type) + g);
-            float4 v4 = reinterpret_cast<float4*>(a.V)[g];
-            int4 r4 = reinterpret_cast<int4*>(a.refrac)[g];
-            const float4 e4 = reinterpret_cast<float4*>(in_e)[g];
-            const float4 i4 = reinterpret_cast<float4*>(in_i)[g];
-            reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-            reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-            const int32_t i0 = (int32_t)(g << 2);
-            fmask |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e4.x, i4.x) ? 1u : 0u;
-            fmask |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e4.y, i4.y) ? 2u : 0u;
-            fmask |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e4.z, i4.z) ? 4u : 0u;
-            fmask |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e4.w, i4.w) ? 8u : 0u;
-            reinterpret_cast<float4*>(a.V)[g] = v4;
-            reinterpret_cast<int4*>(a.refrac)[g] = r4;
+    for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
+        char4 t4[G];
+        float4 v4[G], e4[G], i4[G];
+        int4 r4[G];
+#pragma unroll
+        for (int h = 0; h < G; ++h) {
+            const int64_t g = gb + h * 32 + lane;
+            if (g < ngroups) {
+                t4[h] = __ldg(reinterpret_cast<const char4*>(a.type) + g);
+                v4[h] = reinterpret_cast<float4*>(a.V)[g];
+                r4[h] = reinterpret_cast<int4*>(a.refrac)[g];
+                e4[h] = reinterpret_cast<float4*>(in_e)[g];
+                i4[h] = reinterpret_cast<float4*>(in_i)[g];
+                reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
         }
-        if (a.pull) {
-            // bitmap of this step's spikes: 8 lanes (32 neurons) per word
-            unsigned wv = fmask << (4 * (lane & 7));
-            wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
-            wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
-            wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
-            if ((lane & 7) == 0) a.fired_bits[(gb >> 3) + (lane >> 3)] = wv;
+        unsigned fmask[G];
+#pragma unroll
+        for (int h = 0; h < G; ++h) {
+            const int64_t g = gb + h * 32 + lane;
+            fmask[h] = 0;
+            if (g < ngroups) {
+                const int32_t i0 = (int32_t)(g << 2);
+                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x) ? 1u : 0u;
+                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y) ? 2u : 0u;
+                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z) ? 4u : 0u;
+                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w) ? 8u : 0u;
+                reinterpret_cast<float4*>(a.V)[g] = v4[h];
+                reinterpret_cast<int4*>(a.refrac)[g] = r4[h];
+            }
+            if (a.pull) {
+                // bitmap of this step's spikes: 8 lanes (32 neurons) per word
+                unsigned wv = fmask[h] << (4 * (lane & 7));
+                wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
+                wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
+                wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
+                if ((lane & 7) == 0 && gb + h * 32 < ngroups) a.fired_bits[((gb + h * 32) >> 3) + (lane >> 3)] = wv;
+            }
         }
-        // compaction in neuron order: warp-inclusive scan of spike counts
-        const int c = __popc(fmask);
+        // compaction in neuron order: one warp scan of the per-pass counts
+        // (pass h in bits 8h.., at most 128 spikes each)
+        int c = 0;
+#pragma unroll
+        for (int h = 0; h < G; ++h) c |= __popc(fmask[h]) << (8 * h);
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += v;
         }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const int packed = __shfl_sync(0xffffffffu, incl, 31);
+        int total = 0;
+#pragma unroll
+        for (int h = 0; h < G; ++h) total += (packed >> (8 * h)) & 0xff;
         if (total) {
             int32_t base = 0;
             if (lane == 31) base = atomicAdd(cnt, total);
             base = __shfl_sync(0xffffffffu, base, 31);
-            int32_t pos = base + incl - c;
-            const int32_t i0 = (int32_t)(g << 2);
-            for (int k = 0; k < 4; ++k) {
-                if (fmask & (1u << k)) {
-                    ids[pos] = i0 + k;
-                    if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
-                    ++pos;
+#pragma unroll
+            for (int h = 0; h < G; ++h) {
+                const int ch = (c >> (8 * h)) & 0xff;
+                int32_t pos = base + ((incl >> (8 * h)) & 0xff) - ch;
+                base += (packed >> (8 * h)) & 0xff;
+                const int32_t i0 = (int32_t)((gb + h * 32 + lane) << 2);
+                for (int k = 0; k < 4; ++k) {
+                    if (fmask[h] & (1u << k)) {
+                        ids[pos] = i0 + k;
+                        if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
+                        ++pos;
+                    }
                 }
             }
         }
@@ -329,7 +366,7 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
     }
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    neuron_groups(a, s, hslot, in_e, in_i, warp, nwarps);
+    neuron_groups<1>(a, s, hslot, in_e, in_i, warp, nwarps);
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
@@ -502,7 +539,10 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, con
     // so that a small step spreads over all warps instead of a few
     const int64_t need = (total + nwarps - 1) / nwarps;
     const int per = need >= 32 ? 32 : (need < 1 ? 1 : (int)need);
-    for (int64_t fb = warp * per; fb < total; fb += nwarps * per) {
+    // tasks start at the last warp: the neuron update gives the first warps
+    // its extra passes, so a step with few tasks lands on the least busy ones
+    const int64_t rw = nwarps - 1 - warp;
+    for (int64_t fb = rw * per; fb < total; fb += nwarps * per) {
         // 1. this lane's segment header
         const int64_t f = fb + lane;
         int64_t b = 0;
@@ -552,7 +592,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, con
             for (int u = 0; u < kDeliverUnroll; ++u) {
                 if (base + u * 32 + lane >= tot) continue;
                 const float wt = as_f(w[u].y);
-                atomicAdd((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
+                red_add((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
             }
         }
     }
@@ -581,7 +621,7 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 // share of the neurons for step s and then delivers its share of those
 // arrivals into the other accumulator buffer; the memory-latency chains of
 // different warps overlap on each SM.
-__global__ void __launch_bounds__(kPushBlock, 5) k_fused(StepArgs a)
+__global__ void __launch_bounds__(kPushBlock, 3) k_fused(StepArgs a)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
     const int64_t s = *a.step;
@@ -590,7 +630,7 @@ __global__ void __launch_bounds__(kPushBlock, 5) k_fused(StepArgs a)
     // the first warp sums the spike counts per delay while all warps update
     // their neurons; the barrier then publishes the sums for the delivery
     if (threadIdx.x < 32) deliver_prefix(a, s + 1, pre);
-    neuron_groups(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
+    neuron_groups<2>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
     __syncthreads();
     deliver_tasks(a, s + 1, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);
@@ -636,7 +676,7 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
             if (slot >= a.M) slot -= a.M;
             const float wt = as_f(w[u].y);
             float* ring = wt > 0.0f ? a.ring_e : a.ring_i;
-            atomicAdd(ring + (size_t)slot * (size_t)a.ns + tgt, wt);
+            red_add(ring + (size_t)slot * (size_t)a.ns + tgt, wt);
         }
     }
     if (lane == 0 && ev) atomicAdd(a.events, ev);
