@@ -291,6 +291,7 @@ def run_ours(a, ws, rank, local):
     sim = make_sim(w, local, seed=1 + rank, record=False)
     build_s = time.perf_counter() - t0
     info = sim.info()
+    tune = sim.autotune(steps_per_trial=640)   # launch shape by measurement
     for _ in range(a.warmup):
         sim.run(CHUNK)
     sim.sync()
@@ -376,6 +377,7 @@ def run_ours(a, ws, rank, local):
     if not a.no_driven:
         wd = workload(a.scale, nu=NU_DRIVEN)
         simd = make_sim(wd, local, seed=1 + rank, record=False)
+        simd.autotune(steps_per_trial=640)
         simd.run(CHUNK // 2)
         simd.sync()
         dms, dev, _ = timed_device(simd, CHUNK, 1, ws)
@@ -417,11 +419,102 @@ def run_ours(a, ws, rank, local):
             "events_per_step": ev_all / (a.steps * CHUNK * ws),
             "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
             "clocks": clk.summary(), "gpu_launches": int(launches),
-            "build_s": build_s, "driven_variant": driven,
+            "build_s": build_s, "autotune": tune, "driven_variant": driven,
             "delivery_ceiling": {"reductions_per_s": red_ceiling, "stream_read_gbs": read_ceiling / 1e9,
                                  "how": "mgc_measure_scatter: 1e8 random fp32 red.add into 2^20 "
                                         "accumulators fed by streamed 8-byte records; plain stream "
                                         "of the same records"},
+        }
+        print(json.dumps(line), flush=True)
+
+
+def split_raster(counts, ids, starts, steps):
+    """Per-instance rasters (ids relative to the instance) from a batch raster."""
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    step_of = np.repeat(np.arange(len(counts)), counts)
+    inst = np.searchsorted(starts, ids, side="right") - 1
+    out = []
+    for i in range(len(starts) - 1):
+        m = inst == i
+        c = np.bincount(step_of[m], minlength=steps)[:steps]
+        out.append((c, ids[m] - starts[i]))
+    return out
+
+
+def run_sweep(a, ws, rank, local):
+    """Parameter sweep of independent Brunel instances (N log-uniform in
+    [1e3, 1e5], K = min(N/10, 1000), g ~ U[3, 7], nu_ext ~ U[10, 30] Hz).
+    Batched form: all of this rank's instances in one handle, one kernel per
+    step for all of them.  Plain form: each instance in its own handle, run
+    one after the other for the same steps.  Rasters of the two forms are
+    compared instance by instance.  Instances are dealt to ranks round-robin
+    (weak scaling: no collective on the data path)."""
+    import torch
+
+    import mgbrain_b200 as mgb
+    from mgbrain_b200 import brunel
+    torch.cuda.set_device(local)
+    insts = brunel.sweep_instances(count=a.sweep_count)
+    mine = [p for i, p in enumerate(insts) if i % ws == rank]
+    T = a.sweep_steps
+    n_all = sum(brunel.sweep_block(p)["n"] for p in mine)
+    steps_cap = T + 4096                     # also holds the autotuner's trial steps
+    cap = lambda n: max(4096, n * steps_cap // 200)  # room for a mean rate of 50 Hz
+    raster = dict(raster_steps=steps_cap)
+    t0 = time.perf_counter()
+    sim, starts = brunel.sweep_batch(mine, seed=1, raster_ids=cap(n_all), **raster)
+    build_s = time.perf_counter() - t0
+    info = sim.info()
+    tune = sim.autotune(steps_per_trial=64)
+    sim.read_raster(max_steps=steps_cap, max_ids=cap(n_all))  # drops the trial steps
+    for _ in range(a.warmup):
+        sim.run(T)
+        sim.read_raster(max_steps=T, max_ids=cap(n_all))
+    with ClockSampler(local) as clk:
+        ms, events, launches = timed_device(sim, T, 1, ws)
+    _, counts, ids = sim.read_raster(max_steps=T, max_ids=cap(n_all))
+    per_inst = split_raster(counts, ids, starts, T)
+    sim.close()
+    batch_ev_s = allsum(ws, events) / (allmax(ws, ms) / 1e3)
+
+    plain_ms = plain_events = 0.0
+    plain_launches = 0
+    same = 0
+    for i in range(len(mine)):
+        alone_n = brunel.sweep_block(mine[i])["n"]
+        alone = brunel.sweep_alone(mine, i, seed=1, raster_ids=cap(alone_n), **raster)
+        alone.run(tune["steps"])  # the steps the batch spent in its autotuner
+        alone.read_raster(max_steps=steps_cap, max_ids=cap(alone_n))
+        for _ in range(a.warmup):
+            alone.run(T)
+            alone.read_raster(max_steps=T, max_ids=cap(alone_n))
+        m_i, e_i, l_i = timed_device(alone, T, 1, 1)
+        _, ca, ia = alone.read_raster(max_steps=T, max_ids=cap(alone_n))
+        alone.close()
+        plain_ms += m_i
+        plain_events += e_i
+        plain_launches += l_i
+        cb, ib = per_inst[i]
+        same += int(np.array_equal(cb, ca) and np.array_equal(ib, ia))
+    plain_ev_s = allsum(ws, plain_events) / (allmax(ws, plain_ms) / 1e3)
+    same = int(allsum(ws, same))
+    if rank == 0:
+        line = {
+            "metric": "aggregate synaptic events/s on the parameter sweep, batched vs plain",
+            "value": batch_ev_s, "unit": "events/s", "n_gpus": ws, "steps": T, "warmup": a.warmup,
+            "higher_is_better": True, "scaling": "weak", "dtype": "f32",
+            "data": "synthetic (seeded, generated on the device)",
+            "config": {"workload": f"{a.sweep_count} Brunel instances, N log-uniform [1e3, 1e5], "
+                                   "K = min(N/10, 1000) (80/20) + K/10 external, g ~ U[3, 7], "
+                                   "nu_ext ~ U[10, 30] Hz, delay 1.5 ms, dt 0.1 ms",
+                       "instances_per_gpu": len(mine), "neurons_gpu0": info["n_neurons"],
+                       "synapses_gpu0": info["n_synapses"], "steps_per_form": T},
+            "batched": {"events_per_s": batch_ev_s, "ms": ms, "kernel_launches": launches,
+                        "build_s": build_s, "autotune": tune},
+            "plain": {"events_per_s": plain_ev_s, "ms": plain_ms, "kernel_launches": plain_launches},
+            "batched_over_plain": batch_ev_s / plain_ev_s if plain_ev_s else None,
+            "rasters_identical": f"{same}/{a.sweep_count}",
+            "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
 
@@ -438,13 +531,20 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
+    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep"],
+                    help="brunel1m: the 1M-neuron network (default); sweep: batched vs plain "
+                         "parameter sweep")
+    ap.add_argument("--sweep-count", type=int, default=256)
+    ap.add_argument("--sweep-steps", type=int, default=2000)
     ap.add_argument("--kernel-profile", choices=["quiet", "driven"],
                     help="only build the network at --scale, run --warmup bench steps, 300 "
                          "steps as timed, and 300 profiled steps (separate kernels); for ncu captures")
     a = ap.parse_args()
     ws, rank, local = dist_init()
     try:
-        if a.kernel_profile:
+        if a.workload == "sweep":
+            run_sweep(a, ws, rank, local)
+        elif a.kernel_profile:
             w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
             sim = make_sim(w, local, seed=1, record=False)
             sim.run(CHUNK * a.warmup)

@@ -191,6 +191,25 @@ mgc_status mgc_get_info(mgc_sim* sim, mgc_info* info);
  * reference was profiled externally with nvprof, shell/single.sh:15). */
 mgc_status mgc_profile_steps(mgc_sim* sim, int64_t steps, float* ms);
 
+typedef struct mgc_tune_report {
+    int32_t trials;               /* configurations timed */
+    int32_t chunk_len;            /* chosen synapses per delivery task (deferred method) */
+    int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
+    int32_t reserved;
+    double ms_per_step;           /* time per step of the chosen configuration */
+    double default_ms_per_step;   /* time per step of the builder's configuration */
+    int64_t steps;                /* steps simulated by the trials */
+} mgc_tune_report;
+
+/* Autotuner: times `steps_per_trial` steps (rounded up to whole graphs) of
+ * each launch configuration — synapses per delivery task (the threads a
+ * spike's delay segment gets) x resident blocks per SM of the step kernel —
+ * starting with the builder's choice, and keeps the fastest.  The trials are
+ * real steps: the simulation advances by report->steps.  The configuration
+ * changes no result (it only changes which warp adds which synapse).  No
+ * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
+mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
+
 /* The handle's cudaStream_t, for event timing by the caller. */
 mgc_status mgc_get_stream(mgc_sim* sim, void** stream);
 

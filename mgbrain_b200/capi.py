@@ -22,7 +22,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter",
+    "mgc_measure_scatter", "mgc_autotune",
 )
 
 
@@ -53,6 +53,14 @@ class FixedInDegreeDesc(C.Structure):
         ("seed", C.c_uint64), ("mode", C.c_int32), ("device", C.c_int32),
         ("raster_steps", C.c_int64), ("raster_ids", C.c_int64), ("id_offset", C.c_int32),
         ("proj_offset", C.c_int32),
+    ]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("trials", C.c_int32), ("chunk_len", C.c_int32), ("blocks_per_sm", C.c_int32),
+        ("reserved", C.c_int32), ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double),
+        ("steps", C.c_int64),
     ]
 
 
@@ -103,6 +111,8 @@ def lib():
     L.mgc_row_offsets_static.restype = C.c_int
     L.mgc_measure_scatter.argtypes = [i32, i64, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.mgc_measure_scatter.restype = C.c_int
+    L.mgc_autotune.argtypes = [vp, i64, C.POINTER(TuneReport)]
+    L.mgc_autotune.restype = C.c_int
     for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_create_batch", "mgc_run", "mgc_sync", "mgc_set_rates",
                  "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
                  "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
@@ -284,6 +294,13 @@ class Simulator:
         d = np.zeros(self.S, np.int32)
         check(lib().mgc_export_csr(self._h, _ptr(rp), _ptr(t), _ptr(w), _ptr(d)))
         return rp, t, w, d
+
+    def autotune(self, steps_per_trial=640):
+        """Times the launch configurations and keeps the fastest; the trial
+        steps advance the simulation (report["steps"] of them)."""
+        r = TuneReport()
+        check(lib().mgc_autotune(self._h, int(steps_per_trial), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in TuneReport._fields_ if k != "reserved"}
 
     def profile(self, steps):
         """Milliseconds spent in (neuron update, event push, STDP) over `steps`

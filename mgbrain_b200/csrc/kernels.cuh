@@ -61,8 +61,8 @@ struct StepArgs {
     int32_t dmin;         // deferred: delay of bucket 0
     int32_t D;            //   number of delay buckets per row
     int32_t H;            //   history slots (>= dmax + 1)
-    int32_t bucket_chunks;//   tasks per bucket (longest bucket / (task_lanes * 4))
-    int32_t task_lanes;   //   lanes per delivery task: 8 or 32
+    int32_t bucket_chunks;//   delivery tasks per (spike, delay) segment
+    int32_t chunk_len;    //   synapses per task: segment positions [c*len, (c+1)*len)
     int32_t* hist_ids;    //   [H][n] spike ids per step
     int32_t* hist_cnt;    //   [H]
     const int64_t* bucket;   // [n*D + 1] CSR position of (source, bucket)
@@ -530,7 +530,8 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, con
 {
     const int D = a.D;
     const int32_t hs = hist_slot(a, sa);
-    const int64_t total = pre[D];
+    const int CH = a.bucket_chunks;
+    const int64_t total = pre[D] * CH;  // (spike, delay) segments x chunks
     float* acc_e = acc_buf(a, a.acc_e, sa);
     float* acc_i = acc_buf(a, a.acc_i, sa);
     const int lane = threadIdx.x & 31;
@@ -548,19 +549,24 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, con
         int64_t b = 0;
         int32_t len = 0;
         if (lane < per && f < total) {
-            int lo = 0, hi = D - 1;  // last k with pre[k] <= f
+            const int64_t fs = f / CH;               // segment task
+            const int32_t c = (int32_t)(f - fs * CH);  // chunk of it
+            int lo = 0, hi = D - 1;  // last k with pre[k] <= fs
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (pre[mid] <= f) lo = mid; else hi = mid - 1;
+                if (pre[mid] <= fs) lo = mid; else hi = mid - 1;
             }
             const int k = lo;
-            const int32_t j = (int32_t)(f - pre[k]);
+            const int32_t j = (int32_t)(fs - pre[k]);
             int32_t h = hs - (a.dmin + k);
             if (h < 0) h += a.H;
             const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
             const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
-            b = __ldg(bk);
-            len = (int32_t)(__ldg(bk + 1) - b);
+            const int64_t b0 = __ldg(bk);
+            const int64_t seg = __ldg(bk + 1) - b0;
+            const int64_t c0 = (int64_t)c * a.chunk_len;
+            b = b0 + c0;
+            len = seg > c0 ? (int32_t)(seg - c0 < a.chunk_len ? seg - c0 : a.chunk_len) : 0;
         }
         // 2. segments end to end: exclusive offsets
         int32_t incl = len;

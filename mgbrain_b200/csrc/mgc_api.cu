@@ -55,6 +55,8 @@ mgc_status fail(mgc_status st, const char* fmt, ...)
 constexpr int64_t kDefaultRasterSteps = 1 << 16;
 constexpr int kGraphSteps = 64;
 constexpr size_t kMaxBucketBytes = size_t(16) << 30;  // deferred bucket table budget
+constexpr int64_t kDefaultChunk = 128;                // synapses per delivery task
+constexpr int64_t kMaxChunks = 64;                    // tasks per (spike, delay) segment
 
 int bits_for(int64_t n)
 {
@@ -86,6 +88,7 @@ struct mgc_sim {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     int64_t raster_steps_cap = 0, raster_ids_cap = 0;
+    int64_t max_gap = 0;  // longest (source, delay) segment (deferred)
 
     ~mgc_sim()
     {
@@ -484,6 +487,18 @@ void count_keys(mgc_sim* s, const uint32_t* keys, int64_t count)
                                                                  const_cast<int64_t*>(s->a.bucket));
 }
 
+// Segments of up to `gap` synapses cut into chunks of about `target`
+// (a multiple of 32), at most kMaxChunks per segment.
+void set_chunking(StepArgs& a, int64_t gap, int64_t target)
+{
+    int64_t ch = std::max<int64_t>(1, (gap + target - 1) / target);
+    ch = std::min<int64_t>(ch, kMaxChunks);
+    int64_t len = (std::max<int64_t>(gap, 1) + ch - 1) / ch;
+    len = (len + 31) / 32 * 32;
+    a.bucket_chunks = (int32_t)ch;
+    a.chunk_len = (int32_t)len;
+}
+
 // Shared tail of the builders: offsets, method buffers and launch shapes.
 mgc_status finish_build(mgc_sim* s)
 {
@@ -509,12 +524,10 @@ mgc_status finish_build(mgc_sim* s)
         unsigned long long gap = 0;
         CK(cudaMemcpyAsync(&gap, dmax_gap, 8, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        // short buckets (the common case of many delays): 8 or 16 lanes per
-        // task, several tasks per warp; long buckets: a whole warp per task
-        const double mean_bucket = (double)s->S / std::max<double>(1.0, (double)s->n * a.D);
-        a.task_lanes = mean_bucket <= 16.0 ? 8 : (mean_bucket <= 48.0 ? 16 : 32);
-        const int64_t span = (int64_t)a.task_lanes * 4;
-        a.bucket_chunks = (int32_t)std::max<int64_t>(1, ((int64_t)gap + span - 1) / span);
+        // long segments (few delays, large out-degree) are cut into chunks so
+        // one step's synapses spread over all warps
+        set_chunking(a, (int64_t)gap, kDefaultChunk);
+        s->max_gap = (int64_t)gap;
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
         CKS(s->alloc(&a.acc_e, 2 * (size_t)a.ns));  // two step buffers
@@ -1153,6 +1166,102 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
     for (auto& e : ev) cudaEventDestroy(e);
     for (int k = 0; k < 3; ++k) ms[k] = (float)acc[k];
     return st;
+}
+
+namespace {
+
+// Launch configuration the autotuner varies: synapses per delivery task
+// (deferred method) and resident blocks per SM of the step's main kernel.
+struct TuneCand {
+    int64_t chunk_target;
+    int blocks_per_sm;
+};
+
+int& tuned_grid(mgc_sim* s)
+{
+    if (s->a.deferred) return s->fused ? s->fused_grid : s->deliver_grid;
+    return s->a.pull ? s->pull_grid : s->push_grid;
+}
+
+mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
+{
+    if (s->a.deferred) set_chunking(s->a, s->max_gap, c.chunk_target);
+    tuned_grid(s) = sms * c.blocks_per_sm;
+    if (s->graph) {  // the graph holds the old launch parameters
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    return MGC_OK;
+}
+
+}  // namespace
+
+mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* rep)
+{
+    if (!s || !rep || steps_per_trial < 1) return fail(MGC_ERR_INVALID, "bad autotune arguments");
+    CK(cudaSetDevice(s->device));
+    memset(rep, 0, sizeof(*rep));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, s->device));
+    const int sms = prop.multiProcessorCount;
+    int occ = 1;
+    if (s->a.deferred)
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->fused ? (const void*)k_fused : (const void*)k_deliver,
+                                                         kPushBlock, 0));
+    else
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->a.pull ? (const void*)k_pull : (const void*)k_push,
+                                                         kPushBlock, 0));
+    occ = std::max(1, occ);
+    // the builder's choice first, then the grid of chunk lengths x blocks per SM
+    std::vector<TuneCand> cands;
+    cands.push_back({s->a.deferred ? kDefaultChunk : 0, std::max(1, tuned_grid(s) / sms)});
+    const int64_t targets[] = {64, 128, 256, 512, 1024};
+    for (int64_t t : s->a.deferred ? std::vector<int64_t>(targets, targets + 5) : std::vector<int64_t>{0})
+        for (int b = 1; b <= occ; ++b) {
+            if (t == cands[0].chunk_target && b == cands[0].blocks_per_sm) continue;
+            if (s->a.deferred && t > kDefaultChunk && s->max_gap <= kDefaultChunk) continue;  // same chunking
+            cands.push_back({t, b});
+        }
+    const int64_t steps = (steps_per_trial + kGraphSteps - 1) / kGraphSteps * kGraphSteps;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 1e300;
+    size_t best_i = 0;
+    mgc_status st = MGC_OK;
+    for (size_t i = 0; i < cands.size() && st == MGC_OK; ++i) {
+        st = apply_cand(s, cands[i], sms);
+        if (st == MGC_OK) st = mgc_run(s, kGraphSteps);  // builds the graph, settles the state
+        if (st != MGC_OK) break;
+        cudaEventRecord(e0, s->stream);
+        st = mgc_run(s, steps);
+        cudaEventRecord(e1, s->stream);
+        if (st != MGC_OK) break;
+        float ms = 0.f;
+        cudaError_t err = cudaEventSynchronize(e1);
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        if (err != cudaSuccess) {
+            st = fail(MGC_ERR_CUDA, "autotune: %s", cudaGetErrorString(err));
+            break;
+        }
+        const double per = (double)ms / (double)steps;
+        if (i == 0) rep->default_ms_per_step = per;
+        if (per < best) {
+            best = per;
+            best_i = i;
+        }
+        rep->trials += 1;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (st != MGC_OK) return st;
+    CKS(apply_cand(s, cands[best_i], sms));
+    rep->ms_per_step = best;
+    rep->chunk_len = s->a.deferred ? s->a.chunk_len : 0;
+    rep->blocks_per_sm = cands[best_i].blocks_per_sm;
+    rep->steps = (int64_t)rep->trials * (steps + kGraphSteps);
+    return MGC_OK;
 }
 
 mgc_status mgc_get_stream(mgc_sim* s, void** stream)
