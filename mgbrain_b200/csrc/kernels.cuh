@@ -55,6 +55,8 @@ struct StepArgs {
     float C[30];          // LIFECONSTS
     float P[6];           // STDPCONSTS
     int32_t chunks_per_spike;
+    int32_t has_cur;      // some neuron is LIF or LIFE: the update loads Iexc/Iinh with the group
+                          // (k_fused is instantiated for each case)
     int32_t stdp;
     int32_t record;       // raster recording on
     int32_t deferred;     // deferred delivery (else ring)
@@ -180,8 +182,10 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
 // padded to a multiple of 4 with RAW neurons, which never change); spiking
 // ids are compacted in neuron order within a warp, one atomic per warp.
 // ---------------------------------------------------------------------------
+// One neuron of a group; ie_io/ii_io (LIF and LIFE currents) were loaded
+// with the group when the network has such neurons and are stored back with it.
 __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, int64_t s, float& v, int32_t& rf,
-                                           float re, float ri)
+                                           float re, float ri, float& ie_io, float& ii_io)
 {
     bool fired = false;
     if (t == kPOISSON) {
@@ -205,7 +209,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
         if (rf > 0) {
             --rf;
         } else {
-            float ie = a.Iexc[i], ii = a.Iinh[i];
+            float ie = ie_io, ii = ii_io;
             float nv = __fmul_rn(a.C[17], v);
             nv = __fadd_rn(nv, a.C[14]);
             nv = __fadd_rn(nv, __fmul_rn(ie, a.C[12]));
@@ -221,15 +225,15 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
                 ii = __fadd_rn(ii, ri);
             }
             v = nv;
-            a.Iexc[i] = ie;
-            a.Iinh[i] = ii;
+            ie_io = ie;
+            ii_io = ii;
         }
     } else if (t == kLIFE) {
         // mgcore.cu:197-233: conductances decay every step
-        const float ie = __fadd_rn(re, __fmul_rn(a.Iexc[i], 0.98f));
-        const float ii = __fadd_rn(-ri, __fmul_rn(a.Iinh[i], 0.99f));
-        a.Iexc[i] = ie;
-        a.Iinh[i] = ii;
+        const float ie = __fadd_rn(re, __fmul_rn(ie_io, 0.98f));
+        const float ii = __fadd_rn(-ri, __fmul_rn(ii_io, 0.99f));
+        ie_io = ie;
+        ii_io = ii;
         if (rf > 0) {
             --rf;
         } else if (v >= a.C[4]) {
@@ -259,7 +263,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 // read from (and cleared in) in_e/in_i, which point at the ring slot or the
 // accumulator buffer.  Spiking ids are compacted in neuron order within the
 // pass, one atomic per warp.
-template <int G>
+template <int G, bool CUR>
 __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
                                               int64_t warp, int64_t nwarps)
 {
@@ -272,19 +276,22 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     const int64_t rbase = rec ? *a.raster_pos : 0;
     for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
         char4 t4[G];
-        float4 v4[G], e4[G], i4[G];
+        float4 v4[G], e4[G], i4[G], ce4[G], ci4[G];
         int4 r4[G];
 #pragma unroll
         for (int h = 0; h < G; ++h) {
             const int64_t g = gb + h * 32 + lane;
+            ce4[h] = ci4[h] = make_float4(0.f, 0.f, 0.f, 0.f);
             if (g < ngroups) {
                 t4[h] = __ldg(reinterpret_cast<const char4*>(a.type) + g);
                 v4[h] = reinterpret_cast<float4*>(a.V)[g];
                 r4[h] = reinterpret_cast<int4*>(a.refrac)[g];
                 e4[h] = reinterpret_cast<float4*>(in_e)[g];
                 i4[h] = reinterpret_cast<float4*>(in_i)[g];
-                reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (CUR) {  // in flight with the rest of the group
+                    ce4[h] = reinterpret_cast<float4*>(a.Iexc)[g];
+                    ci4[h] = reinterpret_cast<float4*>(a.Iinh)[g];
+                }
             }
         }
         unsigned fmask[G];
@@ -294,12 +301,22 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             fmask[h] = 0;
             if (g < ngroups) {
                 const int32_t i0 = (int32_t)(g << 2);
-                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x) ? 1u : 0u;
-                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y) ? 2u : 0u;
-                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z) ? 4u : 0u;
-                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w) ? 8u : 0u;
+                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x, ce4[h].x, ci4[h].x) ? 1u : 0u;
+                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y, ce4[h].y, ci4[h].y) ? 2u : 0u;
+                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z, ce4[h].z, ci4[h].z) ? 4u : 0u;
+                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w, ce4[h].w, ci4[h].w) ? 8u : 0u;
+                // the input is cleared only after it was used: a store issued
+                // while the load of the same line is in flight stalls the
+                // memory pipeline (measured 4-6x slower once the state
+                // leaves L2)
+                reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
                 reinterpret_cast<float4*>(a.V)[g] = v4[h];
                 reinterpret_cast<int4*>(a.refrac)[g] = r4[h];
+                if (CUR) {
+                    reinterpret_cast<float4*>(a.Iexc)[g] = ce4[h];
+                    reinterpret_cast<float4*>(a.Iinh)[g] = ci4[h];
+                }
             }
             if (a.pull) {
                 // bitmap of this step's spikes: 8 lanes (32 neurons) per word
@@ -366,7 +383,10 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
     }
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    neuron_groups<1>(a, s, hslot, in_e, in_i, warp, nwarps);
+    if (a.has_cur)
+        neuron_groups<1, true>(a, s, hslot, in_e, in_i, warp, nwarps);
+    else
+        neuron_groups<1, false>(a, s, hslot, in_e, in_i, warp, nwarps);
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
@@ -627,6 +647,7 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 // share of the neurons for step s and then delivers its share of those
 // arrivals into the other accumulator buffer; the memory-latency chains of
 // different warps overlap on each SM.
+template <bool CUR>
 __global__ void __launch_bounds__(kPushBlock, 3) k_fused(StepArgs a)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
@@ -636,7 +657,7 @@ __global__ void __launch_bounds__(kPushBlock, 3) k_fused(StepArgs a)
     // the first warp sums the spike counts per delay while all warps update
     // their neurons; the barrier then publishes the sums for the delivery
     if (threadIdx.x < 32) deliver_prefix(a, s + 1, pre);
-    neuron_groups<2>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
+    neuron_groups<2, CUR>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
     __syncthreads();
     deliver_tasks(a, s + 1, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);

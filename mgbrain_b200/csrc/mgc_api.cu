@@ -383,6 +383,8 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     CKS(s->alloc(&d_type, ns));
     CK(cudaMemcpyAsync(d_type, type, n, cudaMemcpyHostToDevice, s->stream));
     a.type = d_type;
+    a.has_cur = 0;
+    for (int32_t i = 0; i < n; ++i) a.has_cur |= type[i] == kLIF || type[i] == kLIFE;
     float* d_rate;
     CKS(s->alloc(&d_rate, ns));
     if (rate) CK(cudaMemcpyAsync(d_rate, rate, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
@@ -487,6 +489,10 @@ void count_keys(mgc_sim* s, const uint32_t* keys, int64_t count)
                                                                  const_cast<int64_t*>(s->a.bucket));
 }
 
+// The fused step kernel for this network (with or without LIF/LIFE currents).
+using StepKernel = void (*)(StepArgs);
+StepKernel fused_kernel(const mgc_sim* s) { return s->a.has_cur ? k_fused<true> : k_fused<false>; }
+
 // Segments of up to `gap` synapses cut into chunks of about `target`
 // (a multiple of 32), at most kMaxChunks per segment.
 void set_chunking(StepArgs& a, int64_t gap, int64_t target)
@@ -536,7 +542,7 @@ mgc_status finish_build(mgc_sim* s)
         s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
         // fused step kernel: one resident wave, every warp delivers then updates
         s->fused = s->dmin >= 2;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fused, kPushBlock, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_kernel(s), kPushBlock, 0));
         s->fused_grid = prop.multiProcessorCount * std::max(1, occ);
     } else {
         a.M = s->M;
@@ -578,7 +584,7 @@ mgc_status enqueue_step(mgc_sim* s)
                 k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
                 s->launches += 1;
             }
-            k_fused<<<s->fused_grid, kPushBlock, 0, s->stream>>>(s->a);
+            fused_kernel(s)<<<s->fused_grid, kPushBlock, 0, s->stream>>>(s->a);
             s->ahead = true;
             s->launches += 1;
         } else {
@@ -1207,7 +1213,7 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     const int sms = prop.multiProcessorCount;
     int occ = 1;
     if (s->a.deferred)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->fused ? (const void*)k_fused : (const void*)k_deliver,
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->fused ? (const void*)fused_kernel(s) : (const void*)k_deliver,
                                                          kPushBlock, 0));
     else
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->a.pull ? (const void*)k_pull : (const void*)k_push,
