@@ -210,6 +210,67 @@ typedef struct mgc_tune_report {
  * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 
+/* ---- Step scheduler (fused deferred method: minimum delay >= 2) ----------
+ * Each CUDA graph of 64 steps starts with a decision kernel that picks which
+ * of two instantiations of the fused step kernel (compiled for 2 or 3
+ * resident blocks per SM) runs the group, through a conditional SWITCH node:
+ * the choice is made on the device, the host never waits for it, and it
+ * changes no arithmetic (rasters are those of either variant alone).
+ *   STATIC:    the autotuner's variant.
+ *   THRESHOLD: the variant for the last group's delivered events per step
+ *              (above `threshold`: hi_variant, else the other).
+ *   LEARNED:   the same rule on the events per step that a small MLP
+ *              (4 groups x [spikes of up to 4 trace populations, events] ->
+ *              next group, 32 ReLU hidden units) predicts; trained on the
+ *              GPU by the library's own forward/backward/Adam kernel on group
+ *              traces the simulator recorded.
+ * A decision is a miss when it differs from the rule applied to the group's
+ * actual load.  No reference counterpart (fixed schedule, mgcore.cu:535-554). */
+enum { MGC_SCHED_STATIC = 0, MGC_SCHED_THRESHOLD = 1, MGC_SCHED_LEARNED = 2 };
+
+/* MLP shape: flat parameters [W1 (32x20, row-major), b1 (32), W2 (5x32), b2 (5)]. */
+enum { MGC_MLP_IN = 20, MGC_MLP_HIDDEN = 32, MGC_MLP_OUT = 5, MGC_MLP_PARAMS = 837 };
+
+typedef struct mgc_sched_stats {
+    int32_t mode;
+    int32_t trained;
+    int64_t groups;               /* decisions scored (THRESHOLD / LEARNED groups) */
+    int64_t misses;
+    int64_t variant_groups[2];    /* groups run by each variant */
+    double mean_abs_log_err;      /* LEARNED: mean |log1p(predicted) - log1p(actual)| events/step */
+    double threshold;
+    int32_t hi_variant;
+    int32_t static_variant;
+    int32_t recorded_groups;      /* group rows recorded for training */
+    int32_t reserved;
+} mgc_sched_stats;
+
+mgc_status mgc_sched_set_mode(mgc_sim* sim, int32_t mode);
+
+/* The load (delivered events per step) above which hi_variant runs. */
+mgc_status mgc_sched_set_threshold(mgc_sim* sim, double threshold, int32_t hi_variant);
+
+/* Runs `groups`+1 step groups alternating the two variants (real steps),
+ * fits time per step = a + b * load for each and sets the threshold to the
+ * crossing inside the observed load range (else: the faster variant always). */
+mgc_status mgc_sched_calibrate(mgc_sim* sim, int32_t groups, double* threshold);
+
+/* Records (on != 0) the feature row of every step group that runs from now
+ * on, for training; reset drops the rows recorded so far. */
+mgc_status mgc_sched_collect(mgc_sim* sim, int32_t on, int32_t reset);
+
+/* Trains the MLP on the recorded rows (windows of 4 consecutive groups ->
+ * the next), `epochs` passes of Adam, minibatches of 64, on the GPU. */
+mgc_status mgc_sched_train(mgc_sim* sim, int32_t epochs, float lr, uint64_t seed, float* final_loss);
+
+mgc_status mgc_sched_report(mgc_sim* sim, mgc_sched_stats* report, int32_t reset);
+
+/* Loss (1/n) sum_b sum_o (y - t)^2 / 2 and its gradient at `params` for n
+ * (<= 128) samples x [n][20], t [n][5], computed by the training kernel's
+ * forward/backward on `device` (host arrays in and out). */
+mgc_status mgc_mlp_gradient(int32_t device, const float* params, const float* x, const float* y, int32_t n,
+                            float* grad, float* loss);
+
 /* The handle's cudaStream_t, for event timing by the caller. */
 mgc_status mgc_get_stream(mgc_sim* sim, void** stream);
 

@@ -16,13 +16,16 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libm
 MGC_OK, MGC_ERR_INVALID, MGC_ERR_CUDA, MGC_ERR_NOMEM, MGC_ERR_OVERFLOW, MGC_ERR_NODEVICE = range(6)
 RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)
 MODE_AUTO, MODE_PUSH, MODE_DEFERRED, MODE_PULL = 0, 1, 2, 3
+SCHED_STATIC, SCHED_THRESHOLD, SCHED_LEARNED = 0, 1, 2
+MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_PARAMS = 20, 32, 5, 837
 
 EXPORTED = (
     "mgc_create", "mgc_create_fixed_indegree", "mgc_run", "mgc_sync", "mgc_set_rates",
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_sched_set_mode", "mgc_sched_set_threshold",
+    "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
 )
 
 
@@ -61,6 +64,15 @@ class TuneReport(C.Structure):
         ("trials", C.c_int32), ("chunk_len", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("reserved", C.c_int32), ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double),
         ("steps", C.c_int64),
+    ]
+
+
+class SchedStats(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int32), ("trained", C.c_int32), ("groups", C.c_int64), ("misses", C.c_int64),
+        ("variant_groups", C.c_int64 * 2), ("mean_abs_log_err", C.c_double), ("threshold", C.c_double),
+        ("hi_variant", C.c_int32), ("static_variant", C.c_int32), ("recorded_groups", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 
@@ -113,6 +125,16 @@ def lib():
     L.mgc_measure_scatter.restype = C.c_int
     L.mgc_autotune.argtypes = [vp, i64, C.POINTER(TuneReport)]
     L.mgc_autotune.restype = C.c_int
+    L.mgc_sched_set_mode.argtypes = [vp, i32]
+    L.mgc_sched_set_threshold.argtypes = [vp, C.c_double, i32]
+    L.mgc_sched_calibrate.argtypes = [vp, i32, C.POINTER(C.c_double)]
+    L.mgc_sched_collect.argtypes = [vp, i32, i32]
+    L.mgc_sched_train.argtypes = [vp, i32, C.c_float, C.c_uint64, C.POINTER(C.c_float)]
+    L.mgc_sched_report.argtypes = [vp, C.POINTER(SchedStats), i32]
+    L.mgc_mlp_gradient.argtypes = [i32, vp, vp, vp, i32, vp, vp]
+    for name in ("mgc_sched_set_mode", "mgc_sched_set_threshold", "mgc_sched_calibrate", "mgc_sched_collect",
+                 "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient"):
+        getattr(L, name).restype = C.c_int
     for name in ("mgc_create", "mgc_create_fixed_indegree", "mgc_create_batch", "mgc_run", "mgc_sync", "mgc_set_rates",
                  "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr",
                  "mgc_get_info", "mgc_get_stream", "mgc_profile_steps"):
@@ -136,6 +158,18 @@ def measure_scatter(device=0, n_events=100_000_000, n_targets=1 << 20, reps=3):
     check(lib().mgc_measure_scatter(int(device), int(n_events), int(n_targets), int(reps), C.byref(red),
                                     C.byref(rd)))
     return red.value, rd.value
+
+
+def mlp_gradient(params, x, y, device=0):
+    """(loss, grad) of the scheduler MLP at `params` on samples x [n][20],
+    targets y [n][5], computed by the library's training kernel."""
+    p = np.ascontiguousarray(params, np.float32)
+    xs = np.ascontiguousarray(x, np.float32)
+    ys = np.ascontiguousarray(y, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    check(lib().mgc_mlp_gradient(int(device), _ptr(p), _ptr(xs), _ptr(ys), int(xs.shape[0]), _ptr(g), _ptr(loss)))
+    return float(loss[0]), g
 
 
 def effective_steps(steps, min_delay):
@@ -301,6 +335,33 @@ class Simulator:
         r = TuneReport()
         check(lib().mgc_autotune(self._h, int(steps_per_trial), C.byref(r)))
         return {k: getattr(r, k) for k, _ in TuneReport._fields_ if k != "reserved"}
+
+    # ---- step scheduler ---------------------------------------------------
+    def sched_mode(self, mode):
+        check(lib().mgc_sched_set_mode(self._h, int(mode)))
+
+    def sched_threshold(self, threshold, hi_variant=1):
+        check(lib().mgc_sched_set_threshold(self._h, float(threshold), int(hi_variant)))
+
+    def sched_calibrate(self, groups=16):
+        t = C.c_double()
+        check(lib().mgc_sched_calibrate(self._h, int(groups), C.byref(t)))
+        return t.value
+
+    def sched_collect(self, on=True, reset=False):
+        check(lib().mgc_sched_collect(self._h, int(bool(on)), int(bool(reset))))
+
+    def sched_train(self, epochs=200, lr=3e-3, seed=1):
+        loss = C.c_float()
+        check(lib().mgc_sched_train(self._h, int(epochs), float(lr), int(seed), C.byref(loss)))
+        return loss.value
+
+    def sched_report(self, reset=False):
+        r = SchedStats()
+        check(lib().mgc_sched_report(self._h, C.byref(r), int(bool(reset))))
+        d = {k: getattr(r, k) for k, _ in SchedStats._fields_ if k != "reserved"}
+        d["variant_groups"] = [r.variant_groups[0], r.variant_groups[1]]
+        return d
 
     def profile(self, steps):
         """Milliseconds spent in (neuron update, event push, STDP) over `steps`

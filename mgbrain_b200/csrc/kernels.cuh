@@ -40,6 +40,9 @@ constexpr int kNeuronBlock = 256;
 constexpr int kPushBlock = 256;
 constexpr int kChunk = 128;           // synapses per warp task (4 per lane)
 constexpr int kMaxBuckets = 2048;     // delay values the deferred method handles
+constexpr int kTracePops = 4;         // schedule trace: populations counted per step
+constexpr int kTraceCols = kTracePops + 1;  // ... plus the events delivered
+constexpr int kTraceSteps = 1024;     // rows of the per-step trace ring
 
 struct StepArgs {
     int32_t n;            // neurons
@@ -108,6 +111,11 @@ struct StepArgs {
     int64_t* raster_pos;
     int64_t* raster_step0;
     int32_t* status;
+    // schedule trace (fused method): row s % kTraceSteps holds step s's spikes
+    // per trace population and the events its kernel delivered
+    const uint8_t* tpop;      // [ns] trace population of each neuron (< kTracePops)
+    float* trace;             // [kTraceSteps][kTraceCols]
+    unsigned long long* ev_mark;  // events counter at the previous step's end
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
@@ -163,6 +171,13 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
         const int64_t pos = *a.raster_pos;
         if (pos + nspk > a.raster_ids_cap) atomicOr(a.status, kStatusRasterIds);
         *a.raster_pos = pos + nspk;
+    }
+    if (a.trace) {
+        const unsigned long long ev = *(volatile unsigned long long*)a.events;
+        a.trace[(s & (kTraceSteps - 1)) * kTraceCols + kTracePops] = (float)(ev - *a.ev_mark);
+        *a.ev_mark = ev;
+        float* nxt = a.trace + ((s + 1) & (kTraceSteps - 1)) * kTraceCols;
+        for (int c = 0; c < kTraceCols; ++c) nxt[c] = 0.f;
     }
     const int32_t next_h = hslot + 1 == a.H ? 0 : hslot + 1;
     if (a.deferred)
@@ -265,7 +280,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 // pass, one atomic per warp.
 template <int G, bool CUR>
 __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
-                                              int64_t warp, int64_t nwarps)
+                                              int64_t warp, int64_t nwarps, int* pop_cnt = nullptr)
 {
     static_assert(G == 1 || G == 2, "one or two groups per lane");
     const int lane = threadIdx.x & 31;
@@ -355,6 +370,7 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 for (int k = 0; k < 4; ++k) {
                     if (fmask[h] & (1u << k)) {
                         ids[pos] = i0 + k;
+                        if (pop_cnt) atomicAdd(pop_cnt + a.tpop[i0 + k], 1);
                         if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
                         ++pos;
                     }
@@ -647,18 +663,26 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 // share of the neurons for step s and then delivers its share of those
 // arrivals into the other accumulator buffer; the memory-latency chains of
 // different warps overlap on each SM.
-template <bool CUR>
-__global__ void __launch_bounds__(kPushBlock, 3) k_fused(StepArgs a)
+// MINB: resident blocks per SM the kernel is compiled for (its register
+// budget); the schedule chooses between the instantiations.
+template <bool CUR, int MINB>
+__global__ void __launch_bounds__(kPushBlock, MINB) k_fused(StepArgs a)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
+    __shared__ int pop_cnt[kTracePops];
     const int64_t s = *a.step;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    if (threadIdx.x < kTracePops) pop_cnt[threadIdx.x] = 0;
+    __syncthreads();
     // the first warp sums the spike counts per delay while all warps update
     // their neurons; the barrier then publishes the sums for the delivery
     if (threadIdx.x < 32) deliver_prefix(a, s + 1, pre);
-    neuron_groups<2, CUR>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps);
+    neuron_groups<2, CUR>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+                          a.trace ? pop_cnt : nullptr);
     __syncthreads();
+    if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
+        atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
     deliver_tasks(a, s + 1, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);
 }

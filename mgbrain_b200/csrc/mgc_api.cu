@@ -15,6 +15,7 @@
 
 #include "../../include/mgc.h"
 #include "kernels.cuh"
+#include "sched.cuh"
 
 using namespace mgc;
 
@@ -89,6 +90,14 @@ struct mgc_sim {
     int graph_steps = 0;
     int64_t raster_steps_cap = 0, raster_ids_cap = 0;
     int64_t max_gap = 0;  // longest (source, delay) segment (deferred)
+    // fused method: two instantiations of the step kernel (2 or 3 resident
+    // blocks per SM); `fused_variant` runs outside the scheduler's graphs
+    int fused_variant = 1;
+    int fused_grid_v[2] = {1, 1};
+    std::vector<uint8_t> tpop_host;   // trace population of each neuron (set by the builders)
+    SchedState* sched = nullptr;      // device
+    float* sched_data = nullptr;      // device [kMaxDataset][kTraceCols]
+    bool sched_graph = false;         // the step-group graph branches on the scheduler's choice
 
     ~mgc_sim()
     {
@@ -489,9 +498,54 @@ void count_keys(mgc_sim* s, const uint32_t* keys, int64_t count)
                                                                  const_cast<int64_t*>(s->a.bucket));
 }
 
-// The fused step kernel for this network (with or without LIF/LIFE currents).
+// The fused step kernel for this network (with or without LIF/LIFE
+// currents), variant 0 compiled for 2 resident blocks per SM, 1 for 3.
 using StepKernel = void (*)(StepArgs);
-StepKernel fused_kernel(const mgc_sim* s) { return s->a.has_cur ? k_fused<true> : k_fused<false>; }
+StepKernel fused_kernel(const mgc_sim* s, int v)
+{
+    if (s->a.has_cur) return v == 0 ? k_fused<true, 2> : k_fused<true, 3>;
+    return v == 0 ? k_fused<false, 2> : k_fused<false, 3>;
+}
+
+// Trace buffers and scheduler state of the fused method.  Trace population
+// of a neuron: as the builder set it (population index, or neuron type class
+// for synapse-list networks), clamped to kTracePops - 1.
+mgc_status init_sched(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    std::vector<uint8_t> tp(a.ns, 0);
+    for (size_t i = 0; i < s->tpop_host.size() && i < tp.size(); ++i)
+        tp[i] = (uint8_t)std::min<int>(s->tpop_host[i], kTracePops - 1);
+    uint8_t* d_tp;
+    CKS(s->upload(&d_tp, tp.data(), tp.size()));
+    a.tpop = d_tp;
+    CKS(s->alloc(&a.trace, (size_t)kTraceSteps * kTraceCols));
+    CKS(s->alloc(&a.ev_mark, 1));
+    CKS(s->alloc(&s->sched, 1));
+    CKS(s->alloc(&s->sched_data, (size_t)kMaxDataset * kTraceCols));
+    SchedState h;
+    memset(&h, 0, sizeof(h));
+    h.mode = kSchedStatic;
+    h.static_variant = s->fused_variant;
+    h.forced_variant = -1;
+    h.threshold = 1e30f;
+    h.hi_variant = 1;
+    for (int i = 0; i < kMlpIn; ++i) h.xs[i] = 1.f;
+    for (int o = 0; o < kMlpOut; ++o) h.ys[o] = 1.f;
+    CK(cudaMemcpyAsync(s->sched, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
+    return MGC_OK;
+}
+
+// Stream-ordered write of one field of the device scheduler state.
+template <class T>
+mgc_status sched_put(mgc_sim* s, T SchedState::*field, T value)
+{
+    static SchedState layout;  // host object, for the field's offset only
+    const size_t off = (size_t)(reinterpret_cast<const char*>(&(layout.*field)) - reinterpret_cast<const char*>(&layout));
+    T staged = value;
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(s->sched) + off, &staged, sizeof(T), cudaMemcpyHostToDevice, s->stream));
+    return cudaStreamSynchronize(s->stream) == cudaSuccess ? MGC_OK : fail(MGC_ERR_CUDA, "scheduler write failed");
+}
 
 // Segments of up to `gap` synapses cut into chunks of about `target`
 // (a multiple of 32), at most kMaxChunks per segment.
@@ -540,10 +594,15 @@ mgc_status finish_build(mgc_sim* s)
         CKS(s->alloc(&a.acc_i, 2 * (size_t)a.ns));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_deliver, kPushBlock, 0));
         s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
-        // fused step kernel: one resident wave, every warp delivers then updates
+        // fused step kernel: one resident wave, every warp updates then delivers
         s->fused = s->dmin >= 2;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_kernel(s), kPushBlock, 0));
-        s->fused_grid = prop.multiProcessorCount * std::max(1, occ);
+        for (int v = 0; v < 2; ++v) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_kernel(s, v), kPushBlock, 0));
+            s->fused_grid_v[v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+        }
+        s->fused_variant = 1;
+        s->fused_grid = s->fused_grid_v[1];
+        if (s->fused) CKS(init_sched(s));
     } else {
         a.M = s->M;
         CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns));
@@ -584,7 +643,7 @@ mgc_status enqueue_step(mgc_sim* s)
                 k_deliver<<<s->deliver_grid, kPushBlock, 0, s->stream>>>(s->a);
                 s->launches += 1;
             }
-            fused_kernel(s)<<<s->fused_grid, kPushBlock, 0, s->stream>>>(s->a);
+            fused_kernel(s, s->fused_variant)<<<s->fused_grid, kPushBlock, 0, s->stream>>>(s->a);
             s->ahead = true;
             s->launches += 1;
         } else {
@@ -631,6 +690,59 @@ mgc_status build_graph(mgc_sim* s)
     return MGC_OK;
 }
 
+// Step-group graph of the fused method: the scheduler's decision kernel,
+// then a conditional SWITCH node whose body v runs kGraphSteps steps of
+// variant v; the decision kernel sets the branch on the device, so the host
+// never waits for it.
+mgc_status build_sched_graph(mgc_sim* s)
+{
+    struct GraphGuard {
+        cudaGraph_t g = nullptr;
+        ~GraphGuard()
+        {
+            if (g) cudaGraphDestroy(g);
+        }
+    } guard;
+    CK(cudaGraphCreate(&guard.g, 0));
+    cudaGraphConditionalHandle handle;
+    CK(cudaGraphConditionalHandleCreate(&handle, guard.g, (unsigned)s->fused_variant, cudaGraphCondAssignDefault));
+    int32_t set_handle = 1;
+    void* dargs[] = {&s->a, &s->sched, &s->sched_data, &handle, &set_handle};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_sched_decide;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = dargs;
+    cudaGraphNode_t decide;
+    CK(cudaGraphAddKernelNode(&decide, guard.g, nullptr, 0, &kp));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = handle;
+    cp.conditional.type = cudaGraphCondTypeSwitch;
+    cp.conditional.size = 2;
+    cudaGraphNode_t cond;
+    CK(cudaGraphAddNode(&cond, guard.g, &decide, 1, &cp));
+    void* sargs[] = {&s->a};
+    for (int v = 0; v < 2; ++v) {
+        cudaGraph_t body = cp.conditional.phGraph_out[v];
+        cudaGraphNode_t prev = nullptr;
+        for (int i = 0; i < kGraphSteps; ++i) {
+            cudaKernelNodeParams sp = {};
+            sp.func = (void*)fused_kernel(s, v);
+            sp.gridDim = dim3(s->fused_grid_v[v]);
+            sp.blockDim = dim3(kPushBlock);
+            sp.kernelParams = sargs;
+            cudaGraphNode_t node;
+            CK(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &sp));
+            prev = node;
+        }
+    }
+    CK(cudaGraphInstantiate(&s->graph, guard.g, 0));
+    s->graph_steps = kGraphSteps;
+    s->sched_graph = true;
+    return MGC_OK;
+}
+
 mgc_status check_tbits(mgc_sim* s)
 {
     StepArgs& a = s->a;
@@ -666,6 +778,12 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     StepArgs& a = s->a;
     a.stdp = s->stdp;
     a.id_offset = d->id_offset;
+    // trace populations by neuron type: POISSON, LIF family, the rest
+    s->tpop_host.resize(s->n);
+    for (int32_t i = 0; i < s->n; ++i) {
+        const int t = d->type[i];
+        s->tpop_host[i] = t == MGC_POISSON ? 0 : (t == MGC_LIF || t == MGC_LIFE || t == MGC_LIFB ? 1 : 2);
+    }
     const int64_t S = s->S;
     // delay range (mgsim.cpp:42-51); M = max_delay + 1 (:71)
     int32_t dmin = 0x7fffffff, dmax = 0;
@@ -849,12 +967,16 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
     const int64_t S = sbase[n_blocks];
     if (S == 0) dmin = dmax = 1;
     std::vector<int8_t> type(n, (int8_t)MGC_RAW);
+    std::vector<uint8_t> tpop(n, 0);
     std::vector<float> rate(n, 0.0f), v0(n, d0.lifconst[1]);
     for (int b = 0; b < n_blocks; ++b) {
         const mgc_fixed_indegree_desc& d = blocks[b];
         const int64_t nb = start[b + 1] - start[b];
         for (int p = 0; p < d.n_pops; ++p)
-            for (int32_t i = 0; i < d.pop_num[p]; ++i) type[start[b] + d.pop_start[p] + i] = (int8_t)d.pop_type[p];
+            for (int32_t i = 0; i < d.pop_num[p]; ++i) {
+                type[start[b] + d.pop_start[p] + i] = (int8_t)d.pop_type[p];
+                tpop[start[b] + d.pop_start[p] + i] = (uint8_t)std::min(p, kTracePops - 1);
+            }
         if (d.rate) memcpy(rate.data() + start[b], d.rate, 4 * nb);
         if (d.v_init) memcpy(v0.data() + start[b], d.v_init, 4 * nb);
     }
@@ -867,6 +989,7 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
     float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
     CKS(init_common(s.get(), n, type.data(), rate.data(), v0.data(), d0.lifconst, stdpc, d0.seed, d0.raster_steps,
                     d0.raster_ids));
+    s->tpop_host = std::move(tpop);
     StepArgs& a = s->a;
     a.id_offset = d0.id_offset;
     s->dmin = dmin;
@@ -925,10 +1048,10 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         --left;
     }
     if (left >= kGraphSteps) {
-        if (!s->graph) CKS(build_graph(s));
+        if (!s->graph) CKS(s->fused && s->sched ? build_sched_graph(s) : build_graph(s));
         while (left >= s->graph_steps) {
             CK(cudaGraphLaunch(s->graph, s->stream));
-            s->launches += (int64_t)s->graph_steps * kernels_per_step(s);
+            s->launches += (int64_t)s->graph_steps * kernels_per_step(s) + (s->sched_graph ? 1 : 0);
             left -= s->graph_steps;
         }
     }
@@ -1177,7 +1300,8 @@ mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
 namespace {
 
 // Launch configuration the autotuner varies: synapses per delivery task
-// (deferred method) and resident blocks per SM of the step's main kernel.
+// (deferred method) and resident blocks per SM of the step's main kernel
+// (for the fused method: its instantiation for 2 or 3 blocks per SM).
 struct TuneCand {
     int64_t chunk_target;
     int blocks_per_sm;
@@ -1191,12 +1315,19 @@ int& tuned_grid(mgc_sim* s)
 
 mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
 {
-    if (s->a.deferred) set_chunking(s->a, s->max_gap, c.chunk_target);
-    tuned_grid(s) = sms * c.blocks_per_sm;
     if (s->graph) {  // the graph holds the old launch parameters
         CK(cudaStreamSynchronize(s->stream));
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
+        s->sched_graph = false;
+    }
+    if (s->a.deferred) set_chunking(s->a, s->max_gap, c.chunk_target);
+    if (s->fused) {
+        s->fused_variant = c.blocks_per_sm >= 3 ? 1 : 0;
+        s->fused_grid = s->fused_grid_v[s->fused_variant];
+        CKS(sched_put(s, &SchedState::static_variant, (int32_t)s->fused_variant));
+    } else {
+        tuned_grid(s) = sms * c.blocks_per_sm;
     }
     return MGC_OK;
 }
@@ -1211,20 +1342,24 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, s->device));
     const int sms = prop.multiProcessorCount;
-    int occ = 1;
-    if (s->a.deferred)
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->fused ? (const void*)fused_kernel(s) : (const void*)k_deliver,
-                                                         kPushBlock, 0));
-    else
+    int occ = 1, occ_min = 1;
+    if (s->fused) {
+        occ_min = 2;  // the two instantiations of the fused kernel
+        occ = 3;
+    } else if (s->a.deferred) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_deliver, kPushBlock, 0));
+    } else {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->a.pull ? (const void*)k_pull : (const void*)k_push,
                                                          kPushBlock, 0));
+    }
     occ = std::max(1, occ);
     // the builder's choice first, then the grid of chunk lengths x blocks per SM
     std::vector<TuneCand> cands;
-    cands.push_back({s->a.deferred ? kDefaultChunk : 0, std::max(1, tuned_grid(s) / sms)});
+    cands.push_back({s->a.deferred ? kDefaultChunk : 0,
+                     s->fused ? (s->fused_variant == 1 ? 3 : 2) : std::max(1, tuned_grid(s) / sms)});
     const int64_t targets[] = {64, 128, 256, 512, 1024};
     for (int64_t t : s->a.deferred ? std::vector<int64_t>(targets, targets + 5) : std::vector<int64_t>{0})
-        for (int b = 1; b <= occ; ++b) {
+        for (int b = occ_min; b <= occ; ++b) {
             if (t == cands[0].chunk_target && b == cands[0].blocks_per_sm) continue;
             if (s->a.deferred && t > kDefaultChunk && s->max_gap <= kDefaultChunk) continue;  // same chunking
             cands.push_back({t, b});
@@ -1267,6 +1402,251 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     rep->chunk_len = s->a.deferred ? s->a.chunk_len : 0;
     rep->blocks_per_sm = cands[best_i].blocks_per_sm;
     rep->steps = (int64_t)rep->trials * (steps + kGraphSteps);
+    return MGC_OK;
+}
+
+// ---- scheduler -------------------------------------------------------------
+
+namespace {
+
+mgc_status need_sched(mgc_sim* s)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->sched) return fail(MGC_ERR_INVALID, "the step scheduler needs the fused deferred method (min delay >= 2)");
+    CK(cudaSetDevice(s->device));
+    return MGC_OK;
+}
+
+mgc_status read_sched(mgc_sim* s, SchedState* h)
+{
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(h, s->sched, sizeof(*h), cudaMemcpyDeviceToHost));
+    return MGC_OK;
+}
+
+// Least-squares line t = a + b*x.
+bool fit_line(const std::vector<double>& x, const std::vector<double>& t, double* a, double* b)
+{
+    const size_t n = x.size();
+    if (n < 2) return false;
+    double mx = 0, mt = 0;
+    for (size_t i = 0; i < n; ++i) {
+        mx += x[i];
+        mt += t[i];
+    }
+    mx /= n;
+    mt /= n;
+    double sxx = 0, sxt = 0;
+    for (size_t i = 0; i < n; ++i) {
+        sxx += (x[i] - mx) * (x[i] - mx);
+        sxt += (x[i] - mx) * (t[i] - mt);
+    }
+    *b = sxx > 0 ? sxt / sxx : 0.0;
+    *a = mt - *b * mx;
+    return true;
+}
+
+}  // namespace
+
+mgc_status mgc_sched_set_mode(mgc_sim* s, int32_t mode)
+{
+    CKS(need_sched(s));
+    if (mode < MGC_SCHED_STATIC || mode > MGC_SCHED_LEARNED) return fail(MGC_ERR_INVALID, "unknown schedule mode %d", mode);
+    SchedState h;
+    CKS(read_sched(s, &h));
+    if (mode == MGC_SCHED_LEARNED && !h.trained) return fail(MGC_ERR_INVALID, "the scheduler's network is not trained");
+    CKS(sched_put(s, &SchedState::have_prev, (int32_t)0));
+    CKS(sched_put(s, &SchedState::mode, mode));
+    return MGC_OK;
+}
+
+mgc_status mgc_sched_set_threshold(mgc_sim* s, double threshold, int32_t hi_variant)
+{
+    CKS(need_sched(s));
+    if (hi_variant < 0 || hi_variant > 1) return fail(MGC_ERR_INVALID, "variant must be 0 or 1");
+    CKS(sched_put(s, &SchedState::threshold, (float)threshold));
+    CKS(sched_put(s, &SchedState::hi_variant, hi_variant));
+    return MGC_OK;
+}
+
+mgc_status mgc_sched_collect(mgc_sim* s, int32_t on, int32_t reset)
+{
+    CKS(need_sched(s));
+    if (reset) CKS(sched_put(s, &SchedState::n_data, (int32_t)0));
+    CKS(sched_put(s, &SchedState::collect, (int32_t)(on != 0)));
+    return MGC_OK;
+}
+
+mgc_status mgc_sched_calibrate(mgc_sim* s, int32_t groups, double* threshold)
+{
+    CKS(need_sched(s));
+    if (groups < 4 || groups > kMaxDataset / 2) return fail(MGC_ERR_INVALID, "calibrate with 4..%d groups", kMaxDataset / 2);
+    SchedState h;
+    CKS(mgc_run(s, kGraphSteps));  // builds the step-group graph, settles the state
+    CKS(read_sched(s, &h));
+    if (!s->sched_graph) return fail(MGC_ERR_CUDA, "the step-group graph has no scheduler branch");
+    const int32_t collect0 = h.collect;
+    CKS(sched_put(s, &SchedState::collect, (int32_t)1));
+    if (h.n_data + groups + 2 > kMaxDataset) CKS(sched_put(s, &SchedState::n_data, (int32_t)0));
+    CKS(read_sched(s, &h));
+    const int32_t n0 = h.n_data;
+    std::vector<cudaEvent_t> ev(2 * (groups + 1));
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    std::vector<float> ms(groups + 1, 0.f);
+    mgc_status st = MGC_OK;
+    for (int g = 0; g <= groups && st == MGC_OK; ++g) {
+        st = sched_put(s, &SchedState::forced_variant, (int32_t)(g % 2));
+        if (st != MGC_OK) break;
+        cudaEventRecord(ev[2 * g], s->stream);
+        st = mgc_run(s, kGraphSteps);
+        cudaEventRecord(ev[2 * g + 1], s->stream);
+    }
+    if (st == MGC_OK) st = sched_put(s, &SchedState::forced_variant, (int32_t)-1);
+    if (st == MGC_OK && cudaStreamSynchronize(s->stream) != cudaSuccess) st = fail(MGC_ERR_CUDA, "calibration run failed");
+    for (int g = 0; g <= groups && st == MGC_OK; ++g) cudaEventElapsedTime(&ms[g], ev[2 * g], ev[2 * g + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (st != MGC_OK) return st;
+    // features of group g were recorded when group g+1 started
+    std::vector<float> rows((size_t)(groups + 1) * kTraceCols);
+    CK(cudaMemcpy(rows.data(), s->sched_data + (size_t)n0 * kTraceCols, rows.size() * sizeof(float),
+                  cudaMemcpyDeviceToHost));
+    std::vector<double> x[2], t[2];
+    for (int g = 0; g < groups; ++g) {
+        const double load = std::expm1((double)rows[(size_t)(g + 1) * kTraceCols + kTracePops]);
+        x[g % 2].push_back(load);
+        t[g % 2].push_back((double)ms[g] / kGraphSteps);
+    }
+    double a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+    fit_line(x[0], t[0], &a0, &b0);
+    fit_line(x[1], t[1], &a1, &b1);
+    double lo = 1e300, hi = -1e300, m0 = 0, m1 = 0;
+    for (int v = 0; v < 2; ++v)
+        for (size_t i = 0; i < x[v].size(); ++i) {
+            lo = std::min(lo, x[v][i]);
+            hi = std::max(hi, x[v][i]);
+            (v ? m1 : m0) += t[v][i] / x[v].size();
+        }
+    float thr = 1e30f;
+    int32_t hi_v = m0 <= m1 ? 1 : 0;  // with thr = inf: always the faster variant on average
+    if (b0 != b1) {
+        const double xc = (a1 - a0) / (b0 - b1);
+        if (xc > lo && xc < hi) {
+            thr = (float)xc;
+            hi_v = b1 < b0 ? 1 : 0;  // the flatter line wins at high load
+        }
+    }
+    CKS(sched_put(s, &SchedState::threshold, thr));
+    CKS(sched_put(s, &SchedState::hi_variant, hi_v));
+    CKS(sched_put(s, &SchedState::collect, collect0));
+    if (threshold) *threshold = thr;
+    return MGC_OK;
+}
+
+mgc_status mgc_sched_train(mgc_sim* s, int32_t epochs, float lr, uint64_t seed, float* loss)
+{
+    CKS(need_sched(s));
+    if (epochs < 1 || !(lr > 0.f)) return fail(MGC_ERR_INVALID, "bad training arguments");
+    SchedState h;
+    CKS(read_sched(s, &h));
+    const int n_rows = h.n_data;
+    const int n = n_rows - kGroupLag;
+    if (n < 16) return fail(MGC_ERR_INVALID, "%d recorded groups; training needs at least %d", n_rows, kGroupLag + 16);
+    std::vector<float> rows((size_t)n_rows * kTraceCols);
+    CK(cudaMemcpy(rows.data(), s->sched_data, rows.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    // windows: kGroupLag consecutive groups (oldest first) -> the next group
+    std::vector<float> X((size_t)n * kMlpIn), Y((size_t)n * kMlpOut);
+    for (int t = 0; t < n; ++t) {
+        for (int i = 0; i < kMlpIn; ++i) X[(size_t)t * kMlpIn + i] = rows[(size_t)t * kTraceCols + i];
+        for (int o = 0; o < kMlpOut; ++o) Y[(size_t)t * kMlpOut + o] = rows[(size_t)(t + kGroupLag) * kTraceCols + o];
+    }
+    auto standardize = [&](std::vector<float>& M, int cols, float* mean, float* sd) {
+        for (int c = 0; c < cols; ++c) {
+            double m = 0, v = 0;
+            for (int t = 0; t < n; ++t) m += M[(size_t)t * cols + c];
+            m /= n;
+            for (int t = 0; t < n; ++t) v += (M[(size_t)t * cols + c] - m) * (M[(size_t)t * cols + c] - m);
+            const double d = std::max(std::sqrt(v / n), 1e-3);
+            mean[c] = (float)m;
+            sd[c] = (float)d;
+            for (int t = 0; t < n; ++t) M[(size_t)t * cols + c] = (float)((M[(size_t)t * cols + c] - m) / d);
+        }
+    };
+    standardize(X, kMlpIn, h.xm, h.xs);
+    standardize(Y, kMlpOut, h.ym, h.ys);
+    // Glorot-uniform initial weights from the seed, zero biases
+    for (int k = 0; k < kMlpParams; ++k) {
+        const bool w1 = k < mlp_b1(), w2 = k >= mlp_w2() && k < mlp_b2();
+        const double lim = w1 ? std::sqrt(6.0 / (kMlpIn + kMlpHidden)) : std::sqrt(6.0 / (kMlpHidden + kMlpOut));
+        const U32x4 r = philox4x32_10((uint32_t)k, 0u, 0u, 0x4D4C5049u /* "MLPI" */, (uint32_t)seed, (uint32_t)(seed >> 32));
+        h.p[k] = (w1 || w2) ? (float)((2.0 * unit_open0(r.x) - 1.0) * lim) : 0.f;
+    }
+    h.trained = 0;
+    CK(cudaMemcpy(s->sched, &h, sizeof(h), cudaMemcpyHostToDevice));
+    DevTmp tx, ty, tl;
+    float *dX, *dY, *dl;
+    CKS(tmp_alloc(tx, &dX, X.size()));
+    CKS(tmp_alloc(ty, &dY, Y.size()));
+    CKS(tmp_alloc(tl, &dl, 1));
+    CK(cudaMemcpy(dX, X.data(), X.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dY, Y.data(), Y.size() * sizeof(float), cudaMemcpyHostToDevice));
+    k_mlp_train<<<1, 256, 0, s->stream>>>(s->sched, dX, dY, n, epochs, lr, seed, dl);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    float l = 0.f;
+    CK(cudaMemcpy(&l, dl, sizeof(float), cudaMemcpyDeviceToHost));
+    if (loss) *loss = l;
+    CKS(sched_put(s, &SchedState::trained, (int32_t)1));
+    return MGC_OK;
+}
+
+mgc_status mgc_sched_report(mgc_sim* s, mgc_sched_stats* r, int32_t reset)
+{
+    CKS(need_sched(s));
+    if (!r) return fail(MGC_ERR_INVALID, "null report");
+    SchedState h;
+    CKS(read_sched(s, &h));
+    memset(r, 0, sizeof(*r));
+    r->mode = h.mode;
+    r->trained = h.trained;
+    r->groups = h.groups;
+    r->misses = h.misses;
+    r->variant_groups[0] = h.variant_groups[0];
+    r->variant_groups[1] = h.variant_groups[1];
+    r->mean_abs_log_err = h.err_groups ? h.abs_log_err / (double)h.err_groups : 0.0;
+    r->threshold = h.threshold;
+    r->hi_variant = h.hi_variant;
+    r->static_variant = h.static_variant;
+    r->recorded_groups = h.n_data;
+    if (reset) {
+        h.groups = h.misses = h.err_groups = 0;
+        h.variant_groups[0] = h.variant_groups[1] = 0;
+        h.abs_log_err = 0.0;
+        h.have_prev = 0;
+        CK(cudaMemcpy(s->sched, &h, sizeof(h), cudaMemcpyHostToDevice));
+    }
+    return MGC_OK;
+}
+
+mgc_status mgc_mlp_gradient(int32_t device, const float* params, const float* x, const float* y, int32_t n, float* grad,
+                            float* loss)
+{
+    if (!params || !x || !y || !grad || !loss || n < 1 || n > kMaxGradSamples)
+        return fail(MGC_ERR_INVALID, "mgc_mlp_gradient: 1..%d samples", kMaxGradSamples);
+    CK(cudaSetDevice(device));
+    DevTmp tp, tx, ty, tg, tl;
+    float *dp, *dx, *dy, *dg, *dl;
+    CKS(tmp_alloc(tp, &dp, kMlpParams));
+    CKS(tmp_alloc(tx, &dx, (size_t)n * kMlpIn));
+    CKS(tmp_alloc(ty, &dy, (size_t)n * kMlpOut));
+    CKS(tmp_alloc(tg, &dg, kMlpParams));
+    CKS(tmp_alloc(tl, &dl, 1));
+    CK(cudaMemcpy(dp, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dx, x, sizeof(float) * n * kMlpIn, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dy, y, sizeof(float) * n * kMlpOut, cudaMemcpyHostToDevice));
+    k_mlp_gradient<<<1, 256>>>(dp, dx, dy, n, dg, dl);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(grad, dg, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(loss, dl, sizeof(float), cudaMemcpyDeviceToHost));
     return MGC_OK;
 }
 
