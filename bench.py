@@ -519,6 +519,85 @@ def run_sweep(a, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_sched(a, ws, rank, local):
+    """Step scheduler on a drive that alternates every 3 step groups (64
+    steps each) between 20 Hz and 200 Hz inputs, on the Brunel network at
+    --scale: the same steps under the static variant, the threshold rule and
+    the learned rule (trained on the GPU on the first groups' trace); rasters
+    compared, misses and wall time per mode reported.  The threshold comes
+    from mgc_sched_calibrate."""
+    import torch
+
+    import mgbrain_b200 as mgb
+    torch.cuda.set_device(local)
+    group, g_train, g_eval = 64, a.sched_train_groups, a.sched_eval_groups
+    w = workload(a.scale)
+    rate_hi = w["rate"].copy()
+    rate_hi[w["n_lif"]:] = NU_DRIVEN
+    pinned = {k: torch.empty(w["n"], dtype=torch.float32, pin_memory=True) for k in ("lo", "hi")}
+    pinned["lo"].numpy()[:] = w["rate"]
+    pinned["hi"].numpy()[:] = rate_hi
+    L = mgb.lib()
+    import ctypes as C
+
+    def drive(sim, g0, groups):
+        # rates for each group enqueued from pinned memory: no host sync
+        for g in range(g0, g0 + groups):
+            src = pinned["hi" if (g // 3) % 2 == 0 else "lo"]
+            mgb.capi.check(L.mgc_set_rates(sim._h, C.c_void_p(src.data_ptr()), w["n"]))
+            sim.run(group)
+
+    sims = {m: make_sim(w, local, seed=1, record=True) for m in ("static", "threshold", "learned")}
+    calib = sims["static"]
+    calib.run(group)
+    thr = calib.sched_calibrate(groups=16)
+    rep_c = calib.sched_report()
+    calib.close()
+    sims["static"] = make_sim(w, local, seed=1, record=True)
+    for sim in sims.values():
+        sim.run(group)
+        sim.sched_threshold(thr, rep_c["hi_variant"])
+        sim.sched_collect(True, reset=True)
+        drive(sim, 0, g_train)
+        sim.sched_collect(False)
+        sim.read_raster(max_steps=1 << 20, max_ids=w["n"] * 64)
+    t0 = time.perf_counter()
+    loss = sims["learned"].sched_train(epochs=400, lr=3e-3, seed=7)
+    train_s = time.perf_counter() - t0
+    sims["threshold"].sched_mode(mgb.SCHED_THRESHOLD)
+    sims["learned"].sched_mode(mgb.SCHED_LEARNED)
+    out = {}
+    rasters = {}
+    for m, sim in sims.items():
+        sim.sched_report(reset=True)
+        stream = torch.cuda.ExternalStream(sim.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        drive(sim, g_train, g_eval)
+        e1.record(stream)
+        e1.synchronize()
+        rep = sim.sched_report()
+        rasters[m] = sim.read_raster(max_steps=1 << 20, max_ids=w["n"] * 64)
+        out[m] = {"ms": e0.elapsed_time(e1), "groups": rep["groups"], "misses": rep["misses"],
+                  "miss_rate": rep["misses"] / rep["groups"] if rep["groups"] else None,
+                  "variant_groups": rep["variant_groups"]}
+        if m == "learned":
+            out[m]["mean_abs_log_err"] = rep["mean_abs_log_err"]
+    same = all(np.array_equal(rasters[m][1], rasters["static"][1]) and
+               np.array_equal(rasters[m][2], rasters["static"][2]) for m in rasters)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "step-schedule misses and wall time, periodic drive",
+            "config": {"workload": f"Brunel network at scale {a.scale}, inputs alternating 20/200 Hz every "
+                                   "3 groups of 64 steps", "train_groups": g_train, "eval_groups": g_eval},
+            "calibrated_threshold_events_per_step": thr, "hi_variant": rep_c["hi_variant"],
+            "train_loss": loss, "train_s": train_s, "modes": out, "rasters_identical": same,
+        }), flush=True)
+    for sim in sims.values():
+        sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -531,9 +610,11 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
-    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep"],
+    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched"],
                     help="brunel1m: the 1M-neuron network (default); sweep: batched vs plain "
-                         "parameter sweep")
+                         "parameter sweep; sched: the step scheduler's modes on a periodic drive")
+    ap.add_argument("--sched-train-groups", type=int, default=200)
+    ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--sweep-steps", type=int, default=2000)
     ap.add_argument("--kernel-profile", choices=["quiet", "driven"],
@@ -544,6 +625,8 @@ def main():
     try:
         if a.workload == "sweep":
             run_sweep(a, ws, rank, local)
+        elif a.workload == "sched":
+            run_sched(a, ws, rank, local)
         elif a.kernel_profile:
             w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
             sim = make_sim(w, local, seed=1, record=False)
