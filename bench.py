@@ -540,12 +540,16 @@ def run_sched(a, ws, rank, local):
     L = mgb.lib()
     import ctypes as C
 
-    def drive(sim, g0, groups):
+    def drive(sim, g0, groups, loads=None):
         # rates for each group enqueued from pinned memory: no host sync
+        # (unless the per-group loads are wanted)
         for g in range(g0, g0 + groups):
             src = pinned["hi" if (g // 3) % 2 == 0 else "lo"]
             mgb.capi.check(L.mgc_set_rates(sim._h, C.c_void_p(src.data_ptr()), w["n"]))
+            e0 = sim.info()["events"] if loads is not None else 0
             sim.run(group)
+            if loads is not None:
+                loads.append(((g // 3) % 2 == 0, (sim.info()["events"] - e0) / group))
 
     sims = {m: make_sim(w, local, seed=1, record=True) for m in ("static", "threshold", "learned")}
     calib = sims["static"]
@@ -554,11 +558,12 @@ def run_sched(a, ws, rank, local):
     rep_c = calib.sched_report()
     calib.close()
     sims["static"] = make_sim(w, local, seed=1, record=True)
-    for sim in sims.values():
+    loads = []
+    for m, sim in sims.items():
         sim.run(group)
         sim.sched_threshold(thr, rep_c["hi_variant"])
         sim.sched_collect(True, reset=True)
-        drive(sim, 0, g_train)
+        drive(sim, 0, g_train, loads if m == "static" else None)
         sim.sched_collect(False)
         sim.read_raster(max_steps=1 << 20, max_ids=w["n"] * 64)
     t0 = time.perf_counter()
@@ -584,6 +589,25 @@ def run_sched(a, ws, rank, local):
                   "variant_groups": rep["variant_groups"]}
         if m == "learned":
             out[m]["mean_abs_log_err"] = rep["mean_abs_log_err"]
+    # the same rule with its threshold between the two drive levels, where
+    # every change of the drive can make a decision miss
+    hi = float(np.median([x for h, x in loads if h]))
+    lo = float(np.median([x for h, x in loads if not h]))
+    thr_mid = float(np.sqrt(hi * lo))
+    imposed = {}
+    for m in ("threshold", "learned"):
+        sim = sims[m]
+        sim.sched_threshold(thr_mid, 1)
+        sim.sched_report(reset=True)
+        drive(sim, g_train + g_eval, g_eval)
+        rep = sim.sched_report()
+        imposed[m] = {"groups": rep["groups"], "misses": rep["misses"],
+                      "miss_rate": rep["misses"] / rep["groups"] if rep["groups"] else None}
+    sims["static"].sched_threshold(thr_mid, 1)
+    drive(sims["static"], g_train + g_eval, g_eval)
+    for m, sim in sims.items():
+        c, i = sim.read_raster(max_steps=1 << 20, max_ids=w["n"] * 64)[1:]
+        rasters[m] = (None, np.concatenate([rasters[m][1], c]), np.concatenate([rasters[m][2], i]))
     same = all(np.array_equal(rasters[m][1], rasters["static"][1]) and
                np.array_equal(rasters[m][2], rasters["static"][2]) for m in rasters)
     if rank == 0:
@@ -592,7 +616,9 @@ def run_sched(a, ws, rank, local):
             "config": {"workload": f"Brunel network at scale {a.scale}, inputs alternating 20/200 Hz every "
                                    "3 groups of 64 steps", "train_groups": g_train, "eval_groups": g_eval},
             "calibrated_threshold_events_per_step": thr, "hi_variant": rep_c["hi_variant"],
-            "train_loss": loss, "train_s": train_s, "modes": out, "rasters_identical": same,
+            "train_loss": loss, "train_s": train_s, "modes": out,
+            "imposed_threshold": {"events_per_step": thr_mid, "low_load": lo, "high_load": hi, "modes": imposed},
+            "rasters_identical": same,
         }), flush=True)
     for sim in sims.values():
         sim.close()

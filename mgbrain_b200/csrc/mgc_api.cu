@@ -98,6 +98,8 @@ struct mgc_sim {
     SchedState* sched = nullptr;      // device
     float* sched_data = nullptr;      // device [kMaxDataset][kTraceCols]
     bool sched_graph = false;         // the step-group graph branches on the scheduler's choice
+    int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
+    bool sched_collect_h = false, sched_forced_h = false;
 
     ~mgc_sim()
     {
@@ -743,6 +745,25 @@ mgc_status build_sched_graph(mgc_sim* s)
     return MGC_OK;
 }
 
+// The decision kernel and the SWITCH node are in the step-group graph only
+// while something needs them (an adaptive mode, recording, calibration);
+// otherwise the graph is the plain chain of the static variant's kernels.
+bool sched_wanted(const mgc_sim* s)
+{
+    return s->sched && (s->sched_mode_h != kSchedStatic || s->sched_collect_h || s->sched_forced_h);
+}
+
+mgc_status refresh_graph(mgc_sim* s)
+{
+    if (s->graph && s->sched_graph != sched_wanted(s)) {
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        s->sched_graph = false;
+    }
+    return MGC_OK;
+}
+
 mgc_status check_tbits(mgc_sim* s)
 {
     StepArgs& a = s->a;
@@ -1048,7 +1069,7 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         --left;
     }
     if (left >= kGraphSteps) {
-        if (!s->graph) CKS(s->fused && s->sched ? build_sched_graph(s) : build_graph(s));
+        if (!s->graph) CKS(sched_wanted(s) ? build_sched_graph(s) : build_graph(s));
         while (left >= s->graph_steps) {
             CK(cudaGraphLaunch(s->graph, s->stream));
             s->launches += (int64_t)s->graph_steps * kernels_per_step(s) + (s->sched_graph ? 1 : 0);
@@ -1457,7 +1478,8 @@ mgc_status mgc_sched_set_mode(mgc_sim* s, int32_t mode)
     if (mode == MGC_SCHED_LEARNED && !h.trained) return fail(MGC_ERR_INVALID, "the scheduler's network is not trained");
     CKS(sched_put(s, &SchedState::have_prev, (int32_t)0));
     CKS(sched_put(s, &SchedState::mode, mode));
-    return MGC_OK;
+    s->sched_mode_h = mode;
+    return refresh_graph(s);
 }
 
 mgc_status mgc_sched_set_threshold(mgc_sim* s, double threshold, int32_t hi_variant)
@@ -1474,7 +1496,8 @@ mgc_status mgc_sched_collect(mgc_sim* s, int32_t on, int32_t reset)
     CKS(need_sched(s));
     if (reset) CKS(sched_put(s, &SchedState::n_data, (int32_t)0));
     CKS(sched_put(s, &SchedState::collect, (int32_t)(on != 0)));
-    return MGC_OK;
+    s->sched_collect_h = on != 0;
+    return refresh_graph(s);
 }
 
 mgc_status mgc_sched_calibrate(mgc_sim* s, int32_t groups, double* threshold)
@@ -1482,6 +1505,8 @@ mgc_status mgc_sched_calibrate(mgc_sim* s, int32_t groups, double* threshold)
     CKS(need_sched(s));
     if (groups < 4 || groups > kMaxDataset / 2) return fail(MGC_ERR_INVALID, "calibrate with 4..%d groups", kMaxDataset / 2);
     SchedState h;
+    s->sched_forced_h = true;
+    CKS(refresh_graph(s));
     CKS(mgc_run(s, kGraphSteps));  // builds the step-group graph, settles the state
     CKS(read_sched(s, &h));
     if (!s->sched_graph) return fail(MGC_ERR_CUDA, "the step-group graph has no scheduler branch");
@@ -1502,6 +1527,8 @@ mgc_status mgc_sched_calibrate(mgc_sim* s, int32_t groups, double* threshold)
         cudaEventRecord(ev[2 * g + 1], s->stream);
     }
     if (st == MGC_OK) st = sched_put(s, &SchedState::forced_variant, (int32_t)-1);
+    s->sched_forced_h = false;
+    if (st == MGC_OK) st = refresh_graph(s);
     if (st == MGC_OK && cudaStreamSynchronize(s->stream) != cudaSuccess) st = fail(MGC_ERR_CUDA, "calibration run failed");
     for (int g = 0; g <= groups && st == MGC_OK; ++g) cudaEventElapsedTime(&ms[g], ev[2 * g], ev[2 * g + 1]);
     for (auto& e : ev) cudaEventDestroy(e);
