@@ -441,6 +441,12 @@ def split_raster(counts, ids, starts, steps):
     return out
 
 
+def rank_share(count, ws, rank):
+    """Indices of the independent units (sweep instances) rank `rank` of `ws`
+    advances: dealt round-robin, so every unit runs on exactly one rank."""
+    return [i for i in range(count) if i % ws == rank]
+
+
 def run_sweep(a, ws, rank, local):
     """Parameter sweep of independent Brunel instances (N log-uniform in
     [1e3, 1e5], K = min(N/10, 1000), g ~ U[3, 7], nu_ext ~ U[10, 30] Hz).
@@ -455,7 +461,7 @@ def run_sweep(a, ws, rank, local):
     from mgbrain_b200 import brunel
     torch.cuda.set_device(local)
     insts = brunel.sweep_instances(count=a.sweep_count)
-    mine = [p for i, p in enumerate(insts) if i % ws == rank]
+    mine = [insts[i] for i in rank_share(len(insts), ws, rank)]
     T = a.sweep_steps
     n_all = sum(brunel.sweep_block(p)["n"] for p in mine)
     steps_cap = T + 4096                     # also holds the autotuner's trial steps

@@ -439,7 +439,7 @@ mgc_status choose_mode(mgc_sim* s, int requested)
     const int dbits = D > 1 ? bits_for(D) : 0;
     const bool deferred_ok = !s->stdp && s->S > 0 && D <= kMaxBuckets &&
                              a.tbits + dbits <= 32 &&
-                             ((size_t)s->n * (size_t)D + 1) * sizeof(uint32_t) <= kMaxBucketBytes;
+                             ((size_t)s->n * (size_t)D + 1) * sizeof(int64_t) <= kMaxBucketBytes;
     if (requested == MGC_MODE_DEFERRED && !deferred_ok)
         return fail(MGC_ERR_INVALID, "deferred delivery needs static weights and <= %d delays", kMaxBuckets);
     // pull: explicit networks whose per-step pass over all synapses is
