@@ -122,6 +122,8 @@ typedef struct mgc_info {
     int32_t mode;
     int32_t graph_steps;       /* steps per captured CUDA graph */
     int64_t device_bytes;      /* device memory held by the handle */
+    int32_t persistent;        /* steps run as persistent step groups (cooperative launches) */
+    int32_t reserved;
 } mgc_info;
 
 /* Replaces MGSimulator::MGSimulator(Network&, std::vector<int>&, int)
@@ -195,7 +197,7 @@ typedef struct mgc_tune_report {
     int32_t trials;               /* configurations timed */
     int32_t chunk_len;            /* chosen synapses per delivery task (deferred method) */
     int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
-    int32_t reserved;
+    int32_t persistent;           /* 1: the fused method runs as persistent step groups */
     double ms_per_step;           /* time per step of the chosen configuration */
     double default_ms_per_step;   /* time per step of the builder's configuration */
     int64_t steps;                /* steps simulated by the trials */
@@ -203,12 +205,21 @@ typedef struct mgc_tune_report {
 
 /* Autotuner: times `steps_per_trial` steps (rounded up to whole graphs) of
  * each launch configuration — synapses per delivery task (the threads a
- * spike's delay segment gets) x resident blocks per SM of the step kernel —
- * starting with the builder's choice, and keeps the fastest.  The trials are
+ * spike's delay segment gets) x resident blocks per SM of the step kernel,
+ * then (fused method) the best of those as a persistent step group, one
+ * cooperative launch of up to 1024 steps with a bounded grid barrier between
+ * steps — starting with the builder's choice, and keeps the fastest.  The trials are
  * real steps: the simulation advances by report->steps.  The configuration
  * changes no result (it only changes which warp adds which synapse).  No
  * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
+
+/* Runs the fused method as persistent step groups (on != 0) or as CUDA
+ * graphs of single-step kernels (0, the default until the autotuner decides).
+ * Results are the same either way; while a schedule mode other than static,
+ * recording or calibration is on, graphs are used.  No reference
+ * counterpart. */
+mgc_status mgc_set_persistent(mgc_sim* sim, int32_t on);
 
 /* ---- Step scheduler (fused deferred method: minimum delay >= 2) ----------
  * Each CUDA graph of 64 steps starts with a decision kernel that picks which

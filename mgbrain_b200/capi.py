@@ -24,7 +24,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune", "mgc_sched_set_mode", "mgc_sched_set_threshold",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
 )
 
@@ -62,7 +62,7 @@ class FixedInDegreeDesc(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [
         ("trials", C.c_int32), ("chunk_len", C.c_int32), ("blocks_per_sm", C.c_int32),
-        ("reserved", C.c_int32), ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double),
+        ("persistent", C.c_int32), ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double),
         ("steps", C.c_int64),
     ]
 
@@ -81,7 +81,7 @@ class Info(C.Structure):
         ("n_neurons", C.c_int32), ("ring_len", C.c_int32), ("min_delay", C.c_int32),
         ("max_delay", C.c_int32), ("n_synapses", C.c_int64), ("step", C.c_int64),
         ("events", C.c_int64), ("mode", C.c_int32), ("graph_steps", C.c_int32),
-        ("device_bytes", C.c_int64),
+        ("device_bytes", C.c_int64), ("persistent", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -125,6 +125,8 @@ def lib():
     L.mgc_measure_scatter.restype = C.c_int
     L.mgc_autotune.argtypes = [vp, i64, C.POINTER(TuneReport)]
     L.mgc_autotune.restype = C.c_int
+    L.mgc_set_persistent.argtypes = [vp, i32]
+    L.mgc_set_persistent.restype = C.c_int
     L.mgc_sched_set_mode.argtypes = [vp, i32]
     L.mgc_sched_set_threshold.argtypes = [vp, C.c_double, i32]
     L.mgc_sched_calibrate.argtypes = [vp, i32, C.POINTER(C.c_double)]
@@ -334,7 +336,7 @@ class Simulator:
         steps advance the simulation (report["steps"] of them)."""
         r = TuneReport()
         check(lib().mgc_autotune(self._h, int(steps_per_trial), C.byref(r)))
-        return {k: getattr(r, k) for k, _ in TuneReport._fields_ if k != "reserved"}
+        return {k: getattr(r, k) for k, _ in TuneReport._fields_}
 
     # ---- step scheduler ---------------------------------------------------
     def sched_mode(self, mode):
@@ -362,6 +364,9 @@ class Simulator:
         d = {k: getattr(r, k) for k, _ in SchedStats._fields_ if k != "reserved"}
         d["variant_groups"] = [r.variant_groups[0], r.variant_groups[1]]
         return d
+
+    def set_persistent(self, on=True):
+        check(lib().mgc_set_persistent(self._h, int(bool(on))))
 
     def profile(self, steps):
         """Milliseconds spent in (neuron update, event push, STDP) over `steps`

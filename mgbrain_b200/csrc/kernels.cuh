@@ -34,7 +34,7 @@ namespace mgc {
 enum : int { kRAW = 0, kLIF0 = 1, kPOISSON = 2, kLIF = 3, kLIFE = 4, kLIFB = 5 };
 
 // Device status bits, read back by mgc_sync / mgc_read_raster.
-enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2 };
+enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2, kStatusBarrier = 4 };
 
 constexpr int kNeuronBlock = 256;
 constexpr int kPushBlock = 256;
@@ -116,6 +116,7 @@ struct StepArgs {
     const uint8_t* tpop;      // [ns] trace population of each neuron (< kTracePops)
     float* trace;             // [kTraceSteps][kTraceCols]
     unsigned long long* ev_mark;  // events counter at the previous step's end
+    unsigned int* bar;        // [2] grid barrier of the persistent step group: arrivals, generation
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
@@ -280,7 +281,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 // pass, one atomic per warp.
 template <int G, bool CUR>
 __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
-                                              int64_t warp, int64_t nwarps, int* pop_cnt = nullptr)
+                                              int64_t warp, int64_t nwarps, int64_t rbase, int* pop_cnt = nullptr)
 {
     static_assert(G == 1 || G == 2, "one or two groups per lane");
     const int lane = threadIdx.x & 31;
@@ -288,7 +289,6 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     int32_t* ids = step_ids(a, hslot);
     int32_t* cnt = step_count(a, hslot);
     const bool rec = (a.deferred || a.pull) && a.record;  // no push kernel to record
-    const int64_t rbase = rec ? *a.raster_pos : 0;
     for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
         char4 t4[G];
         float4 v4[G], e4[G], i4[G], ce4[G], ci4[G];
@@ -380,6 +380,12 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     }
 }
 
+// Raster position of the current step's first spike id (when this kernel records).
+__device__ __forceinline__ int64_t raster_base(const StepArgs& a)
+{
+    return (a.deferred || a.pull) && a.record ? *a.raster_pos : 0;
+}
+
 __device__ __forceinline__ float* acc_buf(const StepArgs& a, float* base, int64_t s)
 {
     return base + (size_t)(s & 1) * (size_t)a.ns;
@@ -400,9 +406,9 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     if (a.has_cur)
-        neuron_groups<1, true>(a, s, hslot, in_e, in_i, warp, nwarps);
+        neuron_groups<1, true>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
     else
-        neuron_groups<1, false>(a, s, hslot, in_e, in_i, warp, nwarps);
+        neuron_groups<1, false>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
@@ -526,19 +532,19 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
 // ---------------------------------------------------------------------------
 constexpr int kDeliverUnroll = 4;
 
-// History slot of step sa: the current slot advanced by (sa - s).
-__device__ __forceinline__ int32_t hist_slot(const StepArgs& a, int64_t sa)
+// History slot of step sa, given the current step s and its slot.
+__device__ __forceinline__ int32_t hist_slot(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot)
 {
-    int32_t hs = a.slots[1] + (int32_t)(sa - *a.step);
+    int32_t hs = hslot + (int32_t)(sa - s);
     return hs >= a.H ? hs - a.H : hs;
 }
 
 // pre[k] = spikes of the delays before bucket k that arrive at step sa
 // (pre[D] = tasks in all); run by the block's first warp.
-__device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, int64_t* pre)
+__device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot, int64_t* pre)
 {
     const int D = a.D;
-    const int32_t hs = hist_slot(a, sa);
+    const int32_t hs = hist_slot(a, sa, s, hslot);
     const int lane = threadIdx.x;
     int64_t carry = 0;
     if (lane == 0) pre[0] = 0;
@@ -561,11 +567,11 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 }
 
 // The tasks themselves, after deliver_prefix and a block barrier.
-__device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, const int64_t* pre, int64_t warp,
-                                              int64_t nwarps)
+__device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot,
+                                              const int64_t* pre, int64_t warp, int64_t nwarps)
 {
     const int D = a.D;
-    const int32_t hs = hist_slot(a, sa);
+    const int32_t hs = hist_slot(a, sa, s, hslot);
     const int CH = a.bucket_chunks;
     const int64_t total = pre[D] * CH;  // (spike, delay) segments x chunks
     float* acc_e = acc_buf(a, a.acc_e, sa);
@@ -644,9 +650,11 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, con
 __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
                                                  int64_t nwarps)
 {
-    if (threadIdx.x < 32) deliver_prefix(a, sa, pre);
+    const int64_t s = *a.step;
+    const int32_t hslot = a.slots[1];
+    if (threadIdx.x < 32) deliver_prefix(a, sa, s, hslot, pre);
     __syncthreads();
-    deliver_tasks(a, sa, pre, warp, nwarps);
+    deliver_tasks(a, sa, s, hslot, pre, warp, nwarps);
 }
 
 // Arrivals of the current step (used when the minimum delay is one step).
@@ -677,14 +685,119 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_fused(StepArgs a)
     __syncthreads();
     // the first warp sums the spike counts per delay while all warps update
     // their neurons; the barrier then publishes the sums for the delivery
-    if (threadIdx.x < 32) deliver_prefix(a, s + 1, pre);
-    neuron_groups<2, CUR>(a, s, a.slots[1], acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+    const int32_t hslot = a.slots[1];
+    if (threadIdx.x < 32) deliver_prefix(a, s + 1, s, hslot, pre);
+    neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, raster_base(a),
                           a.trace ? pop_cnt : nullptr);
     __syncthreads();
     if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
         atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
-    deliver_tasks(a, s + 1, pre, warp, nwarps);
+    deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent step group: the fused step for `nsteps` consecutive steps in
+// one cooperative launch (all blocks resident), a grid barrier between
+// steps.  Step, slots and raster position live in registers; block 0 keeps
+// the bookkeeping the epilogue does (clearing the next history slot during
+// the step, which no delivery of this step reads; recording the finished
+// step after the barrier) and writes the clock back at the end.  Every
+// barrier wait is bounded: on time-out the kernel sets kStatusBarrier and
+// all blocks return.
+// ---------------------------------------------------------------------------
+constexpr unsigned int kBarrierSpins = 1u << 21;
+
+__device__ __forceinline__ bool grid_barrier(const StepArgs& a, int* abort_flag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int* gen = a.bar + 1;
+        const unsigned int g0 = *gen;
+        __threadfence();
+        if (atomicAdd(a.bar, 1u) == gridDim.x - 1) {
+            atomicExch(a.bar, 0u);
+            __threadfence();
+            atomicAdd(a.bar + 1, 1u);  // release the others
+        } else {
+            unsigned int it = 0;
+            while (*gen == g0) {
+                if (++it > kBarrierSpins) {
+                    atomicOr(a.status, kStatusBarrier);
+                    *abort_flag = 1;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *abort_flag == 0;
+}
+
+template <bool CUR, int MINB>
+__global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t nsteps)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    __shared__ int pop_cnt[kTracePops];
+    __shared__ int abort_flag;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    int64_t s = *a.step;
+    int32_t slot = a.slots[0], hslot = a.slots[1];
+    int64_t rbase = a.record ? *a.raster_pos : 0;
+    const int64_t rstep0 = *a.raster_step0;
+    if (threadIdx.x == 0) abort_flag = 0;
+    for (int32_t i = 0; i < nsteps; ++i) {
+        const int32_t next_h = hslot + 1 == a.H ? 0 : hslot + 1;
+        if (lead) {
+            a.hist_cnt[next_h] = 0;  // step s+1's slot held step s+1-H; no delivery of step s reads it
+            if (a.trace) {
+                float* nxt = a.trace + ((s + 1) & (kTraceSteps - 1)) * kTraceCols;
+                for (int c = 0; c < kTraceCols; ++c) nxt[c] = 0.f;
+            }
+        }
+        if (threadIdx.x < kTracePops) pop_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        if (threadIdx.x < 32) deliver_prefix(a, s + 1, s, hslot, pre);
+        neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+                              a.record ? rbase : 0, a.trace ? pop_cnt : nullptr);
+        __syncthreads();
+        if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
+            atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
+        deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps);
+        if (!grid_barrier(a, &abort_flag)) return;
+        // step s is complete on every block
+        const int32_t nspk = *(volatile int32_t*)(a.hist_cnt + hslot);
+        if (lead) {
+            if (a.record) {
+                const int64_t idx = s - rstep0;
+                if (idx < a.raster_steps_cap)
+                    a.raster_counts[idx] = nspk;
+                else
+                    atomicOr(a.status, kStatusRasterSteps);
+                if (rbase + nspk > a.raster_ids_cap) atomicOr(a.status, kStatusRasterIds);
+            }
+            if (a.trace) {
+                const unsigned long long ev = *(volatile unsigned long long*)a.events;
+                a.trace[(s & (kTraceSteps - 1)) * kTraceCols + kTracePops] = (float)(ev - *a.ev_mark);
+                *a.ev_mark = ev;
+            }
+        }
+        if (a.record) rbase += nspk;
+        s += 1;
+        hslot = next_h;
+        slot = slot + 1 == a.M ? 0 : slot + 1;
+    }
+    if (lead) {
+        if (a.record) *a.raster_pos = rbase;
+        a.slots[0] = slot;
+        a.slots[1] = hslot;
+        __threadfence();
+        *a.step = s;
+    }
 }
 
 // ---------------------------------------------------------------------------

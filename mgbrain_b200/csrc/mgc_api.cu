@@ -98,6 +98,7 @@ struct mgc_sim {
     SchedState* sched = nullptr;      // device
     float* sched_data = nullptr;      // device [kMaxDataset][kTraceCols]
     bool sched_graph = false;         // the step-group graph branches on the scheduler's choice
+    bool persistent = false;          // fused method as one cooperative launch per step group
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
 
@@ -509,6 +510,16 @@ StepKernel fused_kernel(const mgc_sim* s, int v)
     return v == 0 ? k_fused<false, 2> : k_fused<false, 3>;
 }
 
+// The persistent step-group kernel of the same variant.
+using GroupKernel = void (*)(StepArgs, int32_t);
+GroupKernel steps_kernel(const mgc_sim* s, int v)
+{
+    if (s->a.has_cur) return v == 0 ? k_steps<true, 2> : k_steps<true, 3>;
+    return v == 0 ? k_steps<false, 2> : k_steps<false, 3>;
+}
+
+constexpr int32_t kPersistentSteps = 1024;  // steps per cooperative launch
+
 // Trace buffers and scheduler state of the fused method.  Trace population
 // of a neuron: as the builder set it (population index, or neuron type class
 // for synapse-list networks), clamped to kTracePops - 1.
@@ -523,6 +534,7 @@ mgc_status init_sched(mgc_sim* s)
     a.tpop = d_tp;
     CKS(s->alloc(&a.trace, (size_t)kTraceSteps * kTraceCols));
     CKS(s->alloc(&a.ev_mark, 1));
+    CKS(s->alloc(&a.bar, 2));
     CKS(s->alloc(&s->sched, 1));
     CKS(s->alloc(&s->sched_data, (size_t)kMaxDataset * kTraceCols));
     SchedState h;
@@ -1068,6 +1080,20 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         CKS(enqueue_step(s));  // catches up the delivery, leaves ahead = true
         --left;
     }
+    if (s->persistent && s->fused && !sched_wanted(s)) {
+        // one cooperative launch per group: every block resident, a grid
+        // barrier between steps instead of a launch
+        while (left > 0) {
+            int32_t n = (int32_t)std::min<int64_t>(left, kPersistentSteps);
+            void* args[] = {&s->a, &n};
+            CK(cudaMemsetAsync(s->a.bar, 0, 2 * sizeof(unsigned int), s->stream));  // a clean barrier
+            CK(cudaLaunchCooperativeKernel((const void*)steps_kernel(s, s->fused_variant), dim3(s->fused_grid),
+                                           dim3(kPushBlock), args, 0, s->stream));
+            s->launches += 1;
+            left -= n;
+        }
+        return MGC_OK;
+    }
     if (left >= kGraphSteps) {
         if (!s->graph) CKS(sched_wanted(s) ? build_sched_graph(s) : build_graph(s));
         while (left >= s->graph_steps) {
@@ -1087,6 +1113,7 @@ mgc_status mgc_sync(mgc_sim* s)
     CK(cudaStreamSynchronize(s->stream));
     int32_t st = 0;
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
+    if (st & kStatusBarrier) return fail(MGC_ERR_CUDA, "a grid barrier of the persistent step group timed out");
     if (st) return fail(MGC_ERR_OVERFLOW, "raster buffer overflow (status %d)", st);
     return MGC_OK;
 }
@@ -1215,6 +1242,7 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->mode = s->mode;
     info->graph_steps = s->graph_steps ? s->graph_steps : kGraphSteps;
     info->device_bytes = (int64_t)s->bytes;
+    info->persistent = s->persistent && s->fused && !sched_wanted(s);
     return MGC_OK;
 }
 
@@ -1355,6 +1383,14 @@ mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
 
 }  // namespace
 
+mgc_status mgc_set_persistent(mgc_sim* s, int32_t on)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (on && !s->fused) return fail(MGC_ERR_INVALID, "persistent step groups need the fused deferred method");
+    s->persistent = on != 0;
+    return MGC_OK;
+}
+
 mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* rep)
 {
     if (!s || !rep || steps_per_trial < 1) return fail(MGC_ERR_INVALID, "bad autotune arguments");
@@ -1414,6 +1450,28 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
             best_i = i;
         }
         rep->trials += 1;
+    }
+    if (st == MGC_OK && s->fused && !sched_wanted(s)) {
+        // the best shape once more as a persistent step group
+        st = apply_cand(s, cands[best_i], sms);
+        s->persistent = true;
+        if (st == MGC_OK) st = mgc_run(s, kGraphSteps);
+        if (st == MGC_OK) {
+            cudaEventRecord(e0, s->stream);
+            st = mgc_run(s, steps);
+            cudaEventRecord(e1, s->stream);
+        }
+        float ms = 0.f;
+        if (st == MGC_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+            const double per = (double)ms / (double)steps;
+            rep->trials += 1;
+            if (per < best) {
+                best = per;
+                rep->persistent = 1;
+            }
+        }
+        if (st == MGC_OK) st = mgc_sync(s);
+        s->persistent = rep->persistent != 0;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
