@@ -122,7 +122,7 @@ typedef struct mgc_info {
     int32_t mode;
     int32_t graph_steps;       /* steps per captured CUDA graph */
     int64_t device_bytes;      /* device memory held by the handle */
-    int32_t persistent;        /* steps run as persistent step groups (cooperative launches) */
+    int32_t persistent;        /* steps run as step groups: 0 no (graphs), 1 barrier per step, 2 pipelined */
     int32_t reserved;
 } mgc_info;
 
@@ -197,7 +197,7 @@ typedef struct mgc_tune_report {
     int32_t trials;               /* configurations timed */
     int32_t chunk_len;            /* chosen synapses per delivery task (deferred method) */
     int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
-    int32_t persistent;           /* 1: the fused method runs as persistent step groups */
+    int32_t persistent;           /* chosen step-group mode of the fused method (mgc_set_persistent) */
     double ms_per_step;           /* time per step of the chosen configuration */
     double default_ms_per_step;   /* time per step of the builder's configuration */
     int64_t steps;                /* steps simulated by the trials */
@@ -214,12 +214,16 @@ typedef struct mgc_tune_report {
  * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 
-/* Runs the fused method as persistent step groups (on != 0) or as CUDA
- * graphs of single-step kernels (0, the default until the autotuner decides).
- * Results are the same either way; while a schedule mode other than static,
- * recording or calibration is on, graphs are used.  No reference
+/* How the fused method runs: 0 CUDA graphs of single-step kernels (the
+ * default until the autotuner decides); 1 cooperative step groups of up to
+ * 1024 steps with a grid barrier between steps; 2 pipelined step groups
+ * (minimum delay >= 4): during step s each block delivers the arrivals of
+ * step s+2 and waits only until every block has finished step s-2.
+ * Results are the same in every mode; while a schedule mode other than
+ * static, recording or calibration is on, graphs are used.  All waits are
+ * bounded (a time-out makes mgc_sync return MGC_ERR_CUDA).  No reference
  * counterpart. */
-mgc_status mgc_set_persistent(mgc_sim* sim, int32_t on);
+mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
 
 /* ---- Step scheduler (fused deferred method: minimum delay >= 2) ----------
  * Each CUDA graph of 64 steps starts with a decision kernel that picks which

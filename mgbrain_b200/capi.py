@@ -365,8 +365,10 @@ class Simulator:
         d["variant_groups"] = [r.variant_groups[0], r.variant_groups[1]]
         return d
 
-    def set_persistent(self, on=True):
-        check(lib().mgc_set_persistent(self._h, int(bool(on))))
+    def set_persistent(self, mode=1):
+        """0: CUDA graphs of single-step kernels; 1: cooperative step groups
+        with a grid barrier per step; 2: pipelined step groups."""
+        check(lib().mgc_set_persistent(self._h, int(mode)))
 
     def profile(self, steps):
         """Milliseconds spent in (neuron update, event push, STDP) over `steps`

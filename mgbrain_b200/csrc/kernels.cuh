@@ -116,7 +116,8 @@ struct StepArgs {
     const uint8_t* tpop;      // [ns] trace population of each neuron (< kTracePops)
     float* trace;             // [kTraceSteps][kTraceCols]
     unsigned long long* ev_mark;  // events counter at the previous step's end
-    unsigned int* bar;        // [2] grid barrier of the persistent step group: arrivals, generation
+    unsigned int* bar;        // [4] step-group barriers: arrivals + generation (k_steps),
+                              //     phase arrival counters (k_pipe)
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
@@ -281,14 +282,15 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 // pass, one atomic per warp.
 template <int G, bool CUR>
 __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
-                                              int64_t warp, int64_t nwarps, int64_t rbase, int* pop_cnt = nullptr)
+                                              int64_t warp, int64_t nwarps, int64_t rbase, int* pop_cnt = nullptr,
+                                              bool raster = true)
 {
     static_assert(G == 1 || G == 2, "one or two groups per lane");
     const int lane = threadIdx.x & 31;
     const int64_t ngroups = a.ns >> 2;
     int32_t* ids = step_ids(a, hslot);
     int32_t* cnt = step_count(a, hslot);
-    const bool rec = (a.deferred || a.pull) && a.record;  // no push kernel to record
+    const bool rec = raster && (a.deferred || a.pull) && a.record;  // no push kernel to record
     for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
         char4 t4[G];
         float4 v4[G], e4[G], i4[G], ce4[G], ci4[G];
@@ -386,9 +388,14 @@ __device__ __forceinline__ int64_t raster_base(const StepArgs& a)
     return (a.deferred || a.pull) && a.record ? *a.raster_pos : 0;
 }
 
+// Accumulator buffer of the input arriving at step s: four buffers, so the
+// pipelined step group can deliver two steps ahead while the oldest buffer
+// is still being read.
+constexpr int kAccBuffers = 4;
+
 __device__ __forceinline__ float* acc_buf(const StepArgs& a, float* base, int64_t s)
 {
-    return base + (size_t)(s & 1) * (size_t)a.ns;
+    return base + (size_t)(s & (kAccBuffers - 1)) * (size_t)a.ns;
 }
 
 __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
@@ -797,6 +804,130 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
         a.slots[1] = hslot;
         __threadfence();
         *a.step = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined step group (minimum delay >= 4): during step s every block
+// updates its neurons of step s and delivers the arrivals of step s+2 (they
+// depend only on spikes of steps <= s-2), so a block waits only until every
+// block has finished step s-2 — an arrive/wait barrier split across two
+// steps instead of a full barrier per step.  The accumulators rotate over
+// four buffers: step s+2's is the one step s-2 read and cleared.  The
+// history holds H >= max delay + 3 steps so the slot cleared for step s+2
+// is read by no delivery still running.  Block 0 copies finished steps'
+// spike ids from the history into the raster two steps behind.  The
+// prologue delivers the arrivals of step s0+1; the last deliveries are those
+// of the group's last step + 1 - 1, so the group ends in the state the
+// single-step kernels start from.  Waits are bounded (kStatusBarrier).
+//
+// Phases: 0 is the prologue, k >= 1 is iteration k-1.  Blocks are never
+// more than two phases apart (a block in iteration i waited for phase i-1),
+// so four arrival counters used round-robin keep phases apart: counter
+// p % 4 has counted nb per earlier use when phase p completes, and the next
+// phase that uses it (p + 4) starts only after phase p + 2 completed.
+// ---------------------------------------------------------------------------
+constexpr int kPhaseCounters = 4;
+
+__device__ __forceinline__ bool wait_phase(const StepArgs& a, int32_t phase, int* abort_flag)
+{
+    if (threadIdx.x == 0) {
+        volatile unsigned int* arrived = a.bar + (phase % kPhaseCounters);
+        const unsigned int target = gridDim.x * (unsigned int)(phase / kPhaseCounters + 1);
+        unsigned int it = 0;
+        while (*arrived < target) {
+            if (++it > kBarrierSpins) {
+                atomicOr(a.status, kStatusBarrier);
+                *abort_flag = 1;
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *abort_flag == 0;
+}
+
+__device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(a.bar + (phase % kPhaseCounters), 1u);
+    }
+}
+
+// Block 0 copies the spike ids of finished step sc into the raster.
+__device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0, int64_t& rbase)
+{
+    const int32_t cnt = *(volatile int32_t*)(a.hist_cnt + hs);
+    const int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n;
+    for (int32_t j = threadIdx.x; j < cnt; j += blockDim.x)
+        if (rbase + j < a.raster_ids_cap) a.raster_ids[rbase + j] = ids[j];
+    if (threadIdx.x == 0) {
+        const int64_t idx = sc - rstep0;
+        if (idx < a.raster_steps_cap)
+            a.raster_counts[idx] = cnt;
+        else
+            atomicOr(a.status, kStatusRasterSteps);
+        if (rbase + cnt > a.raster_ids_cap) atomicOr(a.status, kStatusRasterIds);
+    }
+    rbase += cnt;
+}
+
+template <bool CUR, int MINB>
+__global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t nsteps)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    __shared__ int abort_flag;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const int64_t s0 = *a.step;
+    const int32_t slot0 = a.slots[0], h0 = a.slots[1];
+    const bool rec = a.record != 0;
+    int64_t rbase = rec ? *a.raster_pos : 0;
+    const int64_t rstep0 = *a.raster_step0;
+    const int64_t s_end = s0 + nsteps;
+    auto hs_of = [&](int64_t x) { return (int32_t)((h0 + (x - s0)) % a.H); };
+    if (threadIdx.x == 0) abort_flag = 0;
+    // prologue: arrivals of step s0+1; the slot of step s0+1 cleared
+    if (lead) a.hist_cnt[hs_of(s0 + 1)] = 0;
+    __syncthreads();
+    if (nsteps > 0) {
+        if (threadIdx.x < 32) deliver_prefix(a, s0 + 1, s0, h0, pre);
+        __syncthreads();
+        deliver_tasks(a, s0 + 1, s0, h0, pre, warp, nwarps);
+    }
+    arrive(a, 0);
+    for (int32_t i = 0; i < nsteps; ++i) {
+        const int64_t s = s0 + i;
+        const int32_t hs = hs_of(s);
+        // every block has finished step s-2 (phase i-1; for i = 1 the prologue)
+        if (i >= 1 && !wait_phase(a, i - 1, &abort_flag)) return;
+        if (lead && s + 2 <= s_end) a.hist_cnt[hs_of(s + 2)] = 0;
+        if (rec && blockIdx.x == 0 && i >= 2) raster_copy(a, s - 2, hs_of(s - 2), rstep0, rbase);
+        const bool deliver = s + 2 <= s_end;
+        if (deliver && threadIdx.x < 32) deliver_prefix(a, s + 2, s, hs, pre);
+        neuron_groups<2, CUR>(a, s, hs, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, 0, nullptr,
+                              false);
+        __syncthreads();
+        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps);
+        arrive(a, i + 1);
+    }
+    // the group's last steps: all blocks done (phases n-1 and n), remaining raster, the clock
+    if (nsteps >= 1 && !wait_phase(a, nsteps - 1, &abort_flag)) return;
+    if (!wait_phase(a, nsteps, &abort_flag)) return;
+    if (rec && blockIdx.x == 0)
+        for (int64_t x = (nsteps >= 2 ? s_end - 2 : s0); x < s_end; ++x) raster_copy(a, x, hs_of(x), rstep0, rbase);
+    if (lead) {
+        if (rec) *a.raster_pos = rbase;
+        if (a.trace) *a.ev_mark = *(volatile unsigned long long*)a.events;  // no trace rows here
+        a.slots[0] = (int32_t)((slot0 + nsteps) % a.M);
+        a.slots[1] = hs_of(s_end);
+        __threadfence();
+        *a.step = s_end;
     }
 }
 

@@ -98,7 +98,9 @@ struct mgc_sim {
     SchedState* sched = nullptr;      // device
     float* sched_data = nullptr;      // device [kMaxDataset][kTraceCols]
     bool sched_graph = false;         // the step-group graph branches on the scheduler's choice
-    bool persistent = false;          // fused method as one cooperative launch per step group
+    int persistent = 0;               // fused method as cooperative step groups: 1 barrier per
+                                      // step, 2 pipelined (min delay >= 4)
+    int group_grid_v[2][2] = {{1, 1}, {1, 1}};  // [persistent-1][variant] co-resident grids
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
 
@@ -468,7 +470,7 @@ mgc_status choose_mode(mgc_sim* s, int requested)
         a.deferred = 1;
         a.D = D;
         a.dmin = s->dmin;
-        a.H = s->dmax + 1;
+        a.H = s->dmax + 3;  // + 2: the pipelined step group clears a slot two steps ahead
     }
     return MGC_OK;
 }
@@ -510,10 +512,15 @@ StepKernel fused_kernel(const mgc_sim* s, int v)
     return v == 0 ? k_fused<false, 2> : k_fused<false, 3>;
 }
 
-// The persistent step-group kernel of the same variant.
+// The step-group kernels of the same variant: p = 1 one barrier per step,
+// p = 2 pipelined.
 using GroupKernel = void (*)(StepArgs, int32_t);
-GroupKernel steps_kernel(const mgc_sim* s, int v)
+GroupKernel steps_kernel(const mgc_sim* s, int p, int v)
 {
+    if (p == 2) {
+        if (s->a.has_cur) return v == 0 ? k_pipe<true, 2> : k_pipe<true, 3>;
+        return v == 0 ? k_pipe<false, 2> : k_pipe<false, 3>;
+    }
     if (s->a.has_cur) return v == 0 ? k_steps<true, 2> : k_steps<true, 3>;
     return v == 0 ? k_steps<false, 2> : k_steps<false, 3>;
 }
@@ -534,7 +541,7 @@ mgc_status init_sched(mgc_sim* s)
     a.tpop = d_tp;
     CKS(s->alloc(&a.trace, (size_t)kTraceSteps * kTraceCols));
     CKS(s->alloc(&a.ev_mark, 1));
-    CKS(s->alloc(&a.bar, 2));
+    CKS(s->alloc(&a.bar, 4));
     CKS(s->alloc(&s->sched, 1));
     CKS(s->alloc(&s->sched_data, (size_t)kMaxDataset * kTraceCols));
     SchedState h;
@@ -604,8 +611,8 @@ mgc_status finish_build(mgc_sim* s)
         s->max_gap = (int64_t)gap;
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
-        CKS(s->alloc(&a.acc_e, 2 * (size_t)a.ns));  // two step buffers
-        CKS(s->alloc(&a.acc_i, 2 * (size_t)a.ns));
+        CKS(s->alloc(&a.acc_e, kAccBuffers * (size_t)a.ns));  // step buffers, s % kAccBuffers
+        CKS(s->alloc(&a.acc_i, kAccBuffers * (size_t)a.ns));
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_deliver, kPushBlock, 0));
         s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
         // fused step kernel: one resident wave, every warp updates then delivers
@@ -616,7 +623,14 @@ mgc_status finish_build(mgc_sim* s)
         }
         s->fused_variant = 1;
         s->fused_grid = s->fused_grid_v[1];
-        if (s->fused) CKS(init_sched(s));
+        if (s->fused) {
+            for (int p = 1; p <= 2; ++p)
+                for (int v = 0; v < 2; ++v) {
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, p, v), kPushBlock, 0));
+                    s->group_grid_v[p - 1][v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+                }
+            CKS(init_sched(s));
+        }
     } else {
         a.M = s->M;
         CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns));
@@ -1082,12 +1096,13 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
     }
     if (s->persistent && s->fused && !sched_wanted(s)) {
         // one cooperative launch per group: every block resident, a grid
-        // barrier between steps instead of a launch
+        // barrier between steps (or the pipelined arrive/wait) instead of a launch
+        const int p = s->persistent, v = s->fused_variant;
         while (left > 0) {
             int32_t n = (int32_t)std::min<int64_t>(left, kPersistentSteps);
             void* args[] = {&s->a, &n};
-            CK(cudaMemsetAsync(s->a.bar, 0, 2 * sizeof(unsigned int), s->stream));  // a clean barrier
-            CK(cudaLaunchCooperativeKernel((const void*)steps_kernel(s, s->fused_variant), dim3(s->fused_grid),
+            CK(cudaMemsetAsync(s->a.bar, 0, 4 * sizeof(unsigned int), s->stream));  // clean barriers
+            CK(cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(s->group_grid_v[p - 1][v]),
                                            dim3(kPushBlock), args, 0, s->stream));
             s->launches += 1;
             left -= n;
@@ -1242,7 +1257,7 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->mode = s->mode;
     info->graph_steps = s->graph_steps ? s->graph_steps : kGraphSteps;
     info->device_bytes = (int64_t)s->bytes;
-    info->persistent = s->persistent && s->fused && !sched_wanted(s);
+    info->persistent = s->fused && !sched_wanted(s) ? s->persistent : 0;
     return MGC_OK;
 }
 
@@ -1383,11 +1398,13 @@ mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
 
 }  // namespace
 
-mgc_status mgc_set_persistent(mgc_sim* s, int32_t on)
+mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
 {
     if (!s) return fail(MGC_ERR_INVALID, "null handle");
-    if (on && !s->fused) return fail(MGC_ERR_INVALID, "persistent step groups need the fused deferred method");
-    s->persistent = on != 0;
+    if (mode < 0 || mode > 2) return fail(MGC_ERR_INVALID, "step-group mode %d (0, 1 or 2)", mode);
+    if (mode && !s->fused) return fail(MGC_ERR_INVALID, "step groups need the fused deferred method");
+    if (mode == 2 && s->dmin < 4) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
+    s->persistent = mode;
     return MGC_OK;
 }
 
@@ -1451,10 +1468,11 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
         }
         rep->trials += 1;
     }
-    if (st == MGC_OK && s->fused && !sched_wanted(s)) {
-        // the best shape once more as a persistent step group
+    for (int p = 1; p <= 2 && st == MGC_OK && s->fused && !sched_wanted(s); ++p) {
+        // the best shape once more as a step group (p = 2: pipelined)
+        if (p == 2 && s->dmin < 4) break;
         st = apply_cand(s, cands[best_i], sms);
-        s->persistent = true;
+        s->persistent = p;
         if (st == MGC_OK) st = mgc_run(s, kGraphSteps);
         if (st == MGC_OK) {
             cudaEventRecord(e0, s->stream);
@@ -1467,12 +1485,12 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
             rep->trials += 1;
             if (per < best) {
                 best = per;
-                rep->persistent = 1;
+                rep->persistent = p;
             }
         }
         if (st == MGC_OK) st = mgc_sync(s);
-        s->persistent = rep->persistent != 0;
     }
+    s->persistent = rep->persistent;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != MGC_OK) return st;

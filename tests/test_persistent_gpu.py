@@ -1,6 +1,7 @@
-"""Persistent step groups (one cooperative launch per group, grid barrier
-between steps) give the rasters and state of the graph path, also when the
-two are mixed and the step count is no multiple of anything."""
+"""Step groups (one cooperative launch per group: a grid barrier between
+steps, or the pipelined arrive/wait two steps apart) give the rasters and
+state of the graph path, also when the modes are mixed and the step counts
+are no multiple of anything."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,8 @@ def make(nu):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("nu", [0.002, 0.02])
-def test_persistent_equals_graphs(nu):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_step_groups_equal_graphs(nu, mode):
     ref = make(nu)
     ref.run(3001)
     _, cr, ir = ref.read_raster()
@@ -26,13 +28,18 @@ def test_persistent_equals_graphs(nu):
     ref.close()
 
     sim = make(nu)
-    sim.set_persistent(True)
+    sim.set_persistent(mode)
     sim.run(1000)
-    assert sim.info()["persistent"] == 1
-    sim.set_persistent(False)
+    assert sim.info()["persistent"] == mode
+    sim.set_persistent(0)
     sim.run(37)
-    sim.set_persistent(True)
-    sim.run(1964)
+    sim.set_persistent(mode)
+    sim.run(1)
+    sim.run(2)
+    sim.set_persistent(3 - mode)
+    sim.run(5)
+    sim.set_persistent(mode)
+    sim.run(1956)
     sim.sync()
     _, c, i = sim.read_raster()
     assert sim.info()["step"] == 3001
@@ -40,4 +47,15 @@ def test_persistent_equals_graphs(nu):
     assert np.array_equal(sim.state()["V"], vr)
     assert sim.info()["events"] == ev
     assert c.sum() > 0
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_pipelined_needs_min_delay_four():
+    w = bench.workload(scale=0.03)
+    projs = [(s, t, k, wt, 2, 5) for (s, t, k, wt, _, _) in w["projs"]]
+    sim = mgb.Simulator.fixed_indegree(w["pops"], projs, w["lif"], rate=w["rate"], v_init=w["v0"], conn_seed=4)
+    sim.set_persistent(1)
+    with pytest.raises(mgb.MgcError):
+        sim.set_persistent(2)
     sim.close()
