@@ -291,7 +291,11 @@ def run_ours(a, ws, rank, local):
     sim = make_sim(w, local, seed=1 + rank, record=False)
     build_s = time.perf_counter() - t0
     info = sim.info()
-    tune = sim.autotune(steps_per_trial=640)   # launch shape by measurement
+    if a.no_autotune:
+        tune = None
+        sim.set_persistent(a.group_mode)
+    else:
+        tune = sim.autotune(steps_per_trial=640)   # launch shape by measurement
     for _ in range(a.warmup):
         sim.run(CHUNK)
     sim.sync()
@@ -320,12 +324,15 @@ def run_ours(a, ws, rank, local):
         v["frac"] = v["achieved_gbs"] / hbm
         v["share"] = kms[0 if k_ == "neuron_update" else 1] / max(1e-9, sum(kms))
     steps_timed = a.steps * CHUNK
-    if launches == steps_timed:
-        # one kernel per step (k_fused: delivery of step s+1 + update of step s):
-        # its average launch duration is the timed region over its launches
-        dom = "k_fused"
+    group_mode = sim.info()["persistent"]
+    if 0 < launches <= steps_timed and steps_timed % launches == 0:
+        # the fused method: one kernel per step (k_fused) or one per step group
+        # (k_steps / k_pipe); each launch covers steps_timed / launches steps
+        # and its average duration is the timed region over its launches
+        per_launch = steps_timed // launches
+        dom = {0: "k_fused", 1: "k_steps", 2: "k_pipe"}[group_mode]
         dur_us = 1e3 * ms / launches
-        dbytes = neuron_bytes + 8.0 * events / steps_timed
+        dbytes = per_launch * (neuron_bytes + 8.0 * events / steps_timed)
         achieved = dbytes / (dur_us * 1e-6) / 1e9
     else:
         dom = max(kern, key=lambda k_: kern[k_]["avg_us"])
@@ -335,13 +342,17 @@ def run_ours(a, ws, rank, local):
     if os.path.exists(tpath):
         try:
             t = json.load(open(tpath)).get(dom)
-            # ncu DRAM bytes of one launch, scaled to this workload by its size
-            traffic = None if t is None else t["bytes_per_launch"] * a.scale
+            # ncu DRAM bytes per step, scaled to this workload's size and to
+            # the steps one launch covers
+            if t is not None:
+                per = steps_timed // launches if launches else 1
+                traffic = t["bytes_per_step"] * a.scale * per
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm,
                 "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
-                "bytes_per_launch": dbytes, "avg_launch_us": dur_us}
+                "bytes_per_launch": dbytes, "avg_launch_us": dur_us,
+                "steps_per_launch": steps_timed // launches if launches else None}
 
     # end to end through the C ABI: rates H2D from pinned memory, run, raster D2H
     sim.close()
@@ -649,6 +660,11 @@ def main():
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--sweep-steps", type=int, default=2000)
+    ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="with --kernel-profile or --no-autotune: 0 graphs of k_fused, 1 k_steps groups, "
+                         "2 k_pipe groups")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the autotuner and run --group-mode (for launch lists)")
     ap.add_argument("--kernel-profile", choices=["quiet", "driven"],
                     help="only build the network at --scale, run --warmup bench steps, 300 "
                          "steps as timed, and 300 profiled steps (separate kernels); for ncu captures")
@@ -662,6 +678,7 @@ def main():
         elif a.kernel_profile:
             w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
             sim = make_sim(w, local, seed=1, record=False)
+            sim.set_persistent(a.group_mode)
             sim.run(CHUNK * a.warmup)
             sim.run(300)           # the timed region's kernels (k_fused per step)
             ms = sim.profile(300)  # then the step split into its kernel classes
