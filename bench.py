@@ -357,6 +357,8 @@ def run_ours(a, ws, rank, local):
     # end to end through the C ABI: rates H2D from pinned memory, run, raster D2H
     sim.close()
     sim = make_sim(w, local, seed=1 + rank, record=True)
+    if not a.no_autotune:
+        sim.autotune(steps_per_trial=640)
     pinned = torch.empty(w["n"], dtype=torch.float32, pin_memory=True)
     pinned.numpy()[:] = w["rate"]
     import ctypes as C

@@ -214,12 +214,14 @@ typedef struct mgc_tune_report {
  * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 
-/* How the fused method runs: 0 CUDA graphs of single-step kernels (the
- * default until the autotuner decides); 1 cooperative step groups of up to
+/* How the fused method runs: 0 CUDA graphs of single-step kernels; 1
+ * cooperative step groups of up to
  * 1024 steps with a grid barrier between steps; 2 pipelined step groups
  * (minimum delay >= 4): during step s each block delivers the arrivals of
  * step s+2 and waits only until every block has finished step s-2.
- * Results are the same in every mode; while a schedule mode other than
+ * Default: 2 when the minimum delay is >= 4, else 1; the autotuner may pick
+ * another.  If the device cannot keep all blocks of a group resident, the
+ * call falls back to 0.  Results are the same in every mode; while a schedule mode other than
  * static, recording or calibration is on, graphs are used.  All waits are
  * bounded (a time-out makes mgc_sync return MGC_ERR_CUDA).  No reference
  * counterpart. */

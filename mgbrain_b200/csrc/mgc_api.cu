@@ -623,6 +623,9 @@ mgc_status finish_build(mgc_sim* s)
         }
         s->fused_variant = 1;
         s->fused_grid = s->fused_grid_v[1];
+        // step groups by default (faster than one launch per step on every
+        // measured load); the pipelined form needs a minimum delay >= 4
+        s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 0;
         if (s->fused) {
             for (int p = 1; p <= 2; ++p)
                 for (int v = 0; v < 2; ++v) {
@@ -1102,12 +1105,21 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
             int32_t n = (int32_t)std::min<int64_t>(left, kPersistentSteps);
             void* args[] = {&s->a, &n};
             CK(cudaMemsetAsync(s->a.bar, 0, 4 * sizeof(unsigned int), s->stream));  // clean barriers
-            CK(cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(s->group_grid_v[p - 1][v]),
-                                           dim3(kPushBlock), args, 0, s->stream));
+            const cudaError_t e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v),
+                                                              dim3(s->group_grid_v[p - 1][v]), dim3(kPushBlock),
+                                                              args, 0, s->stream);
+            if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
+                // the blocks cannot all be resident here (e.g. a shared
+                // device): fall back to the graphs of single-step kernels
+                cudaGetLastError();
+                s->persistent = 0;
+                break;
+            }
+            CK(e);
             s->launches += 1;
             left -= n;
         }
-        return MGC_OK;
+        if (left == 0) return MGC_OK;
     }
     if (left >= kGraphSteps) {
         if (!s->graph) CKS(sched_wanted(s) ? build_sched_graph(s) : build_graph(s));
@@ -1439,6 +1451,7 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
             cands.push_back({t, b});
         }
     const int64_t steps = (steps_per_trial + kGraphSteps - 1) / kGraphSteps * kGraphSteps;
+    s->persistent = 0;  // the shapes are timed as graphs of single-step kernels, step groups after
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
