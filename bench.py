@@ -365,7 +365,7 @@ def run_ours(a, ws, rank, local):
     L = mgb.lib()
     for _ in range(1):
         sim.run(CHUNK)
-        sim.read_raster(max_steps=CHUNK, max_ids=w["n"] * 8)
+        sim.read_raster(max_steps=CHUNK * 2, max_ids=w["n"] * 16)  # also drops the autotuner's steps
     torch.cuda.synchronize()
     barrier(ws)
     h2d = d2h = 0
