@@ -288,6 +288,18 @@ mgc_status mgc_sched_report(mgc_sim* sim, mgc_sched_stats* report, int32_t reset
 mgc_status mgc_mlp_gradient(int32_t device, const float* params, const float* x, const float* y, int32_t n,
                             float* grad, float* loss);
 
+/* Checkpoints: the state a simulation continues from — neuron state and
+ * POISSON rates, the input still in flight (delay ring or accumulators and
+ * spike history), the step clock, the event counter and, with STDP, the
+ * weights — copied to or from host memory.  A handle built from the same
+ * network with the same method that loads a checkpoint continues exactly as
+ * the saved one would have; its raster starts empty at the restored step.
+ * The scheduler's state and the raster are not part of it.  No reference
+ * counterpart (its test/networkio.cpp intent, survey 8f). */
+mgc_status mgc_checkpoint_size(mgc_sim* sim, int64_t* bytes);
+mgc_status mgc_checkpoint_save(mgc_sim* sim, void* buf, int64_t bytes);
+mgc_status mgc_checkpoint_load(mgc_sim* sim, const void* buf, int64_t bytes);
+
 /* The handle's cudaStream_t, for event timing by the caller. */
 mgc_status mgc_get_stream(mgc_sim* sim, void** stream);
 

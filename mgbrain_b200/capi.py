@@ -24,7 +24,8 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_sched_set_mode", "mgc_sched_set_threshold",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_checkpoint_size",
+    "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
 )
 
@@ -127,6 +128,11 @@ def lib():
     L.mgc_autotune.restype = C.c_int
     L.mgc_set_persistent.argtypes = [vp, i32]
     L.mgc_set_persistent.restype = C.c_int
+    L.mgc_checkpoint_size.argtypes = [vp, C.POINTER(i64)]
+    L.mgc_checkpoint_save.argtypes = [vp, vp, i64]
+    L.mgc_checkpoint_load.argtypes = [vp, vp, i64]
+    for name in ("mgc_checkpoint_size", "mgc_checkpoint_save", "mgc_checkpoint_load"):
+        getattr(L, name).restype = C.c_int
     L.mgc_sched_set_mode.argtypes = [vp, i32]
     L.mgc_sched_set_threshold.argtypes = [vp, C.c_double, i32]
     L.mgc_sched_calibrate.argtypes = [vp, i32, C.POINTER(C.c_double)]
@@ -364,6 +370,19 @@ class Simulator:
         d = {k: getattr(r, k) for k, _ in SchedStats._fields_ if k != "reserved"}
         d["variant_groups"] = [r.variant_groups[0], r.variant_groups[1]]
         return d
+
+    def checkpoint(self):
+        """The simulation state as bytes (mgc_checkpoint_save)."""
+        n = C.c_int64()
+        check(lib().mgc_checkpoint_size(self._h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        check(lib().mgc_checkpoint_save(self._h, _ptr(buf), n.value))
+        return buf.tobytes()
+
+    def restore(self, data):
+        """Continues from a checkpoint of the same network (mgc_checkpoint_load)."""
+        buf = np.frombuffer(data, np.uint8)
+        check(lib().mgc_checkpoint_load(self._h, _ptr(buf), buf.size))
 
     def set_persistent(self, mode=1):
         """0: CUDA graphs of single-step kernels; 1: cooperative step groups
