@@ -643,6 +643,82 @@ def run_sched(a, ws, rank, local):
         sim.close()
 
 
+def run_refgpu(a, ws, rank, local):
+    """The reference's own benchmark network (ModelMaker::make_brunel with
+    --ref-syn synapses, Poisson inputs at 20 Hz, generated by the reference's
+    gen_net) simulated for --ref-seconds by the reference's own
+    MGSimulator::simulate on this GPU (its kernels built for sm_100a in
+    oracle/_ref, Poisson draws through the shared counter-based generator)
+    and by this core; wall times, and whether the end states agree."""
+    if rank != 0:
+        return
+    import shutil
+    import tempfile
+
+    import mgbrain_b200 as mgb
+    from mgbrain_b200 import netfile
+    ref_gen = os.path.join(ROOT, "oracle", "_ref", "ref_gen")
+    ref_sim = os.path.join(ROOT, "oracle", "_ref", "ref_sim")
+    if not (os.path.exists(ref_gen) and os.path.exists(ref_sim)):
+        print(json.dumps({"workload": "refgpu", "unavailable": "oracle/_ref is not built (make -C oracle ref)"}))
+        return
+    tmp = tempfile.mkdtemp()
+    try:
+        spec = os.path.join(tmp, "net.spec")
+        with open(spec, "w") as f:
+            f.write(f"timestep 0.0001\nmaker brunel {int(a.ref_syn)}\nrate 0 0.002\n")
+        env = dict(os.environ, MGB_REF_MT_SEED="1", MGB_REF_RAND_SEED="1", MGB_REF_SEED="7")
+        path = os.path.join(tmp, "net.net")
+        t0 = time.perf_counter()
+        subprocess.run([ref_gen, "gen", spec, path], check=True, env=env, capture_output=True)
+        gen_s = time.perf_counter() - t0
+        net = netfile.read_netfile(path)
+        prefix = os.path.join(tmp, "ref")
+        r = subprocess.run([ref_sim, "simulate", path, prefix, str(a.ref_seconds), "-", "0"], check=True, env=env,
+                           capture_output=True, text=True)
+        ref_wall = float(r.stdout.split("wall")[1].split()[0])
+        n, S = net["n"], len(net["src"])
+        b = open(prefix + ".state", "rb").read()
+        ref_v = np.frombuffer(b, np.float32, n, 0)
+        ref_cnt = np.frombuffer(b, np.int32, n, 20 * n)
+        t0 = time.perf_counter()
+        sim = mgb.Simulator.from_arrays(n, net["type"], net["src"], net["tar"], net["weight"],
+                                        netfile.delay_steps(net), netfile.default_lifconst(net),
+                                        netfile.default_stdpconst(net), rate=net["rate"], seed=7, device=local,
+                                        raster_ids=-1)
+        sim.sync()
+        build_s = time.perf_counter() - t0
+        info = sim.info()
+        steps = mgb.effective_steps(int(round(a.ref_seconds / net["step"])), info["min_delay"])
+        import torch
+        stream = torch.cuda.ExternalStream(sim.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        sim.run(steps)
+        e1.record(stream)
+        sim.sync()
+        ours_wall = time.perf_counter() - t0
+        ours_dev = e0.elapsed_time(e1) / 1e3
+        st = sim.state()
+        events = sim.info()["events"]
+        sim.close()
+        print(json.dumps({
+            "workload": "refgpu",
+            "config": {"network": f"the reference's make_brunel, {S} synapses, {n} neurons, inputs 20 Hz, "
+                                  f"dt 0.1 ms, generated by the reference's gen_net",
+                       "seconds": a.ref_seconds, "steps": steps},
+            "reference_simulate_wall_s": ref_wall, "ours_run_wall_s": ours_wall, "ours_device_s": ours_dev,
+            "speedup_wall": ref_wall / ours_wall, "ours_events_per_s": events / ours_wall,
+            "reference_events_per_s": events / ref_wall, "ours_build_s": build_s, "gen_s": gen_s,
+            "fire_cnt_identical": bool(np.array_equal(st["fire_cnt"], ref_cnt)),
+            "V_identical": bool(np.array_equal(st["V"].view(np.int32), ref_v.view(np.int32))),
+            "spikes": int(st["fire_cnt"].sum()),
+        }), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -655,9 +731,12 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
-    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched"],
+    ap.add_argument("--ref-syn", type=float, default=1e8)
+    ap.add_argument("--ref-seconds", type=float, default=1.0)
+    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched", "refgpu"],
                     help="brunel1m: the 1M-neuron network (default); sweep: batched vs plain "
-                         "parameter sweep; sched: the step scheduler's modes on a periodic drive")
+                         "parameter sweep; sched: the step scheduler's modes on a periodic drive; refgpu: "
+                         "the reference's own simulator and this core on the reference's benchmark network")
     ap.add_argument("--sched-train-groups", type=int, default=200)
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
@@ -677,6 +756,8 @@ def main():
             run_sweep(a, ws, rank, local)
         elif a.workload == "sched":
             run_sched(a, ws, rank, local)
+        elif a.workload == "refgpu":
+            run_refgpu(a, ws, rank, local)
         elif a.kernel_profile:
             w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
             sim = make_sim(w, local, seed=1, record=False)

@@ -222,47 +222,9 @@ def oracle_netgen(spec: Spec, mt_seed: int, rand_seed: int):
 # --------------------------------------------------------------------------
 # files
 # --------------------------------------------------------------------------
-def read_netfile(path):
-    with open(path, "rb") as f:
-        b = f.read()
-    assert b[:8] == b"MGBNET02", "bad magic"
-    o = 8
-    n_pops, n = np.frombuffer(b, np.int32, 2, o); o += 8
-    S = int(np.frombuffer(b, np.int64, 1, o)[0]); o += 8
-    step, dw = np.frombuffer(b, np.float32, 2, o); o += 8
-    nl, ns = np.frombuffer(b, np.int32, 2, o); o += 8
-    lif = np.frombuffer(b, np.float32, 30, o).copy(); o += 120
-    stdp = np.frombuffer(b, np.float32, 6, o).copy(); o += 24
-    pops = np.frombuffer(b, np.int32, 4 * n_pops, o).reshape(n_pops, 4).copy(); o += 16 * n_pops
-    n = int(n)
-    typ = np.frombuffer(b, np.int8, n, o).copy(); o += n
-    rate = np.frombuffer(b, np.float32, n, o).copy(); o += 4 * n
-    src = np.frombuffer(b, np.int32, S, o).copy(); o += 4 * S
-    tar = np.frombuffer(b, np.int32, S, o).copy(); o += 4 * S
-    w = np.frombuffer(b, np.float32, S, o).copy(); o += 4 * S
-    d = np.frombuffer(b, np.float32, S, o).copy(); o += 4 * S
-    return dict(n=n, type=typ, rate=rate, src=src, tar=tar, weight=w, delay=d,
-                step=float(step), dw=float(dw), nlifconst=int(nl), nstdpconst=int(ns),
-                lifconst=lif, stdpconst=stdp, pops=pops)
-
-
-def write_netfile(path, net):
-    n, S = int(net["n"]), len(net["src"])
-    pops = np.asarray(net["pops"], np.int32).reshape(-1, 4)
-    with open(path, "wb") as f:
-        f.write(b"MGBNET02")
-        f.write(np.array([len(pops), n], np.int32).tobytes())
-        f.write(np.array([S], np.int64).tobytes())
-        f.write(np.array([net["step"], net["dw"]], np.float32).tobytes())
-        f.write(np.array([net.get("nlifconst", 0), net.get("nstdpconst", 0)], np.int32).tobytes())
-        f.write(np.asarray(net.get("lifconst", np.zeros(30)), np.float32).tobytes())
-        f.write(np.asarray(net.get("stdpconst", np.zeros(6)), np.float32).tobytes())
-        f.write(pops.tobytes())
-        f.write(np.asarray(net["type"], np.int8).tobytes())
-        f.write(np.asarray(net["rate"], np.float32).tobytes())
-        for k, dt in (("src", np.int32), ("tar", np.int32), ("weight", np.float32),
-                      ("delay", np.float32)):
-            f.write(np.asarray(net[k], dt).tobytes())
+# the network file format and the reference's constant selection live in
+# the package; re-exported for the tests
+from mgbrain_b200.netfile import read_netfile, write_netfile  # noqa: E402,F401
 
 
 def read_raster(path):
@@ -288,26 +250,7 @@ def read_state(path, n, S):
 # --------------------------------------------------------------------------
 # simulation through the oracle
 # --------------------------------------------------------------------------
-def default_lifconst(net):
-    """LIFECONSTS the reference kernels see (mgsim.cpp:165-172, mgcore.cu:32-63,
-    :685-748): the network's array when set; else the __constant__ initialiser
-    when only STDP constants are set; else copy_consts_gpu's default array."""
-    if net.get("nlifconst", 0):
-        return np.asarray(net["lifconst"], np.float32)
-    c = np.zeros(30, np.float32)
-    c[21:26] = [0.951229453, 0.967216074, 0.0799999982, 0.0599999987, 0.90483743]
-    c[5], c[6], c[8], c[10], c[11] = 0.25, 10.0, 0.0004, 1.0, 1.0
-    if net.get("nstdpconst", 0):
-        c[0], c[4] = 0.0001, 0.02
-    else:
-        c[0], c[4] = net["step"], 15.0
-    return c
-
-
-def default_stdpconst(net):
-    if net.get("nstdpconst", 0):
-        return np.asarray(net["stdpconst"], np.float32)
-    return np.array([0.1, -0.01, 17, 34, 40, 0], np.float32)
+from mgbrain_b200.netfile import default_lifconst, default_stdpconst  # noqa: E402,F401
 
 
 def quantize_delays(delay_s, step):
