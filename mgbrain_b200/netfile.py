@@ -19,14 +19,13 @@ def read_netfile(path):
     if b[:8] != MAGIC:
         raise ValueError(f"{path}: not an MGBNET02 file")
     o = 8
-    n_pops, n = np.frombuffer(b, np.int32, 2, o); o += 8
+    n_pops, n = (int(x) for x in np.frombuffer(b, np.int32, 2, o)); o += 8  # Python ints: offsets pass 2^31
     S = int(np.frombuffer(b, np.int64, 1, o)[0]); o += 8
     step, dw = np.frombuffer(b, np.float32, 2, o); o += 8
-    nl, ns = np.frombuffer(b, np.int32, 2, o); o += 8
+    nl, ns = (int(x) for x in np.frombuffer(b, np.int32, 2, o)); o += 8
     lif = np.frombuffer(b, np.float32, 30, o).copy(); o += 120
     stdp = np.frombuffer(b, np.float32, 6, o).copy(); o += 24
     pops = np.frombuffer(b, np.int32, 4 * n_pops, o).reshape(n_pops, 4).copy(); o += 16 * n_pops
-    n = int(n)
     typ = np.frombuffer(b, np.int8, n, o).copy(); o += n
     rate = np.frombuffer(b, np.float32, n, o).copy(); o += 4 * n
     src = np.frombuffer(b, np.int32, S, o).copy(); o += 4 * S
