@@ -5,6 +5,13 @@
 #include "mgbrain/constgen.h"
 #include "mgbrain/netgen.h"
 
+#ifndef __CUDACC__  // the core's Philox header, here compiled for the host only
+#define __host__
+#define __device__
+#define __forceinline__ inline
+#endif
+#include "../philox.cuh"
+
 namespace MGBrain {
 
 // Defaults of src/macro.cpp:3-14, plus the additions.
@@ -82,6 +89,25 @@ bool Model::connect(Population& src, Population tar, real weight, real delay, fl
     return connect(src, tar, {weight, weight}, {delay, delay}, ctype, SynapseType::STATIC);
 }
 
+bool Model::connect_fixed_indegree(Population& src, Population tar, int k, real weight, std::array<real, 2> d,
+                                   SynapseType stype, unsigned long long seed)
+{
+    if (k < 0 || (k > 0 && src.num <= 0) || d[1] < d[0]) return false;
+    pros.emplace_back(src.id, tar.id, std::array<real, 2>{weight, weight}, d, 1.0f, stype);
+    pros.back().rule = 1;
+    pros.back().k = k;
+    pros.back().seed = seed;
+    return true;
+}
+
+bool Model::connect_all_but_self(Population& src, Population tar, std::array<real, 2> w, std::array<real, 2> d,
+                                 SynapseType stype)
+{
+    pros.emplace_back(src.id, tar.id, w, d, 1.0f, stype);
+    pros.back().rule = 2;
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // NetGen: the reference's generation algorithm (src/model/netgen.cpp),
 // consuming std::mt19937 and glibc rand() in the same order.
@@ -152,11 +178,39 @@ void NetGen::gen_net(Network& net, Model& model)
     }
     model.indexer = next_id;
 
-    for (const Projection& pr : model.pros) {
+    for (size_t pi = 0; pi < model.pros.size(); ++pi) {
+        const Projection& pr = model.pros[pi];
         const Pop& sp = net.pops[pr.src];
         const Pop& tp = net.pops[pr.tar];
         const int sn = sp.num, tn = tp.num;
         const real w0 = pr.wrange[0], w1 = pr.wrange[1], d0 = pr.drange[0], d1 = pr.drange[1];
+        if (pr.rule == 1) {
+            // fixed in-degree, the device generator's draws (delays in steps)
+            const int dmin = (int)std::round(d0 / Config::STEP), dmax = (int)std::round(d1 / Config::STEP);
+            const uint32_t span = (uint32_t)(dmax - dmin + 1);
+            net.synapses.reserve(net.synapses.size() + (size_t)tn * pr.k);
+            for (int n = 0; n < tn; ++n) {
+                const int t = tp.neurons[n];
+                for (int j = 0; j < pr.k; ++j) {
+                    const mgc::U32x4 r = mgc::conn_draw(pr.seed, (uint32_t)t, (uint32_t)j, (uint32_t)pi);
+                    const int s = sp.neurons[mgc::scale_u32(r.x, (uint32_t)sn)];
+                    const int steps = dmin + (int)mgc::scale_u32(r.y, span);
+                    add_synapse(net, s, t, w0, (real)steps * Config::STEP, pr.stype);
+                }
+            }
+            continue;
+        }
+        if (pr.rule == 2) {
+            net.synapses.reserve(net.synapses.size() + (size_t)sn * tn);
+            for (int m = 0; m < sn; ++m)
+                for (int n = 0; n < tn; ++n) {
+                    if (m == n) continue;
+                    const real w = rand_weight(w0, w1);
+                    const real d = rand_delay(d0, d1);
+                    add_synapse(net, sp.neurons[m], tp.neurons[n], w, d, pr.stype);
+                }
+            continue;
+        }
         if (pr.ctype == 1.0) {
             net.synapses.reserve(net.synapses.size() + (size_t)sn * tn);
             for (int m = 0; m < sn; ++m)

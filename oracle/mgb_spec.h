@@ -17,6 +17,11 @@
  *                                      Model::connect (wrange, drange form)
  *   maker brunel|vogel <nsyn>          ModelMaker::make_brunel / make_vogel
  *   rate <pop> <per-step probability>  (applied to the Network after gen_net)
+ * With MGB_SPEC_EXTENSIONS defined (mgbrain_b200's Model only):
+ *   fixed_indegree <src> <tar> <k> <w> <dmin> <dmax> <seed> <STATIC|STDP>
+ *                                      Model::connect_fixed_indegree
+ *   all_but_self <src> <tar> <wmin> <wmax> <dmin> <dmax> <STATIC|STDP>
+ *                                      Model::connect_all_but_self
  */
 #pragma once
 #include <array>
@@ -93,6 +98,20 @@ Applied apply(const std::string& text, ModelT& m)
             if (which == "brunel") MGBrain::ModelMaker::make_brunel(m, (int)nsyn);
             else if (which == "vogel") MGBrain::ModelMaker::make_vogel(m, (int)nsyn);
             else throw std::runtime_error("unknown maker " + which);
+#ifdef MGB_SPEC_EXTENSIONS
+        } else if (kw == "fixed_indegree") {
+            int s, t, k; float w, dmin, dmax; unsigned long long seed; std::string st;
+            ls >> s >> t >> k >> w >> dmin >> dmax >> seed >> st;
+            m.connect_fixed_indegree(pops.at(s), pops.at(t), k, w, std::array<MGBrain::real, 2>{dmin, dmax},
+                                     st == "STDP" ? MGBrain::SynapseType::STDP : MGBrain::SynapseType::STATIC,
+                                     seed);
+        } else if (kw == "all_but_self") {
+            int s, t; float wmin, wmax, dmin, dmax; std::string st;
+            ls >> s >> t >> wmin >> wmax >> dmin >> dmax >> st;
+            m.connect_all_but_self(pops.at(s), pops.at(t), std::array<MGBrain::real, 2>{wmin, wmax},
+                                   std::array<MGBrain::real, 2>{dmin, dmax},
+                                   st == "STDP" ? MGBrain::SynapseType::STDP : MGBrain::SynapseType::STATIC);
+#endif
         } else if (kw == "rate") {
             int p; float r;
             ls >> p >> r;

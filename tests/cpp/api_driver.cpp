@@ -12,6 +12,7 @@
 #include <sstream>
 
 #include "mgbrain.h"
+#define MGB_SPEC_EXTENSIONS  // this Model has the fixed in-degree and all-but-self rules
 #include "../../oracle/mgb_netfile.h"
 #include "../../oracle/mgb_spec.h"
 
