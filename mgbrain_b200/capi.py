@@ -304,15 +304,15 @@ class Simulator:
 
     # ---- readout --------------------------------------------------------
     def read_raster(self, max_steps=1 << 20, max_ids=None):
-        info = self.info()
+        """(first step, spikes per step, ids per step in ascending order)."""
         if max_ids is None:
             max_ids = max(1, self.n) * 64
-        counts = np.zeros(max_steps, np.int64)
-        ids = np.zeros(max_ids, np.int32)
+        counts = np.empty(max_steps, np.int64)
+        ids = np.empty(max_ids, np.int32)
         first, ns, ni = C.c_int64(), C.c_int64(), C.c_int64()
         check(lib().mgc_read_raster(self._h, C.byref(first), _ptr(counts), max_steps, _ptr(ids),
                                     max_ids, C.byref(ns), C.byref(ni)))
-        del info
+        # copies: the (mostly untouched) capacity buffers are not kept alive
         return first.value, counts[:ns.value].copy(), ids[:ni.value].copy()
 
     def state(self):

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1170,17 +1171,35 @@ mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int
     const int64_t ni = std::min(pos, s->raster_ids_cap);
     std::vector<int32_t> c32(ns);
     if (ns) CK(cudaMemcpy(c32.data(), s->a.raster_counts, 4 * ns, cudaMemcpyDeviceToHost));
-    std::vector<int32_t> hid(ni);
-    if (ni) CK(cudaMemcpy(hid.data(), s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
-    const bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
-    int64_t off = 0;
-    for (int64_t i = 0; i < ns; ++i) {
-        const int64_t c = c32[i];
-        if (off + c <= ni) std::sort(hid.begin() + off, hid.begin() + off + c);
-        if (counts && i < counts_cap) counts[i] = c;
-        off += c;
+    // the ids land in the caller's buffer when it holds them all (else in a
+    // staging buffer), then each step's ids are sorted in place, the steps
+    // split over host threads
+    std::unique_ptr<int32_t[]> staging;
+    int32_t* hid = ids;
+    if (!ids || ids_cap < ni) {
+        staging.reset(new int32_t[std::max<int64_t>(ni, 1)]);
+        hid = staging.get();
     }
-    if (ids) memcpy(ids, hid.data(), 4 * std::min(ni, ids_cap));
+    if (ni) CK(cudaMemcpy(hid, s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
+    const bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
+    std::vector<int64_t> off(ns + 1, 0);
+    for (int64_t i = 0; i < ns; ++i) {
+        off[i + 1] = off[i] + c32[i];
+        if (counts && i < counts_cap) counts[i] = c32[i];
+    }
+    auto sort_steps = [&](int64_t i0, int64_t i1) {
+        for (int64_t i = i0; i < i1; ++i)
+            if (off[i + 1] <= ni) std::sort(hid + off[i], hid + off[i + 1]);
+    };
+    const int64_t nt = std::min<int64_t>(std::max(1u, std::thread::hardware_concurrency()), 16);
+    if (ni > (1 << 16) && ns > 1 && nt > 1) {
+        std::vector<std::thread> pool;
+        for (int64_t t = 0; t < nt; ++t) pool.emplace_back(sort_steps, ns * t / nt, ns * (t + 1) / nt);
+        for (auto& th : pool) th.join();
+    } else {
+        sort_steps(0, ns);
+    }
+    if (ids && hid != ids) memcpy(ids, hid, 4 * std::min(ni, ids_cap));
     if (first_step) *first_step = step0;
     if (n_steps) *n_steps = std::min(ns, counts_cap);
     if (n_ids) *n_ids = std::min(ni, ids_cap);
