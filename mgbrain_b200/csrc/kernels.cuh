@@ -574,8 +574,11 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 }
 
 // The tasks themselves, after deliver_prefix and a block barrier.
+// blk_ev: when given, the warps add their delivered events into this block
+// counter (shared memory) instead of the global one.
 __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot,
-                                              const int64_t* pre, int64_t warp, int64_t nwarps)
+                                              const int64_t* pre, int64_t warp, int64_t nwarps,
+                                              unsigned long long* blk_ev = nullptr)
 {
     const int D = a.D;
     const int32_t hs = hist_slot(a, sa, s, hslot);
@@ -651,7 +654,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
             }
         }
     }
-    if (ev) atomicAdd(a.events, ev);
+    if (ev) atomicAdd(blk_ev ? blk_ev : a.events, ev);
 }
 
 __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
@@ -849,10 +852,25 @@ __device__ __forceinline__ bool wait_phase(const StepArgs& a, int32_t phase, int
     return *abort_flag == 0;
 }
 
-__device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase)
+// The block's step is done: its spike counts per trace population and its
+// delivered events go out (and the block counters are cleared for reuse two
+// steps later), then the block arrives on the phase counter.
+__device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase, int64_t s, int* pop, unsigned long long* ev)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
+        if (pop) {
+            float* row = a.trace + (s & (kTraceSteps - 1)) * kTraceCols;
+            for (int c = 0; c < kTracePops; ++c) {
+                if (a.trace && pop[c]) atomicAdd(row + c, (float)pop[c]);
+                pop[c] = 0;
+            }
+            if (*ev) {
+                atomicAdd(a.events, *ev);
+                if (a.trace) atomicAdd(row + kTracePops, (float)*ev);
+            }
+            *ev = 0;
+        }
         __threadfence();
         atomicAdd(a.bar + (phase % kPhaseCounters), 1u);
     }
@@ -881,6 +899,8 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
     __shared__ int abort_flag;
+    __shared__ int pop_cnt[2][kTracePops];        // by step parity
+    __shared__ unsigned long long blk_ev[2];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -892,29 +912,42 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
     const int64_t s_end = s0 + nsteps;
     auto hs_of = [&](int64_t x) { return (int32_t)((h0 + (x - s0)) % a.H); };
     if (threadIdx.x == 0) abort_flag = 0;
-    // prologue: arrivals of step s0+1; the slot of step s0+1 cleared
-    if (lead) a.hist_cnt[hs_of(s0 + 1)] = 0;
+    if (threadIdx.x < 2 * kTracePops) pop_cnt[threadIdx.x / kTracePops][threadIdx.x % kTracePops] = 0;
+    if (threadIdx.x < 2) blk_ev[threadIdx.x] = 0;
+    // prologue: arrivals of step s0+1; the slot of step s0+1 cleared, and the
+    // trace rows of steps s0+1, s0+2 (row s0 was cleared by the step before)
+    if (lead) {
+        a.hist_cnt[hs_of(s0 + 1)] = 0;
+        if (a.trace)
+            for (int64_t x = s0 + 1; x <= s0 + 2; ++x)
+                for (int c = 0; c < kTraceCols; ++c) a.trace[(x & (kTraceSteps - 1)) * kTraceCols + c] = 0.f;
+    }
     __syncthreads();
     if (nsteps > 0) {
         if (threadIdx.x < 32) deliver_prefix(a, s0 + 1, s0, h0, pre);
         __syncthreads();
         deliver_tasks(a, s0 + 1, s0, h0, pre, warp, nwarps);
     }
-    arrive(a, 0);
+    arrive(a, 0, 0, nullptr, nullptr);
     for (int32_t i = 0; i < nsteps; ++i) {
         const int64_t s = s0 + i;
         const int32_t hs = hs_of(s);
         // every block has finished step s-2 (phase i-1; for i = 1 the prologue)
         if (i >= 1 && !wait_phase(a, i - 1, &abort_flag)) return;
         if (lead && s + 2 <= s_end) a.hist_cnt[hs_of(s + 2)] = 0;
+        if (lead && a.trace) {  // no block writes step s+3's row before lead finishes step s+1
+            float* row = a.trace + ((s + 3) & (kTraceSteps - 1)) * kTraceCols;
+            for (int c = 0; c < kTraceCols; ++c) row[c] = 0.f;
+        }
         if (rec && blockIdx.x == 0 && i >= 2) raster_copy(a, s - 2, hs_of(s - 2), rstep0, rbase);
         const bool deliver = s + 2 <= s_end;
         if (deliver && threadIdx.x < 32) deliver_prefix(a, s + 2, s, hs, pre);
-        neuron_groups<2, CUR>(a, s, hs, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, 0, nullptr,
-                              false);
+        const int b = i & 1;
+        neuron_groups<2, CUR>(a, s, hs, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, 0,
+                              a.trace ? pop_cnt[b] : nullptr, false);
         __syncthreads();
-        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps);
-        arrive(a, i + 1);
+        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps, &blk_ev[b]);
+        arrive(a, i + 1, s, pop_cnt[b], &blk_ev[b]);
     }
     // the group's last steps: all blocks done (phases n-1 and n), remaining raster, the clock
     if (nsteps >= 1 && !wait_phase(a, nsteps - 1, &abort_flag)) return;
@@ -923,7 +956,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
         for (int64_t x = (nsteps >= 2 ? s_end - 2 : s0); x < s_end; ++x) raster_copy(a, x, hs_of(x), rstep0, rbase);
     if (lead) {
         if (rec) *a.raster_pos = rbase;
-        if (a.trace) *a.ev_mark = *(volatile unsigned long long*)a.events;  // no trace rows here
+        if (a.trace) *a.ev_mark = *(volatile unsigned long long*)a.events;  // every block's events are in
         a.slots[0] = (int32_t)((slot0 + nsteps) % a.M);
         a.slots[1] = hs_of(s_end);
         __threadfence();

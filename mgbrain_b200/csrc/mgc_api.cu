@@ -755,9 +755,35 @@ mgc_status build_sched_graph(mgc_sim* s)
     cudaGraphNode_t cond;
     CK(cudaGraphAddNode(&cond, guard.g, &decide, 1, &cp));
     void* sargs[] = {&s->a};
+    int32_t group_steps = kGraphSteps;
+    void* gargs[] = {&s->a, &group_steps};
     for (int v = 0; v < 2; ++v) {
         cudaGraph_t body = cp.conditional.phGraph_out[v];
         cudaGraphNode_t prev = nullptr;
+        if (s->persistent) {
+            // the group as one cooperative step-group kernel of variant v,
+            // after a node that clears its barrier counters
+            const int p = s->persistent;
+            cudaMemsetParams mp = {};
+            mp.dst = s->a.bar;
+            mp.value = 0;
+            mp.elementSize = 4;
+            mp.width = 4;
+            mp.height = 1;
+            mp.pitch = 0;
+            cudaGraphNode_t clear, node;
+            CK(cudaGraphAddMemsetNode(&clear, body, nullptr, 0, &mp));
+            cudaKernelNodeParams gp = {};
+            gp.func = (void*)steps_kernel(s, p, v);
+            gp.gridDim = dim3(s->group_grid_v[p - 1][v]);
+            gp.blockDim = dim3(kPushBlock);
+            gp.kernelParams = gargs;
+            CK(cudaGraphAddKernelNode(&node, body, &clear, 1, &gp));
+            cudaLaunchAttributeValue coop = {};
+            coop.cooperative = 1;
+            CK(cudaGraphKernelNodeSetAttribute(node, cudaLaunchAttributeCooperative, &coop));
+            continue;
+        }
         for (int i = 0; i < kGraphSteps; ++i) {
             cudaKernelNodeParams sp = {};
             sp.func = (void*)fused_kernel(s, v);
@@ -1126,7 +1152,9 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         if (!s->graph) CKS(sched_wanted(s) ? build_sched_graph(s) : build_graph(s));
         while (left >= s->graph_steps) {
             CK(cudaGraphLaunch(s->graph, s->stream));
-            s->launches += (int64_t)s->graph_steps * kernels_per_step(s) + (s->sched_graph ? 1 : 0);
+            s->launches += s->sched_graph && s->persistent ? 2  // the decision kernel and the step group
+                                                           : (int64_t)s->graph_steps * kernels_per_step(s) +
+                                                                 (s->sched_graph ? 1 : 0);
             left -= s->graph_steps;
         }
     }
@@ -1435,6 +1463,12 @@ mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
     if (mode < 0 || mode > 2) return fail(MGC_ERR_INVALID, "step-group mode %d (0, 1 or 2)", mode);
     if (mode && !s->fused) return fail(MGC_ERR_INVALID, "step groups need the fused deferred method");
     if (mode == 2 && s->dmin < 4) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
+    if (s->graph && s->persistent != mode) {  // the scheduler's graph holds step groups of the old mode
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        s->sched_graph = false;
+    }
     s->persistent = mode;
     return MGC_OK;
 }
