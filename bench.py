@@ -463,10 +463,11 @@ def rank_share(count, ws, rank):
 def run_sweep(a, ws, rank, local):
     """Parameter sweep of independent Brunel instances (N log-uniform in
     [1e3, 1e5], K = min(N/10, 1000), g ~ U[3, 7], nu_ext ~ U[10, 30] Hz).
-    Batched form: all of this rank's instances in one handle, one kernel per
-    step for all of them.  Plain form: each instance in its own handle, run
-    one after the other for the same steps.  Rasters of the two forms are
-    compared instance by instance.  Instances are dealt to ranks round-robin
+    Batched + learned form: all of this rank's instances in one handle,
+    autotuned, with the step scheduler calibrated, its network trained on the
+    batch's own group trace and the learned mode on while timed.  Plain form:
+    each instance in its own handle, run one after the other for the same
+    steps.  Rasters of the two forms are compared instance by instance.  Instances are dealt to ranks round-robin
     (weak scaling: no collective on the data path)."""
     import torch
 
@@ -477,7 +478,7 @@ def run_sweep(a, ws, rank, local):
     mine = [insts[i] for i in rank_share(len(insts), ws, rank)]
     T = a.sweep_steps
     n_all = sum(brunel.sweep_block(p)["n"] for p in mine)
-    steps_cap = T + 4096                     # also holds the autotuner's trial steps
+    steps_cap = T + 8192                     # also holds the autotuner's and the scheduler's steps
     cap = lambda n: max(4096, n * steps_cap // 200)  # room for a mean rate of 50 Hz
     raster = dict(raster_steps=steps_cap)
     t0 = time.perf_counter()
@@ -486,6 +487,15 @@ def run_sweep(a, ws, rank, local):
     info = sim.info()
     tune = sim.autotune(steps_per_trial=64)
     sim.read_raster(max_steps=steps_cap, max_ids=cap(n_all))  # drops the trial steps
+    # the learned scheduler: calibrated threshold, trained on this batch's trace
+    thr = sim.sched_calibrate(groups=8)
+    sim.sched_collect(True, reset=True)
+    sim.run(64 * 40)
+    sim.sched_collect(False)
+    loss = sim.sched_train(epochs=300, lr=3e-3, seed=7)
+    sim.sched_mode(mgb.SCHED_LEARNED)
+    sim.read_raster(max_steps=steps_cap, max_ids=cap(n_all))
+    pre_steps = sim.info()["step"]
     for _ in range(a.warmup):
         sim.run(T)
         sim.read_raster(max_steps=T, max_ids=cap(n_all))
@@ -493,6 +503,7 @@ def run_sweep(a, ws, rank, local):
         ms, events, launches = timed_device(sim, T, 1, ws)
     _, counts, ids = sim.read_raster(max_steps=T, max_ids=cap(n_all))
     per_inst = split_raster(counts, ids, starts, T)
+    sched = sim.sched_report()
     sim.close()
     batch_ev_s = allsum(ws, events) / (allmax(ws, ms) / 1e3)
 
@@ -502,7 +513,7 @@ def run_sweep(a, ws, rank, local):
     for i in range(len(mine)):
         alone_n = brunel.sweep_block(mine[i])["n"]
         alone = brunel.sweep_alone(mine, i, seed=1, raster_ids=cap(alone_n), **raster)
-        alone.run(tune["steps"])  # the steps the batch spent in its autotuner
+        alone.run(pre_steps)  # the steps the batch spent in its autotuner and scheduler set-up
         alone.read_raster(max_steps=steps_cap, max_ids=cap(alone_n))
         for _ in range(a.warmup):
             alone.run(T)
@@ -529,7 +540,10 @@ def run_sweep(a, ws, rank, local):
                        "instances_per_gpu": len(mine), "neurons_gpu0": info["n_neurons"],
                        "synapses_gpu0": info["n_synapses"], "steps_per_form": T},
             "batched": {"events_per_s": batch_ev_s, "ms": ms, "kernel_launches": launches,
-                        "build_s": build_s, "autotune": tune},
+                        "build_s": build_s, "autotune": tune,
+                        "scheduler": {"mode": "learned", "calibrated_threshold": thr, "train_loss": loss,
+                                      "groups": sched["groups"], "misses": sched["misses"],
+                                      "variant_groups": sched["variant_groups"]}},
             "plain": {"events_per_s": plain_ev_s, "ms": plain_ms, "kernel_launches": plain_launches},
             "batched_over_plain": batch_ev_s / plain_ev_s if plain_ev_s else None,
             "rasters_identical": f"{same}/{a.sweep_count}",
@@ -740,7 +754,7 @@ def main():
     ap.add_argument("--sched-train-groups", type=int, default=200)
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
-    ap.add_argument("--sweep-steps", type=int, default=2000)
+    ap.add_argument("--sweep-steps", type=int, default=2048)
     ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2],
                     help="with --kernel-profile or --no-autotune: 0 graphs of k_fused, 1 k_steps groups, "
                          "2 k_pipe groups")
