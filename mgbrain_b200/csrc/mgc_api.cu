@@ -1534,10 +1534,15 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
         }
         rep->trials += 1;
     }
-    for (int p = 1; p <= 2 && st == MGC_OK && s->fused && !sched_wanted(s); ++p) {
-        // the best shape once more as a step group (p = 2: pipelined)
+    TuneCand best_c = cands[best_i];
+    for (int t = 0; t < 4 && st == MGC_OK && s->fused && !sched_wanted(s); ++t) {
+        // the best chunking once more as step groups (p = 2: pipelined) of
+        // each kernel instantiation: their best register budget can differ
+        // from the single-step kernel's
+        const int p = 1 + t / 2;
         if (p == 2 && s->dmin < 4) break;
-        st = apply_cand(s, cands[best_i], sms);
+        const TuneCand c{cands[best_i].chunk_target, t % 2 == 0 ? 2 : 3};
+        st = apply_cand(s, c, sms);
         s->persistent = p;
         if (st == MGC_OK) st = mgc_run(s, kGraphSteps);
         if (st == MGC_OK) {
@@ -1552,6 +1557,7 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
             if (per < best) {
                 best = per;
                 rep->persistent = p;
+                best_c = c;
             }
         }
         if (st == MGC_OK) st = mgc_sync(s);
@@ -1560,10 +1566,10 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != MGC_OK) return st;
-    CKS(apply_cand(s, cands[best_i], sms));
+    CKS(apply_cand(s, best_c, sms));
     rep->ms_per_step = best;
     rep->chunk_len = s->a.deferred ? s->a.chunk_len : 0;
-    rep->blocks_per_sm = cands[best_i].blocks_per_sm;
+    rep->blocks_per_sm = best_c.blocks_per_sm;
     rep->steps = (int64_t)rep->trials * (steps + kGraphSteps);
     return MGC_OK;
 }
