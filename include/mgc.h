@@ -123,6 +123,8 @@ typedef struct mgc_info {
     int32_t graph_steps;       /* steps per captured CUDA graph */
     int64_t device_bytes;      /* device memory held by the handle */
     int32_t persistent;        /* steps run as step groups: 0 no (graphs), 1 barrier per step, 2 pipelined */
+    int32_t first_neuron;      /* partition handles: whole-network id of neuron 0 (else 0) */
+    int32_t total_neurons;     /* partition handles: neurons of the whole network (else n_neurons) */
     int32_t reserved;
 } mgc_info;
 
@@ -147,6 +149,50 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* desc, mgc_si
  * blocks share blocks[0]'s LIF constants, mode, device and raster sizes.
  * No reference counterpart (the reference simulates one network). */
 mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, mgc_sim** out);
+
+/* Partitions: one network split into neuron ranges [first, first + count),
+ * one handle per range, each on its own device (or several on one).  Replaces
+ * MGSimulator(Network&, std::vector<int>& part, int npart) with npart > 1
+ * (mgsim.cpp:337-363, build_multinet's per-partition split :8-144) and its
+ * exchange: the reference's partitions push cross-partition events into
+ * per-pair spike buffers and copy them between GPUs every min_delay/2 steps
+ * (simulate_sparse, mgsim.cpp:794-848; trans_spikes_sparse /
+ * recvs_spikes_sparse, mgcore.cu:470-646).  Here a partition holds the
+ * synapses that TARGET its neurons, with every source of the network, and
+ * the partitions exchange spike ids: after at most min_delay - 1 steps
+ * (mgc_run refuses more), each exports the spike ids of those steps
+ * (mgc_part_export), the caller gathers them across partitions (NCCL
+ * all-gather, or any copy), and each imports the others' (mgc_part_import).
+ * The union of the partitions' rasters and state equals the whole network's
+ * run.  Static weights only (the deferred method), min_delay >= 2.  The
+ * description is that of the whole network; ids in rasters, exports and
+ * imports are whole-network ids; state and rates are the partition's
+ * neurons.  Autotuning, profiling and scheduler calibration (which run steps
+ * of their own) are refused on partition handles.  No reference counterpart
+ * for the fixed in-degree form. */
+mgc_status mgc_create_partition(const mgc_net_desc* desc, int32_t first, int32_t count, mgc_sim** out);
+mgc_status mgc_create_fixed_indegree_partition(const mgc_fixed_indegree_desc* desc, int32_t first, int32_t count,
+                                               mgc_sim** out);
+
+/* Spike ids of the `count` steps run since the last import (count must
+ * equal that number), oldest step first: counts[j] (host array) = spikes of
+ * step j of the window, ids (device memory of the handle's device, or
+ * mapped page-locked host memory; ids_cap entries) = their ids, step after
+ * step; *total = their sum.  Waits for the handle's stream.  MGC_ERR_OVERFLOW
+ * (counts and *total still set) when they do not fit ids_cap; ids_cap = 0
+ * queries the counts only. */
+mgc_status mgc_part_export(mgc_sim* sim, int32_t count, int32_t* counts, int32_t* ids, int64_t ids_cap,
+                           int64_t* total);
+
+/* Appends the other partitions' spikes of the same `count` steps: counts
+ * (host, [nranks][count]) are every partition's exports, ids (device
+ * memory as above) holds partition r's ids at ids + r * stride, in its
+ * export order; the entries of `self` are skipped.  Waits for the handle's
+ * stream.  An id outside the network refuses the whole import
+ * (MGC_ERR_INVALID; the handle then refuses further imports and mgc_sync
+ * reports it). */
+mgc_status mgc_part_import(mgc_sim* sim, int32_t count, int32_t nranks, int32_t self, const int32_t* counts,
+                           const int32_t* ids, int64_t stride);
 
 /* Enqueues `steps` steps on the handle's stream and returns without
  * waiting.  Replaces the step loop of MGSimulator::simulate_sparse

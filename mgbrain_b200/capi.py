@@ -27,6 +27,7 @@ EXPORTED = (
     "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_checkpoint_size",
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
+    "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
 )
 
 
@@ -82,7 +83,8 @@ class Info(C.Structure):
         ("n_neurons", C.c_int32), ("ring_len", C.c_int32), ("min_delay", C.c_int32),
         ("max_delay", C.c_int32), ("n_synapses", C.c_int64), ("step", C.c_int64),
         ("events", C.c_int64), ("mode", C.c_int32), ("graph_steps", C.c_int32),
-        ("device_bytes", C.c_int64), ("persistent", C.c_int32), ("reserved", C.c_int32),
+        ("device_bytes", C.c_int64), ("persistent", C.c_int32), ("first_neuron", C.c_int32),
+        ("total_neurons", C.c_int32), ("reserved", C.c_int32),
     ]
 
 
@@ -103,6 +105,13 @@ def lib():
     L.mgc_create.argtypes = [C.POINTER(NetDesc), C.POINTER(vp)]
     L.mgc_create_fixed_indegree.argtypes = [C.POINTER(FixedInDegreeDesc), C.POINTER(vp)]
     L.mgc_create_batch.argtypes = [C.POINTER(FixedInDegreeDesc), i32, C.POINTER(vp)]
+    L.mgc_create_partition.argtypes = [C.POINTER(NetDesc), i32, i32, C.POINTER(vp)]
+    L.mgc_create_fixed_indegree_partition.argtypes = [C.POINTER(FixedInDegreeDesc), i32, i32, C.POINTER(vp)]
+    L.mgc_part_export.argtypes = [vp, i32, vp, vp, i64, C.POINTER(i64)]
+    L.mgc_part_import.argtypes = [vp, i32, i32, i32, vp, vp, i64]
+    for name in ("mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export",
+                 "mgc_part_import"):
+        getattr(L, name).restype = C.c_int
     L.mgc_run.argtypes = [vp, i64]
     L.mgc_sync.argtypes = [vp]
     L.mgc_set_rates.argtypes = [vp, vp, i32]
@@ -191,13 +200,17 @@ class Simulator:
         self._h = C.c_void_p(handle)
         self.n = n
         self.S = S
+        self.first = 0     # partition handles: whole-network id of neuron 0
+        self.n_src = n     # CSR rows (the whole network's neurons for a partition)
         self._keep = keep
 
     # ---- construction ---------------------------------------------------
     @classmethod
     def from_arrays(cls, n, type_, src, tar, weight, delay_steps, lifconst, stdpconst=None,
                     rate=None, v_init=None, stdp=False, plastic=None, seed=1, device=0,
-                    mode=MODE_AUTO, raster_steps=0, raster_ids=0):
+                    mode=MODE_AUTO, raster_steps=0, raster_ids=0, part=None):
+        """part: (first, count) builds the partition of neurons [first, first+count)
+        of this network (mgc_create_partition)."""
         L = lib()
         arrs = dict(
             type=np.ascontiguousarray(type_, np.int8),
@@ -221,8 +234,19 @@ class Simulator:
         d.stdp, d.mode, d.seed, d.device = int(bool(stdp)), int(mode), int(seed), int(device)
         d.raster_steps, d.raster_ids = int(raster_steps), int(raster_ids)
         h = C.c_void_p()
+        if part is not None:
+            check(L.mgc_create_partition(C.byref(d), int(part[0]), int(part[1]), C.byref(h)))
+            return cls._partition(h.value)
         check(L.mgc_create(C.byref(d), C.byref(h)))
         return cls(h.value, int(n), d.n_synapses)
+
+    @classmethod
+    def _partition(cls, handle):
+        s = cls(handle, 0, 0)
+        i = s.info()
+        s.n, s.S = i["n_neurons"], i["n_synapses"]
+        s.first, s.n_src = i["first_neuron"], i["total_neurons"]
+        return s
 
     @staticmethod
     def _block_desc(pops, projs, lifconst, rate=None, v_init=None, conn_seed=1, seed=1, device=0,
@@ -258,9 +282,14 @@ class Simulator:
     def fixed_indegree(cls, pops, projs, lifconst, **kw):
         """pops: list of (start, num, type); projs: (src_pop, tar_pop, k, w, dmin, dmax);
         keywords: rate, v_init, conn_seed, seed, device, mode, raster_steps, raster_ids,
-        id_offset, proj_offset."""
+        id_offset, proj_offset; part=(first, count) builds that partition of the
+        network (mgc_create_fixed_indegree_partition)."""
+        part = kw.pop("part", None)
         d, keep, n, S = cls._block_desc(pops, projs, lifconst, **kw)
         h = C.c_void_p()
+        if part is not None:
+            check(lib().mgc_create_fixed_indegree_partition(C.byref(d), int(part[0]), int(part[1]), C.byref(h)))
+            return cls._partition(h.value)
         check(lib().mgc_create_fixed_indegree(C.byref(d), C.byref(h)))
         return cls(h.value, n, S)
 
@@ -330,12 +359,30 @@ class Simulator:
         return w
 
     def export_csr(self):
-        rp = np.zeros(self.n + 1, np.int64)
+        rp = np.zeros(self.n_src + 1, np.int64)
         t = np.zeros(self.S, np.int32)
         w = np.zeros(self.S, np.float32)
         d = np.zeros(self.S, np.int32)
         check(lib().mgc_export_csr(self._h, _ptr(rp), _ptr(t), _ptr(w), _ptr(d)))
         return rp, t, w, d
+
+    # ---- partitions -------------------------------------------------------
+    def part_export(self, count, ids):
+        """Spike ids of the `count` steps run since the last import, written into
+        `ids` (a contiguous int32 device tensor of the handle's device, or None
+        for the counts only); returns (counts per step, total)."""
+        counts = np.zeros(max(1, int(count)), np.int32)
+        total = C.c_int64()
+        ptr, cap = (C.c_void_p(ids.data_ptr()), ids.numel()) if ids is not None else (None, 0)
+        check(lib().mgc_part_export(self._h, int(count), _ptr(counts), ptr, int(cap), C.byref(total)))
+        return counts[:int(count)], int(total.value)
+
+    def part_import(self, count, self_rank, counts, ids, stride):
+        """Appends the other partitions' spikes: counts [nranks][count] (host),
+        partition r's ids at ids[r * stride:] (contiguous int32 device tensor)."""
+        c = np.ascontiguousarray(counts, np.int32)
+        check(lib().mgc_part_import(self._h, int(count), int(c.shape[0]), int(self_rank), _ptr(c),
+                                    C.c_void_p(ids.data_ptr()) if ids is not None else None, int(stride)))
 
     def autotune(self, steps_per_trial=640):
         """Times the launch configurations and keeps the fastest; the trial

@@ -34,7 +34,7 @@ namespace mgc {
 enum : int { kRAW = 0, kLIF0 = 1, kPOISSON = 2, kLIF = 3, kLIFE = 4, kLIFB = 5 };
 
 // Device status bits, read back by mgc_sync / mgc_read_raster.
-enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2, kStatusBarrier = 4 };
+enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2, kStatusBarrier = 4, kStatusExchange = 8 };
 
 constexpr int kNeuronBlock = 256;
 constexpr int kPushBlock = 256;
@@ -47,6 +47,9 @@ constexpr int kTraceSteps = 1024;     // rows of the per-step trace ring
 struct StepArgs {
     int32_t n;            // neurons
     int32_t ns;           // neuron arrays' length: n rounded up to a multiple of 4
+    int32_t n_src;        // CSR rows (spike sources): n, or the whole network's neurons
+                          // when this handle simulates one partition of it
+    int32_t src_base;     // id of local neuron 0 in the spike history and raster
     int32_t deliver_blocks;  // fused step kernel: blocks that deliver
     int32_t M;            // ring slots = max_delay + 1
     int32_t tbits;        // target bits in a packed CSR word
@@ -68,9 +71,9 @@ struct StepArgs {
     int32_t H;            //   history slots (>= dmax + 1)
     int32_t bucket_chunks;//   delivery tasks per (spike, delay) segment
     int32_t chunk_len;    //   synapses per task: segment positions [c*len, (c+1)*len)
-    int32_t* hist_ids;    //   [H][n] spike ids per step
+    int32_t* hist_ids;    //   [H][n_src] spike ids per step
     int32_t* hist_cnt;    //   [H]
-    const int64_t* bucket;   // [n*D + 1] CSR position of (source, bucket)
+    const int64_t* bucket;   // [n_src*D + 1] CSR position of (source, bucket)
     float* acc_e;         //   [2][ns] input arriving at steps of each parity
     float* acc_i;
     int32_t pull;         // pull method (per-target pass at emission, STDP fused)
@@ -154,7 +157,7 @@ __device__ __forceinline__ int32_t* step_count(const StepArgs& a, int32_t hslot)
 
 __device__ __forceinline__ int32_t* step_ids(const StepArgs& a, int32_t hslot)
 {
-    return a.deferred ? a.hist_ids + (size_t)hslot * (size_t)a.n : a.spk;
+    return a.deferred ? a.hist_ids + (size_t)hslot * (size_t)a.n_src : a.spk;
 }
 
 __device__ __forceinline__ void step_epilogue(const StepArgs& a)
@@ -371,9 +374,9 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 const int32_t i0 = (int32_t)((gb + h * 32 + lane) << 2);
                 for (int k = 0; k < 4; ++k) {
                     if (fmask[h] & (1u << k)) {
-                        ids[pos] = i0 + k;
+                        ids[pos] = a.src_base + i0 + k;
                         if (pop_cnt) atomicAdd(pop_cnt + a.tpop[i0 + k], 1);
-                        if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = i0 + k;
+                        if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = a.src_base + i0 + k;
                         ++pos;
                     }
                 }
@@ -612,7 +615,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
             const int32_t j = (int32_t)(fs - pre[k]);
             int32_t h = hs - (a.dmin + k);
             if (h < 0) h += a.H;
-            const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n + j];
+            const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n_src + j];
             const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
             const int64_t b0 = __ldg(bk);
             const int64_t seg = __ldg(bk + 1) - b0;
@@ -880,7 +883,7 @@ __device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase, int64_t
 __device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0, int64_t& rbase)
 {
     const int32_t cnt = *(volatile int32_t*)(a.hist_cnt + hs);
-    const int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n;
+    const int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
     for (int32_t j = threadIdx.x; j < cnt; j += blockDim.x)
         if (rbase + j < a.raster_ids_cap) a.raster_ids[rbase + j] = ids[j];
     if (threadIdx.x == 0) {

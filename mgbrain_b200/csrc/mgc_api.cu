@@ -74,6 +74,12 @@ struct mgc_sim {
     cudaStream_t stream = nullptr;
     StepArgs a{};
     int32_t n = 0, M = 0, dmin = 0, dmax = 0;
+    int32_t n_src = 0;   // CSR rows: n, or the whole network's neurons (partition)
+    int sbits = 1;       // bits of a source id in the sort keys
+    bool partition = false;  // simulates neurons [a.src_base, a.src_base + n) of a larger network
+    int32_t pending = 0;     // partition: steps run since the last spike import
+    int32_t* xch = nullptr;  // partition: device scratch of the exchange (spike counts)
+    int64_t xch_cap = 0;
     int64_t S = 0;
     int mode = MGC_MODE_PUSH;
     bool stdp = false;
@@ -178,12 +184,12 @@ __global__ void k_max_gap(const int64_t* off, int64_t count, unsigned long long*
     GRID_STRIDE(i, count) atomicMax(out, (unsigned long long)(off[i + 1] - off[i]));
 }
 
-__global__ void k_validate(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int32_t n,
-                           int32_t dlim, int32_t* bad)
+__global__ void k_validate(const int32_t* src, const int32_t* tar, const int32_t* delay, int64_t S, int32_t n_src,
+                           int32_t n, int32_t dlim, int32_t* bad)
 {
     GRID_STRIDE(k, S)
     {
-        if (src[k] < 0 || src[k] >= n || tar[k] < 0 || tar[k] >= n || delay[k] < 1 || delay[k] >= dlim)
+        if (src[k] < 0 || src[k] >= n_src || tar[k] < 0 || tar[k] >= n || delay[k] < 1 || delay[k] >= dlim)
             atomicOr(bad, 1);
     }
 }
@@ -268,7 +274,7 @@ struct ProjEntry {
     float w;
     int32_t rid;     // projection index in the draws
     int32_t id_off;  // added to target ids in the draws
-    int32_t pad;
+    int32_t tar_sub; // subtracted from target ids in the CSR words (a partition's first neuron)
 };
 
 __device__ __forceinline__ void fid_decode(const ProjEntry* pt, int32_t npr, int64_t i, int32_t& src, int32_t& tar,
@@ -288,6 +294,7 @@ __device__ __forceinline__ void fid_decode(const ProjEntry* pt, int32_t npr, int
     src = e.src_start + (int32_t)scale_u32(x.x, (uint32_t)e.src_num);
     delay = e.dmin + (int32_t)scale_u32(x.y, (uint32_t)e.dspan);
     w = e.w;
+    tar -= e.tar_sub;
 }
 
 // Keys of synapses [base, base + count) of one block; values are offsets
@@ -387,6 +394,9 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     StepArgs& a = s->a;
     a.n = n;
     a.ns = (n + 3) & ~3;  // neuron arrays padded with RAW neurons for 16-byte access
+    a.n_src = n;
+    a.src_base = 0;
+    s->n_src = n;
     const size_t ns = a.ns;
     a.seed = seed;
     memcpy(a.C, lifc, sizeof(a.C));
@@ -441,9 +451,10 @@ mgc_status choose_mode(mgc_sim* s, int requested)
     StepArgs& a = s->a;
     const int D = s->dmax - s->dmin + 1;
     const int dbits = D > 1 ? bits_for(D) : 0;
-    const bool deferred_ok = !s->stdp && s->S > 0 && D <= kMaxBuckets &&
-                             a.tbits + dbits <= 32 &&
-                             ((size_t)s->n * (size_t)D + 1) * sizeof(int64_t) <= kMaxBucketBytes;
+    // (a partition takes the deferred method even without synapses of its own)
+    const bool deferred_ok = !s->stdp && (s->S > 0 || s->partition) && D <= kMaxBuckets &&
+                             std::max(a.tbits, s->sbits) + dbits <= 32 &&
+                             ((size_t)s->n_src * (size_t)D + 1) * sizeof(int64_t) <= kMaxBucketBytes;
     if (requested == MGC_MODE_DEFERRED && !deferred_ok)
         return fail(MGC_ERR_INVALID, "deferred delivery needs static weights and <= %d delays", kMaxBuckets);
     // pull: explicit networks whose per-step pass over all synapses is
@@ -484,11 +495,11 @@ mgc_status begin_layout(mgc_sim* s)
 {
     StepArgs& a = s->a;
     int64_t* row_ptr;
-    CKS(s->alloc(&row_ptr, (size_t)s->n + 1));
+    CKS(s->alloc(&row_ptr, (size_t)s->n_src + 1));
     a.row_ptr = row_ptr;
     if (a.deferred) {
         int64_t* bucket;
-        CKS(s->alloc(&bucket, (size_t)s->n * a.D + 1));
+        CKS(s->alloc(&bucket, (size_t)s->n_src * a.D + 1));
         a.bucket = bucket;
     }
     return MGC_OK;
@@ -587,15 +598,15 @@ mgc_status finish_build(mgc_sim* s)
     StepArgs& a = s->a;
     int64_t* row_ptr = const_cast<int64_t*>(a.row_ptr);
     int64_t max_len = 0;
-    CKS(exclusive_scan(row_ptr, s->n, s->stream));
+    CKS(exclusive_scan(row_ptr, s->n_src, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    if (s->S > 0) CKS(max_row(row_ptr, s->n, &max_len));
+    if (s->S > 0) CKS(max_row(row_ptr, s->n_src, &max_len));
     a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_len + kChunk - 1) / kChunk);
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, s->device));
     int occ = 0;
     if (a.deferred) {
-        const int64_t nb = (int64_t)s->n * a.D;
+        const int64_t nb = (int64_t)s->n_src * a.D;
         int64_t* bucket = const_cast<int64_t*>(a.bucket);
         CKS(exclusive_scan(bucket, nb, s->stream));
         DevTmp t;
@@ -610,7 +621,7 @@ mgc_status finish_build(mgc_sim* s)
         // one step's synapses spread over all warps
         set_chunking(a, (int64_t)gap, kDefaultChunk);
         s->max_gap = (int64_t)gap;
-        CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n, false));
+        CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n_src, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
         CKS(s->alloc(&a.acc_e, kAccBuffers * (size_t)a.ns));  // step buffers, s % kAccBuffers
         CKS(s->alloc(&a.acc_i, kAccBuffers * (size_t)a.ns));
@@ -825,16 +836,92 @@ mgc_status check_tbits(mgc_sim* s)
     StepArgs& a = s->a;
     a.tbits = bits_for(s->n);
     a.tmask = a.tbits >= 32 ? 0xffffffffu : ((1u << a.tbits) - 1u);
+    s->sbits = bits_for(s->n_src);
     if (a.tbits + bits_for((int64_t)s->dmax + 1) > 32)
         return fail(MGC_ERR_INVALID, "max delay %d with %d neurons does not fit a 32-bit CSR word", s->dmax, s->n);
     return MGC_OK;
 }
 
+// One partition of a larger network: the handle simulates neurons
+// [first, first + count) of n_src, holds the synapses that target them
+// (targets renumbered from 0, sources kept) and takes the whole network's
+// delay range, so that every partition has the same history length and
+// exchange window.
+struct PartSpec {
+    int32_t n_src, first, count, dmin, dmax;
+};
+
+// Applies a partition spec to a handle whose neuron arrays are built.
+void apply_part(mgc_sim* s, const PartSpec& p)
+{
+    s->partition = true;
+    s->n_src = p.n_src;
+    s->a.n_src = p.n_src;
+    s->a.src_base = p.first;
+}
+
+mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim** out);
+mgc_status create_fixed_indegree(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, const PartSpec* part,
+                                 mgc_sim** out);
+
 }  // namespace
 
 extern "C" {
 
-mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
+mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out) { return create_explicit(d, nullptr, out); }
+
+mgc_status mgc_create_partition(const mgc_net_desc* d, int32_t first, int32_t count, mgc_sim** out)
+{
+    if (!d || !out) return fail(MGC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (d->n_neurons <= 0 || !d->type) return fail(MGC_ERR_INVALID, "network needs neurons and types");
+    if (first < 0 || count <= 0 || (int64_t)first + count > d->n_neurons)
+        return fail(MGC_ERR_INVALID, "partition [%d, %lld) outside the network's %d neurons", first,
+                    (long long)first + count, d->n_neurons);
+    if (d->stdp) return fail(MGC_ERR_INVALID, "a partition needs static weights (the deferred method)");
+    if (d->mode != MGC_MODE_AUTO && d->mode != MGC_MODE_DEFERRED)
+        return fail(MGC_ERR_INVALID, "a partition runs the deferred method");
+    if (d->n_synapses < 0 || (d->n_synapses > 0 && (!d->syn_src || !d->syn_tar || !d->syn_weight || !d->syn_delay)))
+        return fail(MGC_ERR_INVALID, "synapse arrays missing");
+    // the whole network's delay range; the synapses of this partition's targets
+    PartSpec p{d->n_neurons, first, count, 0x7fffffff, 0};
+    std::vector<int32_t> src, tar, dl;
+    std::vector<float> w;
+    const int32_t last = first + count;
+    for (int64_t k = 0; k < d->n_synapses; ++k) {
+        p.dmin = std::min(p.dmin, d->syn_delay[k]);
+        p.dmax = std::max(p.dmax, d->syn_delay[k]);
+        const int32_t t = d->syn_tar[k];
+        if (t < first || t >= last) continue;
+        src.push_back(d->syn_src[k]);
+        tar.push_back(t - first);
+        dl.push_back(d->syn_delay[k]);
+        w.push_back(d->syn_weight[k]);
+    }
+    if (d->n_synapses == 0) p.dmin = p.dmax = 1;
+    if (p.dmin < 2)
+        return fail(MGC_ERR_INVALID, "partitions exchange spikes every min_delay - 1 steps: min_delay %d < 2", p.dmin);
+    mgc_net_desc loc = *d;
+    loc.n_neurons = count;
+    loc.type = d->type + first;
+    loc.rate = d->rate ? d->rate + first : nullptr;
+    loc.v_init = d->v_init ? d->v_init + first : nullptr;
+    loc.n_synapses = (int64_t)src.size();
+    loc.syn_src = src.data();
+    loc.syn_tar = tar.data();
+    loc.syn_weight = w.data();
+    loc.syn_delay = dl.data();
+    loc.syn_plastic = nullptr;
+    loc.mode = MGC_MODE_DEFERRED;
+    loc.id_offset = d->id_offset + first;  // POISSON draws keyed by the global id
+    return create_explicit(&loc, &p, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim** out)
 {
     if (!d || !out) return fail(MGC_ERR_INVALID, "null argument");
     *out = nullptr;
@@ -852,6 +939,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     s->explicit_net = true;
     CKS(init_common(s.get(), s->n, d->type, d->rate, d->v_init, d->lifconst, d->stdpconst, d->seed,
                     d->raster_steps, d->raster_ids));
+    if (part) apply_part(s.get(), *part);
     StepArgs& a = s->a;
     a.stdp = s->stdp;
     a.id_offset = d->id_offset;
@@ -870,6 +958,10 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
     }
     if (S == 0) dmin = dmax = 1;
     if (dmin < 1) return fail(MGC_ERR_INVALID, "synaptic delay below one step (%d)", dmin);
+    if (part) {
+        dmin = part->dmin;
+        dmax = part->dmax;
+    }
     s->dmin = dmin;
     s->dmax = dmax;
     s->M = dmax + 1;
@@ -903,7 +995,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
             CK(cudaMemcpyAsync(pl, d->syn_plastic, S, cudaMemcpyHostToDevice, s->stream));
         }
         CK(cudaMemsetAsync(bad, 0, 4, s->stream));
-        k_validate<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, s->n, 1 << (32 - a.tbits), bad);
+        k_validate<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, s->n_src, s->n, 1 << (32 - a.tbits), bad);
         int32_t hbad = 0;
         CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
@@ -943,7 +1035,7 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
         CKS(tmp_alloc(t_order, &order, S));
         CKS(tmp_alloc(t_keys2, &keys2, S));
         k_explicit_keys<<<grid_for(S), 256, 0, s->stream>>>(src, dl, S, dbits, s->dmin, keys, vals);
-        CKS(sort_pairs(keys, keys2, vals, order, S, a.tbits + dbits, s->stream));
+        CKS(sort_pairs(keys, keys2, vals, order, S, s->sbits + dbits, s->stream));
         int32_t* csr_src = nullptr;
         uint8_t* plastic = nullptr;
         if (s->stdp && !a.pull) {
@@ -986,10 +1078,14 @@ mgc_status mgc_create(const mgc_net_desc* d, mgc_sim** out)
 // id_offset = start_b and proj_offset = the number of earlier projections.
 // Each block is generated and sorted separately (a block's synapses occupy
 // one contiguous CSR range), so the total may exceed what one sort takes.
-mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, mgc_sim** out)
+// With a partition spec (one block): only the neurons [first, first + count)
+// and the synapses that target them, drawn as in the whole network.
+mgc_status create_fixed_indegree(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, const PartSpec* part,
+                                 mgc_sim** out)
 {
     if (!blocks || !out || n_blocks <= 0) return fail(MGC_ERR_INVALID, "null argument or no blocks");
     *out = nullptr;
+    if (part && n_blocks != 1) return fail(MGC_ERR_INVALID, "a partition is cut from one network");
     const mgc_fixed_indegree_desc& d0 = blocks[0];
     if (d0.mode < MGC_MODE_AUTO || d0.mode > MGC_MODE_DEFERRED)
         return fail(MGC_ERR_INVALID, "unknown mode %d", d0.mode);
@@ -1019,6 +1115,14 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
             e.src_start = (int32_t)start[b] + d.pop_start[sp];
             e.src_num = d.pop_num[sp];
             e.tar_start = (int32_t)start[b] + d.pop_start[tp];
+            int32_t tar_num = d.pop_num[tp];
+            if (part) {  // the targets inside the partition, renumbered from its first neuron
+                const int64_t lo = std::max<int64_t>(e.tar_start, part->first);
+                const int64_t hi = std::min<int64_t>((int64_t)e.tar_start + tar_num, (int64_t)part->first + part->count);
+                e.tar_start = (int32_t)lo;
+                tar_num = (int32_t)std::max<int64_t>(0, hi - lo);
+                e.tar_sub = part->first;
+            }
             e.k = std::max(1, d.pr_k[r]);
             e.dmin = d.pr_dmin[r];
             e.dspan = d.pr_dmax[r] - d.pr_dmin[r] + 1;
@@ -1027,9 +1131,9 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
             e.rid = (int32_t)(pbase[b] + r + d.proj_offset);
             e.id_off = d.id_offset;  // block-local ids are already shifted by start_b
             pt.push_back(e);
-            const int64_t sr = (int64_t)d.pop_num[tp] * d.pr_k[r];
+            const int64_t sr = (int64_t)tar_num * d.pr_k[r];
             S += sr;
-            if (sr > 0) {
+            if ((int64_t)d.pop_num[tp] * d.pr_k[r] > 0) {  // the whole network's delay range
                 dmin = std::min(dmin, d.pr_dmin[r]);
                 dmax = std::max(dmax, d.pr_dmax[r]);
             }
@@ -1042,7 +1146,22 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
     if (start[n_blocks] > 0x7fffffff) return fail(MGC_ERR_INVALID, "more than 2^31-1 neurons");
     const int32_t n = (int32_t)start[n_blocks];
     const int64_t S = sbase[n_blocks];
-    if (S == 0) dmin = dmax = 1;
+    if (dmin > dmax) dmin = dmax = 1;  // no synapses in the whole network
+    PartSpec ps{};
+    if (part) {
+        ps = *part;
+        ps.n_src = n;
+        ps.dmin = dmin;
+        ps.dmax = dmax;
+        if (ps.first < 0 || ps.count <= 0 || (int64_t)ps.first + ps.count > n)
+            return fail(MGC_ERR_INVALID, "partition [%d, %lld) outside the network's %d neurons", ps.first,
+                        (long long)ps.first + ps.count, n);
+        if (dmin < 2)
+            return fail(MGC_ERR_INVALID, "partitions exchange spikes every min_delay - 1 steps: min_delay %d < 2",
+                        dmin);
+        if (d0.mode != MGC_MODE_AUTO && d0.mode != MGC_MODE_DEFERRED)
+            return fail(MGC_ERR_INVALID, "a partition runs the deferred method");
+    }
     std::vector<int8_t> type(n, (int8_t)MGC_RAW);
     std::vector<uint8_t> tpop(n, 0);
     std::vector<float> rate(n, 0.0f), v0(n, d0.lifconst[1]);
@@ -1057,18 +1176,20 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
         if (d.rate) memcpy(rate.data() + start[b], d.rate, 4 * nb);
         if (d.v_init) memcpy(v0.data() + start[b], d.v_init, 4 * nb);
     }
+    const int32_t first = part ? ps.first : 0, nloc = part ? ps.count : n;
     std::unique_ptr<mgc_sim> s(new mgc_sim);
     s->device = d0.device;
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    s->n = n;
+    s->n = nloc;
     s->S = S;
     s->stdp = false;
     float stdpc[6] = {0.1f, -0.01f, 17.0f, 34.0f, 40.0f, 0.0f};
-    CKS(init_common(s.get(), n, type.data(), rate.data(), v0.data(), d0.lifconst, stdpc, d0.seed, d0.raster_steps,
-                    d0.raster_ids));
-    s->tpop_host = std::move(tpop);
+    CKS(init_common(s.get(), nloc, type.data() + first, rate.data() + first, v0.data() + first, d0.lifconst, stdpc,
+                    d0.seed, d0.raster_steps, d0.raster_ids));
+    s->tpop_host.assign(tpop.begin() + first, tpop.begin() + first + nloc);
+    if (part) apply_part(s.get(), ps);
     StepArgs& a = s->a;
-    a.id_offset = d0.id_offset;
+    a.id_offset = d0.id_offset + first;  // POISSON draws keyed by the global id
     s->dmin = dmin;
     s->dmax = dmax;
     s->M = dmax + 1;
@@ -1098,7 +1219,7 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
             const ProjEntry* bpt = dpt + pbase[b];
             const int npr = (int)(pbase[b + 1] - pbase[b]);
             k_fid_keys<<<grid_for(Sb), 256, 0, s->stream>>>(bpt, npr, sbase[b], Sb, dbits, s->dmin, keys, vals);
-            CKS(sort_pairs(keys, keys2, vals, order, Sb, a.tbits + dbits, s->stream));
+            CKS(sort_pairs(keys, keys2, vals, order, Sb, s->sbits + dbits, s->stream));
             k_fid_gather<<<grid_for(Sb), 256, 0, s->stream>>>(bpt, npr, sbase[b], order, Sb, a.tbits, syn + sbase[b]);
             count_keys(s.get(), keys2, Sb);
             CK(cudaGetLastError());
@@ -1110,14 +1231,38 @@ mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blo
     return MGC_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_create_batch(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks, mgc_sim** out)
+{
+    return create_fixed_indegree(blocks, n_blocks, nullptr, out);
+}
+
 mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim** out)
 {
-    return mgc_create_batch(d, 1, out);
+    return create_fixed_indegree(d, 1, nullptr, out);
+}
+
+mgc_status mgc_create_fixed_indegree_partition(const mgc_fixed_indegree_desc* d, int32_t first, int32_t count,
+                                               mgc_sim** out)
+{
+    const PartSpec p{0, first, count, 0, 0};  // sizes and delays filled in from the description
+    return create_fixed_indegree(d, 1, &p, out);
 }
 
 mgc_status mgc_run(mgc_sim* s, int64_t steps)
 {
     if (!s || steps < 0) return fail(MGC_ERR_INVALID, "bad run arguments");
+    if (s->partition) {
+        // a delivery of step x reads spikes of steps <= x - min_delay, so at
+        // most min_delay - 1 steps may run between two imports
+        if (s->pending + steps > s->dmin - 1)
+            return fail(MGC_ERR_INVALID, "partition: %lld steps since the last exchange, at most %d (min_delay - 1)",
+                        (long long)(s->pending + steps), s->dmin - 1);
+        s->pending += (int32_t)steps;
+    }
     CK(cudaSetDevice(s->device));
     int64_t left = steps;
     if (s->a.deferred && s->fused && !s->ahead && left > 0) {
@@ -1170,6 +1315,7 @@ mgc_status mgc_sync(mgc_sim* s)
     int32_t st = 0;
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
     if (st & kStatusBarrier) return fail(MGC_ERR_CUDA, "a grid barrier of the persistent step group timed out");
+    if (st & kStatusExchange) return fail(MGC_ERR_INVALID, "an imported spike id was out of range (exchange refused)");
     if (st) return fail(MGC_ERR_OVERFLOW, "raster buffer overflow (status %d)", st);
     return MGC_OK;
 }
@@ -1280,7 +1426,7 @@ mgc_status mgc_export_csr(mgc_sim* s, int64_t* row_ptr, int32_t* tgt, float* wei
     if (!s) return fail(MGC_ERR_INVALID, "null handle");
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->stream));
-    if (row_ptr) CK(cudaMemcpy(row_ptr, s->a.row_ptr, 8 * ((size_t)s->n + 1), cudaMemcpyDeviceToHost));
+    if (row_ptr) CK(cudaMemcpy(row_ptr, s->a.row_ptr, 8 * ((size_t)s->n_src + 1), cudaMemcpyDeviceToHost));
     if (tgt || weight || delay) {
         // in pieces, so a large CSR needs no second full-size host copy
         const int64_t piece = int64_t(1) << 24;
@@ -1317,12 +1463,15 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->graph_steps = s->graph_steps ? s->graph_steps : kGraphSteps;
     info->device_bytes = (int64_t)s->bytes;
     info->persistent = s->fused && !sched_wanted(s) ? s->persistent : 0;
+    info->first_neuron = s->a.src_base;
+    info->total_neurons = s->n_src;
     return MGC_OK;
 }
 
 mgc_status mgc_profile_steps(mgc_sim* s, int64_t steps, float* ms)
 {
     if (!s || !ms || steps < 0) return fail(MGC_ERR_INVALID, "bad profile arguments");
+    if (s->partition) return fail(MGC_ERR_INVALID, "partition handles run steps only between exchanges (mgc_run)");
     CK(cudaSetDevice(s->device));
     constexpr int kBatch = 64;
     std::vector<cudaEvent_t> ev(4 * kBatch);
@@ -1476,6 +1625,7 @@ mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
 mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* rep)
 {
     if (!s || !rep || steps_per_trial < 1) return fail(MGC_ERR_INVALID, "bad autotune arguments");
+    if (s->partition) return fail(MGC_ERR_INVALID, "partition handles run steps only between exchanges (mgc_run)");
     CK(cudaSetDevice(s->device));
     memset(rep, 0, sizeof(*rep));
     cudaDeviceProp prop;
@@ -1651,6 +1801,7 @@ mgc_status mgc_sched_collect(mgc_sim* s, int32_t on, int32_t reset)
 mgc_status mgc_sched_calibrate(mgc_sim* s, int32_t groups, double* threshold)
 {
     CKS(need_sched(s));
+    if (s->partition) return fail(MGC_ERR_INVALID, "partition handles run steps only between exchanges (mgc_run)");
     if (groups < 4 || groups > kMaxDataset / 2) return fail(MGC_ERR_INVALID, "calibrate with 4..%d groups", kMaxDataset / 2);
     SchedState h;
     s->sched_forced_h = true;
@@ -1855,7 +2006,7 @@ std::vector<Segment> state_segments(mgc_sim* s)
     if (a.deferred) {
         v.push_back({a.acc_e, 4 * kAccBuffers * ns});
         v.push_back({a.acc_i, 4 * kAccBuffers * ns});
-        v.push_back({a.hist_ids, 4 * (size_t)a.H * n});
+        v.push_back({a.hist_ids, 4 * (size_t)a.H * (size_t)s->n_src});
         v.push_back({a.hist_cnt, 4 * (size_t)a.H});
     } else {
         v.push_back({a.ring_e, 4 * (size_t)s->M * ns});
@@ -1896,6 +2047,8 @@ mgc_status mgc_checkpoint_size(mgc_sim* s, int64_t* bytes)
 mgc_status mgc_checkpoint_save(mgc_sim* s, void* buf, int64_t bytes)
 {
     if (!s || !buf) return fail(MGC_ERR_INVALID, "null argument");
+    if (s->partition && s->pending)
+        return fail(MGC_ERR_INVALID, "partition: save a checkpoint right after an exchange");
     CK(cudaSetDevice(s->device));
     const CheckpointHeader h = checkpoint_header(s);
     if (bytes < h.bytes) return fail(MGC_ERR_INVALID, "checkpoint buffer of %lld bytes, need %lld", (long long)bytes,
@@ -1943,6 +2096,184 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
         CK(cudaMemcpy(s->a.ev_mark, &ev, 8, cudaMemcpyHostToDevice));
     }
     s->ahead = h.ahead != 0;
+    return MGC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Spike exchange between partitions.  A partition handle's history holds the
+// spike ids (whole-network ids) of every neuron; its own neuron update writes
+// its neurons' spikes, and the other partitions' spikes of the steps run since
+// the last exchange are appended after them.  Deliveries of step x read the
+// spikes of steps <= x - min_delay, so exchanging every <= min_delay - 1 steps
+// hands each partition every spike before it is delivered.
+// ---------------------------------------------------------------------------
+namespace {
+
+// History slot of the step `back` steps before the device's current one.
+__device__ __forceinline__ int32_t slot_back(const StepArgs& a, int32_t back)
+{
+    const int32_t h = a.slots[1] - back;
+    return h < 0 ? h + a.H : h;
+}
+
+// Block j: the spikes of step (current - count + j) into counts[j] and, when
+// they fit, into ids after those of the earlier steps.
+__global__ void k_part_export(StepArgs a, int32_t count, int32_t* counts, int32_t* ids, int64_t cap)
+{
+    const int32_t j = blockIdx.x;
+    int64_t off = 0;
+    for (int32_t q = 0; q < j; ++q) off += a.hist_cnt[slot_back(a, count - q)];
+    const int32_t hs = slot_back(a, count - j);
+    const int32_t c = a.hist_cnt[hs];
+    if (threadIdx.x == 0) counts[j] = c;
+    if (!ids || off + c > cap) return;  // the host reports the overflow from the counts
+    const int32_t* src = a.hist_ids + (size_t)hs * (size_t)a.n_src;
+    for (int32_t i = threadIdx.x; i < c; i += blockDim.x) ids[off + i] = src[i];
+}
+
+// Block (j, r), r != self: rank r's spikes of step (current - count + j),
+// stored from ids + r * stride after its spikes of the earlier steps, go
+// after the slot's own spikes and those of the ranks before r.  cnt is
+// [nranks][count].  An id outside the network, or a slot that would hold
+// more than every neuron, sets kStatusExchange and the counts stay as they
+// were (k_part_commit), so no delivery reads what was written.
+__global__ void k_part_import(StepArgs a, int32_t count, int32_t nranks, int32_t self, const int32_t* cnt,
+                              const int32_t* ids, int64_t stride)
+{
+    const int32_t j = blockIdx.x, r = blockIdx.y;
+    if (r == self) return;
+    const int32_t hs = slot_back(a, count - j);
+    const int64_t own = a.hist_cnt[hs];
+    int64_t dst = own, total = own;
+    for (int32_t q = 0; q < nranks; ++q) {
+        if (q == self) continue;
+        const int32_t c = cnt[(size_t)q * count + j];
+        if (q < r) dst += c;
+        total += c;
+    }
+    if (total > a.n_src) {
+        if (threadIdx.x == 0) atomicOr(a.status, kStatusExchange);
+        return;
+    }
+    int64_t src = (int64_t)r * stride;
+    for (int32_t q = 0; q < j; ++q) src += cnt[(size_t)r * count + q];
+    const int32_t c = cnt[(size_t)r * count + j];
+    int32_t* out = a.hist_ids + (size_t)hs * (size_t)a.n_src;
+    for (int32_t i = threadIdx.x; i < c; i += blockDim.x) {
+        const int32_t id = ids[src + i];
+        if (id < 0 || id >= a.n_src) {
+            atomicOr(a.status, kStatusExchange);
+            continue;
+        }
+        out[dst + i] = id;
+    }
+}
+
+// The slots' counts grow by the imported spikes, unless the import failed.
+__global__ void k_part_commit(StepArgs a, int32_t count, int32_t nranks, int32_t self, const int32_t* cnt)
+{
+    if (*(volatile int32_t*)a.status & kStatusExchange) return;
+    for (int32_t j = threadIdx.x; j < count; j += blockDim.x) {
+        int32_t add = 0;
+        for (int32_t q = 0; q < nranks; ++q)
+            if (q != self) add += cnt[(size_t)q * count + j];
+        a.hist_cnt[slot_back(a, count - j)] += add;
+    }
+}
+
+mgc_status xch_reserve(mgc_sim* s, int64_t count)
+{
+    if (s->xch_cap >= count) return MGC_OK;
+    CKS(s->alloc(&s->xch, (size_t)count));
+    s->xch_cap = count;
+    return MGC_OK;
+}
+
+// Kernels read and write the exchange buffers directly: device memory of the
+// handle's device, managed memory, or page-locked host memory mapped into
+// the device's address space.
+bool device_accessible(const void* p, int device)
+{
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (at.type == cudaMemoryTypeDevice) return at.device == device;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    if (at.type == cudaMemoryTypeHost) return at.devicePointer == p;
+    return false;
+}
+
+mgc_status check_window(mgc_sim* s, int32_t count)
+{
+    if (!s->partition) return fail(MGC_ERR_INVALID, "not a partition handle");
+    if (count < 1 || count != s->pending)
+        return fail(MGC_ERR_INVALID, "exchange the %d steps run since the last import (got %d)", s->pending, count);
+    return MGC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_part_export(mgc_sim* s, int32_t count, int32_t* counts, int32_t* ids, int64_t ids_cap, int64_t* total)
+{
+    if (!s || !counts || !total || ids_cap < 0) return fail(MGC_ERR_INVALID, "null argument");
+    CKS(check_window(s, count));
+    CK(cudaSetDevice(s->device));
+    if (ids_cap > 0 && (!ids || !device_accessible(ids, s->device)))
+        return fail(MGC_ERR_INVALID, "spike id buffer is not device memory of device %d", s->device);
+    CKS(xch_reserve(s, count));
+    k_part_export<<<count, 256, 0, s->stream>>>(s->a, count, s->xch, ids_cap > 0 ? ids : nullptr, ids_cap);
+    CK(cudaGetLastError());
+    s->launches += 1;
+    CK(cudaMemcpyAsync(counts, s->xch, 4 * (size_t)count, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    int64_t sum = 0;
+    for (int32_t j = 0; j < count; ++j) sum += counts[j];
+    *total = sum;
+    if (sum > ids_cap) return fail(MGC_ERR_OVERFLOW, "%lld spike ids to export, room for %lld", (long long)sum,
+                                   (long long)ids_cap);
+    return MGC_OK;
+}
+
+mgc_status mgc_part_import(mgc_sim* s, int32_t count, int32_t nranks, int32_t self, const int32_t* counts,
+                           const int32_t* ids, int64_t stride)
+{
+    if (!s || !counts || nranks < 1 || self < 0 || self >= nranks || stride < 0)
+        return fail(MGC_ERR_INVALID, "bad import arguments");
+    CKS(check_window(s, count));
+    bool any = false;
+    for (int32_t r = 0; r < nranks; ++r) {
+        int64_t sum = 0;
+        for (int32_t j = 0; j < count; ++j) {
+            const int32_t c = counts[(size_t)r * count + j];
+            if (c < 0 || c > s->n_src) return fail(MGC_ERR_INVALID, "rank %d step %d: bad spike count %d", r, j, c);
+            sum += c;
+        }
+        if (sum > stride) return fail(MGC_ERR_INVALID, "rank %d sends %lld ids in a stride of %lld", r,
+                                      (long long)sum, (long long)stride);
+        any |= r != self && sum > 0;
+    }
+    CK(cudaSetDevice(s->device));
+    if (any && (!ids || !device_accessible(ids, s->device)))
+        return fail(MGC_ERR_INVALID, "spike id buffer is not device memory of device %d", s->device);
+    CKS(xch_reserve(s, (int64_t)nranks * count));
+    CK(cudaMemcpyAsync(s->xch, counts, 4 * (size_t)nranks * count, cudaMemcpyHostToDevice, s->stream));
+    if (any) {
+        k_part_import<<<dim3(count, nranks), 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch, ids, stride);
+        k_part_commit<<<1, 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch);
+        CK(cudaGetLastError());
+        s->launches += 2;
+    }
+    CK(cudaStreamSynchronize(s->stream));  // the counts were staged from the caller's memory
+    int32_t st = 0;
+    CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
+    if (st & kStatusExchange) return fail(MGC_ERR_INVALID, "an imported spike id was out of range (exchange refused)");
+    s->pending = 0;
     return MGC_OK;
 }
 
