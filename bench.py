@@ -128,7 +128,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend="gloo"):
+    """Process group of a multi-rank run: gloo for the host-side timing
+    reductions, NCCL where spike ids cross GPUs (partitioned workload)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -136,7 +138,9 @@ def dist_init():
         import datetime
 
         import torch.distributed as dist
-        backend = "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
     return ws, rank, local
 
@@ -147,24 +151,27 @@ def barrier(ws):
         dist.barrier()
 
 
+def _reduce(x, op):
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"   # NCCL reduces device tensors only
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
 def allmax(ws, x):
     if ws == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _reduce(x, dist.ReduceOp.MAX)
 
 
 def allsum(ws, x):
     if ws == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, dist.ReduceOp.SUM)
 
 
 # --------------------------------------------------------------------------
@@ -438,6 +445,61 @@ def run_ours(a, ws, rank, local):
                                         "accumulators fed by streamed 8-byte records; plain stream "
                                         "of the same records"},
         }
+        print(json.dumps(line), flush=True)
+
+
+def run_partition(a, ws, rank, local):
+    """The large Brunel network split into one partition per rank (strong
+    scaling): each rank simulates its neuron range on its GPU and the ranks
+    all-gather spike ids every min_delay - 1 = 9 steps (NCCL; at one rank the
+    exchange has nothing to send and measures the windowing's own cost).
+    Device time on the partition's stream, max over ranks; at one rank the
+    end state is compared with the unpartitioned handle's."""
+    import torch
+
+    import mgbrain_b200 as mgb
+    from mgbrain_b200.partition import DistributedPartition, PartitionGroup, split
+    torch.cuda.set_device(local)
+    w = workload(a.scale)
+    first, count = split(w["n"], ws)[rank]
+    t0 = time.perf_counter()
+    sim = mgb.Simulator.fixed_indegree(w["pops"], w["projs"], w["lif"], rate=w["rate"], v_init=w["v0"],
+                                       conn_seed=1, seed=1, device=local, raster_ids=-1, part=(first, count))
+    sim.sync()
+    build_s = time.perf_counter() - t0
+    part = DistributedPartition(sim, device=f"cuda:{local}") if ws > 1 else PartitionGroup([sim], [local])
+    for _ in range(a.warmup):
+        part.run(CHUNK)
+    torch.cuda.synchronize()
+    barrier(ws)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0 = sim.info()["events"]
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            part.run(CHUNK)
+        e1.record(stream)
+        e1.synchronize()
+    ms = allmax(ws, e0.elapsed_time(e1))
+    events = allsum(ws, sim.info()["events"] - ev0)
+    line = {"workload": "partition", "metric": METRIC, "value": events / (ms / 1e3), "unit": "events/s",
+            "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "scaling": "strong", "window_steps": part.window,
+            "sim_s_per_wall_s": a.steps * CHUNK * DT / (ms / 1e3), "build_s": build_s,
+            "partition": {"first": first, "neurons": count, "synapses": sim.S},
+            "exchange": "NCCL all-gather of counts, then of ids" if ws > 1 else "none (one partition)",
+            "clocks": clk.summary()}
+    if ws == 1:
+        whole = make_sim(w, local, seed=1, record=False)
+        whole.run(CHUNK * (a.warmup + a.steps))
+        ws_ = whole.state()
+        st = sim.state()
+        line["identical_to_whole"] = bool(np.array_equal(st["V"].view(np.int32), ws_["V"].view(np.int32)) and
+                                          np.array_equal(st["fire_cnt"], ws_["fire_cnt"]))
+        whole.close()
+    sim.close()
+    if rank == 0:
         print(json.dumps(line), flush=True)
 
 
@@ -747,10 +809,11 @@ def main():
     ap.add_argument("--no-driven", action="store_true")
     ap.add_argument("--ref-syn", type=float, default=1e8)
     ap.add_argument("--ref-seconds", type=float, default=1.0)
-    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched", "refgpu"],
+    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched", "refgpu", "partition"],
                     help="brunel1m: the 1M-neuron network (default); sweep: batched vs plain "
                          "parameter sweep; sched: the step scheduler's modes on a periodic drive; refgpu: "
-                         "the reference's own simulator and this core on the reference's benchmark network")
+                         "the reference's own simulator and this core on the reference's benchmark network; "
+                         "partition: the 1M-neuron network split over the ranks, spike ids exchanged")
     ap.add_argument("--sched-train-groups", type=int, default=200)
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
@@ -764,9 +827,11 @@ def main():
                     help="only build the network at --scale, run --warmup bench steps, 300 "
                          "steps as timed, and 300 profiled steps (separate kernels); for ncu captures")
     a = ap.parse_args()
-    ws, rank, local = dist_init()
+    ws, rank, local = dist_init("nccl" if a.workload == "partition" and a.impl == "ours" else "gloo")
     try:
-        if a.workload == "sweep":
+        if a.workload == "partition" and a.impl == "ours":
+            run_partition(a, ws, rank, local)
+        elif a.workload == "sweep":
             run_sweep(a, ws, rank, local)
         elif a.workload == "sched":
             run_sched(a, ws, rank, local)

@@ -194,6 +194,21 @@ mgc_status mgc_part_export(mgc_sim* sim, int32_t count, int32_t* counts, int32_t
 mgc_status mgc_part_import(mgc_sim* sim, int32_t count, int32_t nranks, int32_t self, const int32_t* counts,
                            const int32_t* ids, int64_t stride);
 
+/* Host-side fault injection for callers' error paths: the n-th device
+ * allocation from now (n >= 1) fails as if the device were out of memory;
+ * 0 turns it off.  The entry point that meets it returns MGC_ERR_NOMEM and
+ * frees what it had allocated.  No reference counterpart (the reference's
+ * CUDACHECK exits the process, cudamem.cuh:8-18). */
+mgc_status mgc_fault_inject_alloc(int64_t n);
+
+/* Self-test of the step groups' bounded waits, with no fault: runs the
+ * pipelined group's phase wait (which = 0) or the per-step grid barrier
+ * (which = 1) against a counter that nothing advances.  *status gets the
+ * device status bits (4: the wait gave up, as mgc_sync reports it for a
+ * step group), *ms the kernel's duration; the device stays usable.  No
+ * reference counterpart (the reference has no waits inside kernels). */
+mgc_status mgc_selftest_wait_timeout(int32_t device, int32_t which, int32_t* status, double* ms);
+
 /* Enqueues `steps` steps on the handle's stream and returns without
  * waiting.  Replaces the step loop of MGSimulator::simulate_sparse
  * (mgsim.cpp:794-857) calling mgsim_step_sparse (mgcore.cu:535-554);

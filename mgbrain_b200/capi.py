@@ -28,6 +28,7 @@ EXPORTED = (
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
+    "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout",
 )
 
 
@@ -109,8 +110,10 @@ def lib():
     L.mgc_create_fixed_indegree_partition.argtypes = [C.POINTER(FixedInDegreeDesc), i32, i32, C.POINTER(vp)]
     L.mgc_part_export.argtypes = [vp, i32, vp, vp, i64, C.POINTER(i64)]
     L.mgc_part_import.argtypes = [vp, i32, i32, i32, vp, vp, i64]
+    L.mgc_fault_inject_alloc.argtypes = [i64]
+    L.mgc_selftest_wait_timeout.argtypes = [i32, i32, C.POINTER(i32), C.POINTER(C.c_double)]
     for name in ("mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export",
-                 "mgc_part_import"):
+                 "mgc_part_import", "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout"):
         getattr(L, name).restype = C.c_int
     L.mgc_run.argtypes = [vp, i64]
     L.mgc_sync.argtypes = [vp]
@@ -187,6 +190,19 @@ def mlp_gradient(params, x, y, device=0):
     loss = np.zeros(1, np.float32)
     check(lib().mgc_mlp_gradient(int(device), _ptr(p), _ptr(xs), _ptr(ys), int(xs.shape[0]), _ptr(g), _ptr(loss)))
     return float(loss[0]), g
+
+
+def fault_inject_alloc(n):
+    """The n-th device allocation from now fails as out of memory (0: off)."""
+    check(lib().mgc_fault_inject_alloc(int(n)))
+
+
+def selftest_wait_timeout(which, device=0):
+    """(status bits, ms): a step-group wait (0 phase wait, 1 grid barrier)
+    run against a counter nothing advances; 4 = it gave up."""
+    st, ms = C.c_int32(), C.c_double()
+    check(lib().mgc_selftest_wait_timeout(int(device), int(which), C.byref(st), C.byref(ms)))
+    return st.value, ms.value
 
 
 def effective_steps(steps, min_delay):

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -53,6 +54,23 @@ mgc_status fail(mgc_status st, const char* fmt, ...)
         mgc_status s_ = (expr);      \
         if (s_ != MGC_OK) return s_; \
     } while (0)
+
+// Host-side fault injection (mgc_fault_inject_alloc): when positive, the
+// device allocation that brings the count to zero fails as if the device
+// were out of memory.
+std::atomic<int64_t> g_fail_alloc{0};
+
+cudaError_t dev_malloc(void** p, size_t bytes)
+{
+    int64_t n = g_fail_alloc.load();
+    while (n > 0) {
+        if (g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+            if (n == 1) return cudaErrorMemoryAllocation;
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
 
 constexpr int64_t kDefaultRasterSteps = 1 << 16;
 constexpr int kGraphSteps = 64;
@@ -125,7 +143,7 @@ struct mgc_sim {
     {
         void* v = nullptr;
         size_t b = std::max<size_t>(count, 1) * sizeof(T);
-        CK(cudaMalloc(&v, b));
+        CK(dev_malloc(&v, b));
         allocs.push_back(v);
         bytes += b;
         if (zero) CK(cudaMemsetAsync(v, 0, b, stream));
@@ -156,7 +174,7 @@ struct DevTmp {
 template <class T>
 mgc_status tmp_alloc(DevTmp& t, T** p, size_t count)
 {
-    CK(cudaMalloc(&t.p, std::max<size_t>(count, 1) * sizeof(T)));
+    CK(dev_malloc(&t.p, std::max<size_t>(count, 1) * sizeof(T)));
     *p = static_cast<T*>(t.p);
     return MGC_OK;
 }
@@ -339,7 +357,7 @@ mgc_status sort_pairs(const K* keys_in, K* keys_out, const uint32_t* vals_in, ui
     size_t tb = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
     DevTmp t;
-    CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
+    CK(dev_malloc(&t.p, std::max<size_t>(tb, 1)));
     CK(cub::DeviceRadixSort::SortPairs(t.p, tb, keys_in, keys_out, vals_in, vals_out, (int)S, 0, key_bits, st));
     CK(cudaStreamSynchronize(st));
     return MGC_OK;
@@ -353,7 +371,7 @@ mgc_status exclusive_scan(T* v, int64_t count, cudaStream_t st)
     size_t tb = 0;
     CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, v, v, (int)(count + 1), st));
     DevTmp t;
-    CK(cudaMalloc(&t.p, std::max<size_t>(tb, 1)));
+    CK(dev_malloc(&t.p, std::max<size_t>(tb, 1)));
     CK(cub::DeviceScan::ExclusiveSum(t.p, tb, v, v, (int)(count + 1), st));
     return MGC_OK;
 }
@@ -2274,6 +2292,75 @@ mgc_status mgc_part_import(mgc_sim* s, int32_t count, int32_t nranks, int32_t se
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
     if (st & kStatusExchange) return fail(MGC_ERR_INVALID, "an imported spike id was out of range (exchange refused)");
     s->pending = 0;
+    return MGC_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Failure handling without a GPU fault: host-side allocation failures, and
+// the step groups' bounded waits run against a counter that nothing advances.
+// ---------------------------------------------------------------------------
+namespace {
+
+// which = 0: the pipelined group's phase wait for phase 1 (gridDim.x
+// arrivals on counter 1; none come).  which = 1: the per-step grid barrier
+// with block 0 alone arriving (the other blocks leave).  Both give up after
+// their spin limit with kStatusBarrier.
+__global__ void k_wait_selftest(StepArgs a, int32_t which)
+{
+    __shared__ int abort_flag;
+    if (threadIdx.x == 0) abort_flag = 0;
+    __syncthreads();
+    if (which == 0) {
+        wait_phase(a, 1, &abort_flag);
+    } else {
+        if (blockIdx.x != 0) return;
+        grid_barrier(a, &abort_flag);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_fault_inject_alloc(int64_t n)
+{
+    if (n < 0) return fail(MGC_ERR_INVALID, "allocation count must be >= 0");
+    g_fail_alloc.store(n);
+    return MGC_OK;
+}
+
+mgc_status mgc_selftest_wait_timeout(int32_t device, int32_t which, int32_t* status, double* ms)
+{
+    if (!status || !ms || which < 0 || which > 1) return fail(MGC_ERR_INVALID, "bad self-test arguments");
+    CKS(pick_device(device));
+    DevTmp tb, ts;
+    unsigned int* bar;
+    int32_t* st;
+    CKS(tmp_alloc(tb, &bar, 4));
+    CKS(tmp_alloc(ts, &st, 1));
+    CK(cudaMemset(bar, 0, 4 * sizeof(unsigned int)));
+    CK(cudaMemset(st, 0, sizeof(int32_t)));
+    StepArgs a{};
+    a.bar = bar;
+    a.status = st;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0));
+    k_wait_selftest<<<which == 0 ? 1 : 2, 32>>>(a, which);
+    const cudaError_t le = cudaGetLastError();
+    CK(cudaEventRecord(e1));
+    const cudaError_t se = cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(le);
+    CK(se);
+    CK(cudaMemcpy(status, st, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    *ms = t;
     return MGC_OK;
 }
 

@@ -5,6 +5,11 @@ cuda:0 and exchanges spike ids with the other ranks through gloo; rank 0
 then gathers every rank's raster and state and compares them with the whole
 network run on its own.
 
+`fail`: no GPU.  As `fake`, but rank 1 raises inside its fifth window and
+its process ends without joining the next exchange; the other ranks must
+learn of it from their collective (an error, within the process group's
+short timeout) instead of waiting for good.
+
 `fake [world steps]`: no GPU.  A stand-in partition with the handle's
 exchange interface fires a fixed pseudo-random pattern and keeps the spike
 history the way the library does (own spikes first, then the imported ones);
@@ -41,8 +46,12 @@ class FakePartition:
     def info(self):
         return {"min_delay": self.min_delay}
 
+    fail_at = None              # window at which run() raises (failure test)
+
     def run(self, k):
         assert self.pending + k <= self.min_delay - 1, "ran past the exchange window"
+        if self.fail_at is not None and len(self.hist) // max(1, self.min_delay - 1) >= self.fail_at:
+            raise RuntimeError("injected rank failure")
         for _ in range(k):
             s = len(self.hist)
             own = self.spikes[s]
@@ -88,6 +97,32 @@ def fake(world_steps):
     print(json.dumps(out), flush=True)
 
 
+def fail():
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    from mgbrain_b200.partition import DistributedPartition, split
+    ws, rank = int(os.environ["WORLD_SIZE"]), int(os.environ["RANK"])
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=15))
+    n_src, min_delay = 1000, 4
+    spikes = pattern(n_src, 60)
+    first, n = split(n_src, ws)[rank]
+    sim = FakePartition(n_src, first, n, min_delay, spikes)
+    if rank == 1:
+        sim.fail_at = 5
+    part = DistributedPartition(sim, device="cpu")
+    t0 = time.time()
+    try:
+        part.run(60)
+        out = {"rank": rank, "detected": False}
+    except Exception as e:  # noqa: BLE001 - any collective error is the detection
+        out = {"rank": rank, "detected": True, "error": type(e).__name__, "seconds": time.time() - t0,
+               "steps": len(sim.hist)}
+    print(json.dumps(out), flush=True)
+    os._exit(3 if rank == 1 else 0)   # no destroy: a failed group cannot be torn down collectively
+
+
 def gpu():
     import torch.distributed as dist
     import mgbrain_b200 as mgb
@@ -131,5 +166,7 @@ def gpu():
 if __name__ == "__main__":
     if sys.argv[1] == "fake":
         fake(int(sys.argv[2]) if len(sys.argv) > 2 else 50)
+    elif sys.argv[1] == "fail":
+        fail()
     else:
         gpu()

@@ -41,6 +41,28 @@ def test_gloo_ranks_share_every_spike(world):
         assert o["equal"], o
 
 
+def test_failed_rank_is_detected_not_waited_for():
+    """Rank 1 fails inside a window and leaves; rank 0's next exchange ends
+    with an error (peer gone, or the group's 15 s timeout) instead of
+    hanging."""
+    port = free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2",
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, os.path.join(HERE, "partition_worker.py"), "fail"],
+                                      env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        o, e = p.communicate(timeout=240)
+        outs.append((p.returncode, json.loads(o.strip().splitlines()[-1])))
+    (rc0, o0), (rc1, o1) = outs
+    assert rc1 == 3 and o1["detected"] and o1["error"] == "RuntimeError"
+    assert rc0 == 0 and o0["detected"], o0
+    assert o0["seconds"] < 120
+    assert o0["steps"] >= 15        # the windows before the failure completed
+
+
 def test_split_and_window():
     assert split(10, 3) == [(0, 3), (3, 3), (6, 4)]
     assert sum(c for _, c in split(1_100_000, 8)) == 1_100_000
