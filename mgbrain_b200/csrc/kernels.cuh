@@ -84,8 +84,8 @@ struct StepArgs {
     const uint8_t* in_plastic;  // [S] or null
     // neuron state
     const int8_t* type;
-    const float* rate;
-    float* V;
+    const float* rate;    // POISSON per-step probabilities (staging; the update reads them from V)
+    float* V;             // V; for POISSON neurons their probability
     float* Iexc;
     float* Iinh;
     int32_t* refrac;
@@ -209,8 +209,11 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 {
     bool fired = false;
     if (t == kPOISSON) {
-        // mgcore.cu:121-131: fires when the per-step probability beats the draw
-        fired = __ldg(a.rate + i) > poisson_uniform(a.seed, (int64_t)i + a.id_offset, s);
+        // mgcore.cu:121-131: fires when the per-step probability beats the
+        // draw.  A POISSON neuron's V is never used, so its V slot holds the
+        // probability (mgc_set_rates writes it there): it arrives with the
+        // group's loads instead of a second, dependent load.
+        fired = v > poisson_uniform(a.seed, (int64_t)i + a.id_offset, s);
     } else if (t == kLIFB) {
         // mgcore.cu:164-196: threshold on the old V, then leak + input
         if (rf > 0) {
@@ -855,24 +858,33 @@ __device__ __forceinline__ bool wait_phase(const StepArgs& a, int32_t phase, int
     return *abort_flag == 0;
 }
 
-// The block's step is done: its spike counts per trace population and its
-// delivered events go out (and the block counters are cleared for reuse two
-// steps later), then the block arrives on the phase counter.
-__device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase, int64_t s, int* pop, unsigned long long* ev)
+// The block's step is done, then it arrives on the phase counter.  With the
+// schedule trace on, its spike counts per trace population and its delivered
+// events go into step s's trace row and the events counter every step (and
+// the block counters are cleared for reuse); without it the block's events
+// accumulate in `ev` and go out once, with the group's last step (flush), so
+// that the blocks do not queue on one counter every step.
+__device__ __forceinline__ void arrive(const StepArgs& a, int32_t phase, int64_t s, int* pop, unsigned long long* ev,
+                                       bool flush)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
         if (pop) {
-            float* row = a.trace + (s & (kTraceSteps - 1)) * kTraceCols;
-            for (int c = 0; c < kTracePops; ++c) {
-                if (a.trace && pop[c]) atomicAdd(row + c, (float)pop[c]);
-                pop[c] = 0;
+            if (a.trace) {
+                float* row = a.trace + (s & (kTraceSteps - 1)) * kTraceCols;
+                for (int c = 0; c < kTracePops; ++c) {
+                    if (pop[c]) atomicAdd(row + c, (float)pop[c]);
+                    pop[c] = 0;
+                }
+                if (*ev) {
+                    atomicAdd(a.events, *ev);
+                    atomicAdd(row + kTracePops, (float)*ev);
+                }
+                *ev = 0;
+            } else if (flush) {
+                if (*ev) atomicAdd(a.events, *ev);
+                *ev = 0;
             }
-            if (*ev) {
-                atomicAdd(a.events, *ev);
-                if (a.trace) atomicAdd(row + kTracePops, (float)*ev);
-            }
-            *ev = 0;
         }
         __threadfence();
         atomicAdd(a.bar + (phase % kPhaseCounters), 1u);
@@ -931,10 +943,11 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
         __syncthreads();
         deliver_tasks(a, s0 + 1, s0, h0, pre, warp, nwarps);
     }
-    arrive(a, 0, 0, nullptr, nullptr);
+    arrive(a, 0, 0, nullptr, nullptr, false);
     for (int32_t i = 0; i < nsteps; ++i) {
         const int64_t s = s0 + i;
         const int32_t hs = hs_of(s);
+        const bool deliver = s + 2 <= s_end;
         // every block has finished step s-2 (phase i-1; for i = 1 the prologue)
         if (i >= 1 && !wait_phase(a, i - 1, &abort_flag)) return;
         if (lead && s + 2 <= s_end) a.hist_cnt[hs_of(s + 2)] = 0;
@@ -943,14 +956,14 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
             for (int c = 0; c < kTraceCols; ++c) row[c] = 0.f;
         }
         if (rec && blockIdx.x == 0 && i >= 2) raster_copy(a, s - 2, hs_of(s - 2), rstep0, rbase);
-        const bool deliver = s + 2 <= s_end;
-        if (deliver && threadIdx.x < 32) deliver_prefix(a, s + 2, s, hs, pre);
         const int b = i & 1;
+        unsigned long long* evb = a.trace ? &blk_ev[b] : &blk_ev[0];  // per step, or for the group
+        if (deliver && threadIdx.x < 32) deliver_prefix(a, s + 2, s, hs, pre);
         neuron_groups<2, CUR>(a, s, hs, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, 0,
                               a.trace ? pop_cnt[b] : nullptr, false);
         __syncthreads();
-        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps, &blk_ev[b]);
-        arrive(a, i + 1, s, pop_cnt[b], &blk_ev[b]);
+        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps, evb);
+        arrive(a, i + 1, s, pop_cnt[b], evb, i == nsteps - 1);
     }
     // the group's last steps: all blocks done (phases n-1 and n), remaining raster, the clock
     if (nsteps >= 1 && !wait_phase(a, nsteps - 1, &abort_flag)) return;
@@ -959,7 +972,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
         for (int64_t x = (nsteps >= 2 ? s_end - 2 : s0); x < s_end; ++x) raster_copy(a, x, hs_of(x), rstep0, rbase);
     if (lead) {
         if (rec) *a.raster_pos = rbase;
-        if (a.trace) *a.ev_mark = *(volatile unsigned long long*)a.events;  // every block's events are in
+        *a.ev_mark = *(volatile unsigned long long*)a.events;  // every block's events are in
         a.slots[0] = (int32_t)((slot0 + nsteps) % a.M);
         a.slots[1] = hs_of(s_end);
         __threadfence();

@@ -95,6 +95,8 @@ struct mgc_sim {
     int32_t n_src = 0;   // CSR rows: n, or the whole network's neurons (partition)
     int sbits = 1;       // bits of a source id in the sort keys
     bool partition = false;  // simulates neurons [a.src_base, a.src_base + n) of a larger network
+    std::vector<int32_t> pois_idx;  // POISSON neurons, and the V they report (their V slot holds
+    std::vector<float> pois_v;      // the per-step probability)
     int32_t pending = 0;     // partition: steps run since the last spike import
     int32_t* xch = nullptr;  // partition: device scratch of the exchange (spike counts)
     int64_t xch_cap = 0;
@@ -194,6 +196,15 @@ __global__ void k_count_buckets(const uint32_t* key, int64_t S, int dbits, int D
     {
         const uint32_t src = key[k] >> dbits, b = key[k] & ((1u << dbits) - 1u);
         atomicAdd(reinterpret_cast<unsigned long long*>(cnt + (size_t)src * D + b), 1ull);
+    }
+}
+
+// New POISSON probabilities into the neurons' V slots.
+__global__ void k_rate_to_v(const int8_t* type, const float* rate, float* V, int32_t n)
+{
+    GRID_STRIDE(i, n)
+    {
+        if (type[i] == kPOISSON) V[i] = rate[i];
     }
 }
 
@@ -434,6 +445,16 @@ mgc_status init_common(mgc_sim* s, int32_t n, const int8_t* type, const float* r
     a.rate = d_rate;
     std::vector<float> v0(ns, 0.0f);
     for (int32_t i = 0; i < n; ++i) v0[i] = v_init ? v_init[i] : lifc[1];  // mgsim.cpp:97
+    // a POISSON neuron's V slot holds its probability (the update reads it
+    // there); the V it reports is the initial one, which never changes
+    s->pois_idx.clear();
+    s->pois_v.clear();
+    for (int32_t i = 0; i < n; ++i)
+        if (type[i] == kPOISSON) {
+            s->pois_idx.push_back(i);
+            s->pois_v.push_back(v0[i]);
+            v0[i] = rate ? rate[i] : 0.0f;
+        }
     CKS(s->upload(&a.V, v0.data(), ns));
     CKS(s->alloc(&a.Iexc, ns));
     CKS(s->alloc(&a.Iinh, ns));
@@ -1293,7 +1314,10 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         const int p = s->persistent, v = s->fused_variant;
         while (left > 0) {
             int32_t n = (int32_t)std::min<int64_t>(left, kPersistentSteps);
-            void* args[] = {&s->a, &n};
+            // the schedule trace only while the scheduler's graph runs
+            StepArgs ga = s->a;
+            ga.trace = nullptr;
+            void* args[] = {&ga, &n};
             CK(cudaMemsetAsync(s->a.bar, 0, 4 * sizeof(unsigned int), s->stream));  // clean barriers
             const cudaError_t e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v),
                                                               dim3(s->group_grid_v[p - 1][v]), dim3(kPushBlock),
@@ -1343,6 +1367,9 @@ mgc_status mgc_set_rates(mgc_sim* s, const float* rate, int32_t n)
     if (!s || !rate || n != s->n) return fail(MGC_ERR_INVALID, "rate array must hold n_neurons entries");
     CK(cudaSetDevice(s->device));
     CK(cudaMemcpyAsync(const_cast<float*>(s->a.rate), rate, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+    k_rate_to_v<<<grid_for(n), 256, 0, s->stream>>>(s->a.type, s->a.rate, s->a.V, n);
+    CK(cudaGetLastError());
+    s->launches += 1;
     return MGC_OK;
 }
 
@@ -1411,7 +1438,10 @@ mgc_status mgc_read_state(mgc_sim* s, float* v, float* i_exc, float* i_inh, int3
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->stream));
     const size_t n = s->n;
-    if (v) CK(cudaMemcpy(v, s->a.V, 4 * n, cudaMemcpyDeviceToHost));
+    if (v) {
+        CK(cudaMemcpy(v, s->a.V, 4 * n, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < s->pois_idx.size(); ++k) v[s->pois_idx[k]] = s->pois_v[k];
+    }
     if (i_exc) CK(cudaMemcpy(i_exc, s->a.Iexc, 4 * n, cudaMemcpyDeviceToHost));
     if (i_inh) CK(cudaMemcpy(i_inh, s->a.Iinh, 4 * n, cudaMemcpyDeviceToHost));
     if (refrac) CK(cudaMemcpy(refrac, s->a.refrac, 4 * n, cudaMemcpyDeviceToHost));
