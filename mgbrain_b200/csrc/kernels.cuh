@@ -204,8 +204,10 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
 // ---------------------------------------------------------------------------
 // One neuron of a group; ie_io/ii_io (LIF and LIFE currents) were loaded
 // with the group when the network has such neurons and are stored back with it.
+// u: the neuron's POISSON draw of this step (poisson_uniform), computed for
+// its group of four.
 __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, int64_t s, float& v, int32_t& rf,
-                                           float re, float ri, float& ie_io, float& ii_io)
+                                           float re, float ri, float& ie_io, float& ii_io, float u)
 {
     bool fired = false;
     if (t == kPOISSON) {
@@ -213,7 +215,7 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
         // draw.  A POISSON neuron's V is never used, so its V slot holds the
         // probability (mgc_set_rates writes it there): it arrives with the
         // group's loads instead of a second, dependent load.
-        fired = v > poisson_uniform(a.seed, (int64_t)i + a.id_offset, s);
+        fired = v > u;
     } else if (t == kLIFB) {
         // mgcore.cu:164-196: threshold on the old V, then leak + input
         if (rf > 0) {
@@ -324,10 +326,14 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             fmask[h] = 0;
             if (g < ngroups) {
                 const int32_t i0 = (int32_t)(g << 2);
-                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x, ce4[h].x, ci4[h].x) ? 1u : 0u;
-                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y, ce4[h].y, ci4[h].y) ? 2u : 0u;
-                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z, ce4[h].z, ci4[h].z) ? 4u : 0u;
-                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w, ce4[h].w, ci4[h].w) ? 8u : 0u;
+                // one Philox block serves the group's four POISSON draws
+                float u[4] = {0.f, 0.f, 0.f, 0.f};
+                if (t4[h].x == kPOISSON || t4[h].y == kPOISSON || t4[h].z == kPOISSON || t4[h].w == kPOISSON)
+                    poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
+                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x, ce4[h].x, ci4[h].x, u[0]) ? 1u : 0u;
+                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y, ce4[h].y, ci4[h].y, u[1]) ? 2u : 0u;
+                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z, ce4[h].z, ci4[h].z, u[2]) ? 4u : 0u;
+                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w, ce4[h].w, ci4[h].w, u[3]) ? 8u : 0u;
                 // the input is cleared only after it was used: a store issued
                 // while the load of the same line is in flight stalls the
                 // memory pipeline (measured 4-6x slower once the state

@@ -72,6 +72,26 @@ __host__ __device__ __forceinline__ float poisson_uniform(uint64_t seed, int64_t
     return unit_open0(pick(r, (int)(neuron & 3)));
 }
 
+// The draws of four consecutive neurons first, first+1, .., first+3 at a
+// step, equal to poisson_uniform of each: one Philox block when the four
+// share one (first % 4 == 0), else two.
+__host__ __device__ __forceinline__ void poisson_uniform4(uint64_t seed, int64_t first, int64_t step, float u[4])
+{
+    const uint64_t st = (uint64_t)step;
+    const uint32_t blk = (uint32_t)((uint64_t)first >> 2);
+    const int off = (int)(first & 3);
+    U32x4 r = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), blk, kTagPoisson, (uint32_t)seed,
+                            (uint32_t)(seed >> 32));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int w = off + k;
+        if (w == 4)  // the next neurons' block
+            r = philox4x32_10((uint32_t)st, (uint32_t)(st >> 32), blk + 1u, kTagPoisson, (uint32_t)seed,
+                              (uint32_t)(seed >> 32));
+        u[k] = unit_open0(pick(r, w & 3));
+    }
+}
+
 // Draw for synapse k of target t in projection r of the fixed in-degree
 // generator: x = source pick, y = delay pick.
 __host__ __device__ __forceinline__ U32x4 conn_draw(uint64_t conn_seed, uint32_t t, uint32_t k, uint32_t r)
