@@ -245,6 +245,19 @@ mgc_status mgc_read_weights(mgc_sim* sim, float* weight);
  * (any may be NULL). */
 mgc_status mgc_export_csr(mgc_sim* sim, int64_t* row_ptr, int32_t* tgt, float* weight, int32_t* delay);
 
+/* Cut and balance statistics of a neuron partition over the handle's
+ * synapses, computed on the device: replaces PartitionAnalysis's host loops
+ * (src/partition/analysis.cpp: getCostNum, getZoneNeu, getZoneSyn,
+ * getZoneOut, getZoneIn).  part[i] (host, one entry per network neuron,
+ * 0 <= part[i] < nparts <= 4096) is neuron i's zone.  Outputs (host arrays
+ * of nparts, any may be NULL): zone_neurons[z] = neurons in z; zone_syn[z] =
+ * synapses whose source is in z; zone_out[z] / zone_in[z] = synapses that
+ * cross zones, by source zone / by target zone; *cut = all crossing
+ * synapses.  A partition handle counts the synapses it holds (those that
+ * target its neurons). */
+mgc_status mgc_partition_stats(mgc_sim* sim, const int32_t* part, int32_t nparts, int64_t* cut,
+                               int64_t* zone_neurons, int64_t* zone_syn, int64_t* zone_out, int64_t* zone_in);
+
 mgc_status mgc_get_info(mgc_sim* sim, mgc_info* info);
 
 /* Runs `steps` steps with each kernel class bracketed by CUDA events (the

@@ -28,7 +28,7 @@ EXPORTED = (
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
-    "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout",
+    "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats",
 )
 
 
@@ -111,6 +111,8 @@ def lib():
     L.mgc_part_export.argtypes = [vp, i32, vp, vp, i64, C.POINTER(i64)]
     L.mgc_part_import.argtypes = [vp, i32, i32, i32, vp, vp, i64]
     L.mgc_fault_inject_alloc.argtypes = [i64]
+    L.mgc_partition_stats.argtypes = [vp, vp, i32, C.POINTER(i64), vp, vp, vp, vp]
+    L.mgc_partition_stats.restype = C.c_int
     L.mgc_selftest_wait_timeout.argtypes = [i32, i32, C.POINTER(i32), C.POINTER(C.c_double)]
     for name in ("mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export",
                  "mgc_part_import", "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout"):
@@ -381,6 +383,17 @@ class Simulator:
         d = np.zeros(self.S, np.int32)
         check(lib().mgc_export_csr(self._h, _ptr(rp), _ptr(t), _ptr(w), _ptr(d)))
         return rp, t, w, d
+
+    def partition_stats(self, part, nparts):
+        """Cut and balance of a neuron partition over this handle's synapses
+        (mgc_partition_stats): dict with cut and the per-zone arrays."""
+        p = np.ascontiguousarray(part, np.int32)
+        out = {k: np.zeros(int(nparts), np.int64) for k in ("zone_neurons", "zone_syn", "zone_out", "zone_in")}
+        cut = C.c_int64()
+        check(lib().mgc_partition_stats(self._h, _ptr(p), int(nparts), C.byref(cut), _ptr(out["zone_neurons"]),
+                                        _ptr(out["zone_syn"]), _ptr(out["zone_out"]), _ptr(out["zone_in"])))
+        out["cut"] = int(cut.value)
+        return out
 
     # ---- partitions -------------------------------------------------------
     def part_export(self, count, ids):

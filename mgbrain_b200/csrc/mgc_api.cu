@@ -1492,6 +1492,98 @@ mgc_status mgc_export_csr(mgc_sim* s, int64_t* row_ptr, int32_t* tgt, float* wei
     return MGC_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Partition statistics on the device: one warp per source row of the CSR,
+// the zones' counters in shared memory, flushed once per block.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kMaxZones = 4096;
+
+__global__ void k_partition_stats(const int64_t* row_ptr, const uint2* syn, int32_t n_src, uint32_t tmask,
+                                  int32_t tar_base, const int32_t* part, int32_t nparts, unsigned long long* out)
+{
+    extern __shared__ unsigned int zc[];  // [3][nparts]: syn by source zone, out by source zone, in by target zone
+    for (int z = threadIdx.x; z < 3 * nparts; z += blockDim.x) zc[z] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t src = warp; src < n_src; src += nwarps) {
+        const int64_t b = row_ptr[src], e = row_ptr[src + 1];
+        if (e == b) continue;
+        const int32_t zs = part[src];
+        unsigned int crossing = 0;
+        for (int64_t q = b + lane; q < e; q += 32) {
+            const int32_t zt = part[(int32_t)(syn[q].x & tmask) + tar_base];
+            if (zt != zs) {
+                ++crossing;
+                atomicAdd(&zc[2 * nparts + zt], 1u);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) crossing += __shfl_xor_sync(0xffffffffu, crossing, o);
+        if (lane == 0) {
+            atomicAdd(&zc[zs], (unsigned int)(e - b));
+            atomicAdd(&zc[nparts + zs], crossing);
+        }
+    }
+    __syncthreads();
+    for (int z = threadIdx.x; z < 3 * nparts; z += blockDim.x)
+        if (zc[z]) atomicAdd(out + z, (unsigned long long)zc[z]);
+}
+
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_partition_stats(mgc_sim* s, const int32_t* part, int32_t nparts, int64_t* cut, int64_t* zone_neurons,
+                               int64_t* zone_syn, int64_t* zone_out, int64_t* zone_in)
+{
+    if (!s || !part) return fail(MGC_ERR_INVALID, "null argument");
+    if (nparts < 1 || nparts > kMaxZones) return fail(MGC_ERR_INVALID, "1..%d zones (got %d)", kMaxZones, nparts);
+    const int32_t n = s->n_src;
+    std::vector<int64_t> zn(nparts, 0);
+    for (int32_t i = 0; i < n; ++i) {
+        if (part[i] < 0 || part[i] >= nparts)
+            return fail(MGC_ERR_INVALID, "neuron %d in zone %d, outside 0..%d", i, part[i], nparts - 1);
+        zn[part[i]] += 1;
+    }
+    CK(cudaSetDevice(s->device));
+    DevTmp tp, to;
+    int32_t* dpart;
+    unsigned long long* dout;
+    CKS(tmp_alloc(tp, &dpart, (size_t)n));
+    CKS(tmp_alloc(to, &dout, 3 * (size_t)nparts));
+    CK(cudaMemcpyAsync(dpart, part, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemsetAsync(dout, 0, 8 * 3 * (size_t)nparts, s->stream));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, s->device));
+    const size_t smem = 4 * 3 * (size_t)nparts;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_partition_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // a partition handle's targets are local ids; their zones are those of
+    // the whole-network ids from its first neuron on
+    k_partition_stats<<<prop.multiProcessorCount * 4, 256, smem, s->stream>>>(s->a.row_ptr, s->a.syn, n, s->a.tmask,
+                                                                              s->a.src_base, dpart, nparts, dout);
+    CK(cudaGetLastError());
+    s->launches += 1;
+    std::vector<unsigned long long> h(3 * (size_t)nparts);
+    CK(cudaMemcpyAsync(h.data(), dout, 8 * h.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    int64_t total_cut = 0;
+    for (int32_t z = 0; z < nparts; ++z) {
+        if (zone_neurons) zone_neurons[z] = zn[z];
+        if (zone_syn) zone_syn[z] = (int64_t)h[z];
+        if (zone_out) zone_out[z] = (int64_t)h[nparts + z];
+        if (zone_in) zone_in[z] = (int64_t)h[2 * nparts + z];
+        total_cut += (int64_t)h[nparts + z];
+    }
+    if (cut) *cut = total_cut;
+    return MGC_OK;
+}
+
 mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
 {
     if (!s || !info) return fail(MGC_ERR_INVALID, "null argument");
