@@ -11,10 +11,21 @@
 // Config::THROW_ON_ERROR.
 // Deliberate differences: a second simulate() continues from where the
 // first stopped (the reference restarts its step counter, mgsim.cpp:810);
-// npart > 1 runs every partition on the one GPU; the destructor does not
-// call cudaDeviceReset.
+// the destructor does not call cudaDeviceReset.
+//
+// npart > 1 (mgsim.cpp:337-363): with Config::enable_single_gpu() the
+// reference maps every partition to device 0; here the network then runs
+// as one handle on Config::DEVICE, which computes the same.  Otherwise the
+// reference spreads the partitions over the GPUs; here each partition gets
+// its own handle (mgc_create_partition) on device (DEVICE + p) % devices,
+// and the partitions exchange spike ids every min_delay - 1 steps.  That
+// needs the partition's neurons to be consecutive ids (SIMPLE and BSIM
+// partitions are), static weights and a minimum delay >= 2; otherwise the
+// network runs as one handle and a line on stderr says why.
 #pragma once
+#include <cstdint>
 #include <stdexcept>
+#include <vector>
 
 #include "network.h"
 
@@ -29,7 +40,18 @@ public:
 };
 
 class MGSimulator {
-    mgc_sim* sim = nullptr;
+    // One handle per partition (a single one covering every neuron unless
+    // the partitions run separately).
+    struct Piece {
+        mgc_sim* sim = nullptr;
+        int first = 0, count = 0, device = 0;
+        int32_t* xout = nullptr;  // device: exported spike ids of a window
+        int32_t* xin = nullptr;   // device: every partition's ids, imported
+        long long xin_cap = 0;
+    };
+    std::vector<Piece> pieces;
+    mgc_sim* sim = nullptr;       // pieces[0].sim
+    std::vector<int32_t> syn_tar; // partitions: each synapse's target (weights in synapse order)
     double sim_time = 0.0;
     int npart = 1;
     int min_delay = 1;
@@ -42,6 +64,7 @@ class MGSimulator {
     bool raster_complete = true;
     void check(int status, const char* what);
     void drain_raster();
+    void exchange(int steps);
     real get_firing_rate(real time);
 
 public:
@@ -68,7 +91,10 @@ public:
     long long get_events();
     int get_min_delay() const { return min_delay; }
     int get_ring_len() const { return max_delay + 1; }
+    // The C ABI handle (of the first partition when they run separately).
     mgc_sim* handle() { return sim; }
+    // Handles the network runs on: 1, or one per partition.
+    int get_handles() const { return (int)pieces.size(); }
 };
 
 }  // namespace MGBrain

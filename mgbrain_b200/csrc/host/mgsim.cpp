@@ -1,6 +1,9 @@
 // MGBrain C++ API: MGSimulator over the C ABI of the CUDA core.
 #include "mgbrain/mgsim.h"
 
+#include <cuda_runtime.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -60,7 +63,6 @@ void MGSimulator::check(int status, const char* what)
 MGSimulator::MGSimulator(Network& net, std::vector<int>& part, int nparts)
 {
     npart = nparts < 1 ? 1 : nparts;
-    std::cout << (npart == 1 ? "run single-net on single-GPU" : "run multi-net on single-GPU") << std::endl;
     const size_t n = net.neurons.size();
     const size_t S = net.synapses.size();
     n_neurons = (int)n;
@@ -120,35 +122,153 @@ MGSimulator::MGSimulator(Network& net, std::vector<int>& part, int nparts)
     d.device = Config::DEVICE;
     d.raster_steps = 65536;
     d.raster_ids = 0;
-    check(mgc_create(&d, &sim), "mgc_create");
     this->part = part;
+
+    // the partitions as separate handles: each a run of consecutive ids
+    std::vector<std::pair<int, int>> ranges;  // (first, count) of the non-empty zones
+    const char* why = nullptr;
+    if (npart > 1 && !Config::SINGLE_GPU) {
+        bool consecutive = part.size() == n;
+        for (size_t i = 0; consecutive && i < n; ++i)
+            consecutive = part[i] >= 0 && part[i] < npart && (i == 0 || part[i] >= part[i - 1]);
+        if (!consecutive)
+            why = "the partitions are not runs of consecutive neuron ids";
+        else if (Config::STDP)
+            why = "plastic weights (STDP) run in one handle";
+        else if (min_delay < 2)
+            why = "a minimum delay of one step leaves no exchange window";
+        for (size_t i = 0; !why && i < n;) {
+            size_t j = i;
+            while (j < n && part[j] == part[i]) ++j;
+            ranges.emplace_back((int)i, (int)(j - i));
+            i = j;
+        }
+    }
+    if (why) {
+        std::cerr << "mgbrain_b200: " << why << "; the " << npart << " partitions run as one handle" << std::endl;
+        ranges.clear();
+    }
+    if (ranges.size() > 1) {
+        int devices = 1;
+        if (cudaGetDeviceCount(&devices) != cudaSuccess || devices < 1) devices = 1;
+        std::cout << "run multi-net on " << (devices > 1 ? "multi-GPU" : "single-GPU") << std::endl;
+        for (size_t p = 0; p < ranges.size(); ++p) {
+            Piece pc;
+            pc.first = ranges[p].first;
+            pc.count = ranges[p].second;
+            pc.device = (Config::DEVICE + (int)p) % devices;
+            d.device = pc.device;
+            d.mode = MGC_MODE_DEFERRED;
+            check(mgc_create_partition(&d, pc.first, pc.count, &pc.sim), "mgc_create_partition");
+            pieces.push_back(pc);
+            const size_t cap = (size_t)(min_delay - 1) * (size_t)pc.count;
+            cudaSetDevice(pc.device);
+            if (cudaMalloc(&pieces.back().xout, 4 * std::max<size_t>(cap, 1)) != cudaSuccess)
+                check(MGC_ERR_NOMEM, "exchange buffer");
+        }
+        syn_tar = tar;
+    } else {
+        std::cout << (npart == 1 ? "run single-net on single-GPU" : "run multi-net on single-GPU") << std::endl;
+        Piece pc;
+        pc.count = (int)n;
+        pc.device = Config::DEVICE;
+        check(mgc_create(&d, &pc.sim), "mgc_create");
+        pieces.push_back(pc);
+    }
+    sim = pieces[0].sim;
 }
 
 MGSimulator::~MGSimulator()
 {
-    if (sim) mgc_destroy(sim);
+    for (Piece& p : pieces) {
+        if (p.xout || p.xin) cudaSetDevice(p.device);
+        if (p.xout) cudaFree(p.xout);
+        if (p.xin) cudaFree(p.xin);
+        if (p.sim) mgc_destroy(p.sim);
+    }
+}
+
+// The partitions' spike ids of the last `steps` steps, each partition's
+// appended to every other's history (through host memory, so the partitions
+// may sit on any devices).
+void MGSimulator::exchange(int steps)
+{
+    const int R = (int)pieces.size();
+    std::vector<int32_t> counts((size_t)R * steps);
+    std::vector<int64_t> total(R);
+    std::vector<std::vector<int32_t>> ids(R);
+    for (int r = 0; r < R; ++r) {
+        Piece& p = pieces[r];
+        const int64_t cap = (int64_t)(min_delay - 1) * p.count;
+        check(mgc_part_export(p.sim, steps, counts.data() + (size_t)r * steps, p.xout, cap, &total[r]),
+              "mgc_part_export");
+        ids[r].resize(std::max<int64_t>(total[r], 1));
+        cudaSetDevice(p.device);
+        if (total[r] && cudaMemcpy(ids[r].data(), p.xout, 4 * (size_t)total[r], cudaMemcpyDeviceToHost) != cudaSuccess)
+            check(MGC_ERR_CUDA, "exchange copy");
+    }
+    const int64_t stride = std::max<int64_t>(1, *std::max_element(total.begin(), total.end()));
+    std::vector<int32_t> all((size_t)R * stride, 0);
+    for (int r = 0; r < R; ++r) std::copy(ids[r].begin(), ids[r].begin() + total[r], all.begin() + (size_t)r * stride);
+    for (int r = 0; r < R; ++r) {
+        Piece& p = pieces[r];
+        cudaSetDevice(p.device);
+        if (p.xin_cap < (long long)all.size()) {
+            if (p.xin) cudaFree(p.xin);
+            p.xin = nullptr;
+            if (cudaMalloc(&p.xin, 4 * all.size()) != cudaSuccess) check(MGC_ERR_NOMEM, "exchange buffer");
+            p.xin_cap = (long long)all.size();
+        }
+        if (cudaMemcpy(p.xin, all.data(), 4 * all.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            check(MGC_ERR_CUDA, "exchange copy");
+        check(mgc_part_import(p.sim, steps, R, r, counts.data(), p.xin, stride), "mgc_part_import");
+    }
 }
 
 void MGSimulator::drain_raster()
 {
-    int64_t first = 0, ns = 0, ni = 0;
-    mgc_info info;
-    check(mgc_get_info(sim, &info), "mgc_get_info");
-    const int64_t steps = info.step - (int64_t)raster_counts.size();
-    if (steps <= 0) return;
-    std::vector<int64_t> counts(steps);
-    int64_t total_cap = (int64_t)n_neurons * 64 + (1 << 20);
-    std::vector<int32_t> ids(total_cap);
-    const int st = mgc_read_raster(sim, &first, counts.data(), steps, ids.data(), total_cap, &ns, &ni);
-    if (st == MGC_ERR_OVERFLOW) {
-        // more spikes than the raster holds: keep simulating, stop recording
-        if (!raster_complete) std::cerr << "mgbrain_b200: raster buffer overflow, raster incomplete" << std::endl;
-        raster_complete = false;
-    } else {
-        check(st, "mgc_read_raster");
+    const long long before = (long long)raster_counts.size();
+    std::vector<std::vector<int64_t>> pc(pieces.size());
+    std::vector<std::vector<int32_t>> pi(pieces.size());
+    int64_t steps = 0;
+    for (size_t q = 0; q < pieces.size(); ++q) {
+        mgc_info info;
+        check(mgc_get_info(pieces[q].sim, &info), "mgc_get_info");
+        steps = info.step - before;
+        if (steps <= 0) return;
+        int64_t first = 0, ns = 0, ni = 0;
+        pc[q].resize(steps);
+        const int64_t cap = (int64_t)pieces[q].count * 64 + (1 << 20);
+        pi[q].resize(cap);
+        const int st = mgc_read_raster(pieces[q].sim, &first, pc[q].data(), steps, pi[q].data(), cap, &ns, &ni);
+        if (st == MGC_ERR_OVERFLOW) {
+            // more spikes than the raster holds: keep simulating, stop recording
+            if (raster_complete) std::cerr << "mgbrain_b200: raster buffer overflow, raster incomplete" << std::endl;
+            raster_complete = false;
+        } else {
+            check(st, "mgc_read_raster");
+        }
+        pc[q].resize(ns);
+        pi[q].resize(ni);
+        steps = std::min<int64_t>(steps, ns);
     }
-    for (int64_t i = 0; i < ns; ++i) raster_counts.push_back(counts[i]);
-    raster_ids.insert(raster_ids.end(), ids.begin(), ids.begin() + ni);
+    if (pieces.size() == 1) {
+        raster_counts.insert(raster_counts.end(), pc[0].begin(), pc[0].end());
+        raster_ids.insert(raster_ids.end(), pi[0].begin(), pi[0].end());
+        return;
+    }
+    // partitions: step by step, the union of their (whole-network) ids, ascending
+    std::vector<size_t> pos(pieces.size(), 0);
+    for (int64_t s = 0; s < steps; ++s) {
+        const size_t at = raster_ids.size();
+        for (size_t q = 0; q < pieces.size(); ++q) {
+            const size_t c = (size_t)pc[q][s];
+            raster_ids.insert(raster_ids.end(), pi[q].begin() + pos[q], pi[q].begin() + pos[q] + c);
+            pos[q] += c;
+        }
+        std::sort(raster_ids.begin() + at, raster_ids.end());
+        raster_counts.push_back((long long)(raster_ids.size() - at));
+    }
 }
 
 void MGSimulator::simulate(real time)
@@ -158,14 +278,30 @@ void MGSimulator::simulate(real time)
     const long long steps = static_cast<int>(std::round(time / Config::STEP));
     const long long eff = mgc_effective_steps(steps, min_delay);
     timer t;
-    for (long long left = eff; left > 0;) {
-        const long long c = std::min(left, kChunkSteps);
-        check(mgc_run(sim, c), "mgc_run");
-        check(mgc_sync(sim), "mgc_sync");
-        drain_raster();
-        left -= c;
+    if (pieces.size() == 1) {
+        for (long long left = eff; left > 0;) {
+            const long long c = std::min(left, kChunkSteps);
+            check(mgc_run(sim, c), "mgc_run");
+            check(mgc_sync(sim), "mgc_sync");
+            drain_raster();
+            left -= c;
+        }
+    } else {
+        // windows of at most min_delay - 1 steps, each followed by the exchange
+        long long since_drain = 0;
+        for (long long left = eff; left > 0;) {
+            const int c = (int)std::min<long long>(left, min_delay - 1);
+            for (Piece& p : pieces) check(mgc_run(p.sim, c), "mgc_run");
+            exchange(c);
+            left -= c;
+            since_drain += c;
+            if (since_drain >= kChunkSteps || left == 0) {
+                drain_raster();
+                since_drain = 0;
+            }
+        }
     }
-    check(mgc_sync(sim), "mgc_sync");
+    for (Piece& p : pieces) check(mgc_sync(p.sim), "mgc_sync");
     total_steps += eff;
     sim_time = t.stop();
     if (Config::FIRE_CHECK) get_firing_rate(time);
@@ -201,37 +337,61 @@ const std::vector<int>& MGSimulator::spike_ids() { return raster_ids; }
 std::vector<real> MGSimulator::get_v()
 {
     std::vector<real> v(n_neurons);
-    check(mgc_read_state(sim, v.data(), nullptr, nullptr, nullptr, nullptr, nullptr), "mgc_read_state");
+    for (Piece& p : pieces)
+        check(mgc_read_state(p.sim, v.data() + p.first, nullptr, nullptr, nullptr, nullptr, nullptr), "mgc_read_state");
     return v;
 }
 
 std::vector<int> MGSimulator::get_fire_cnt()
 {
     std::vector<int> c(n_neurons);
-    check(mgc_read_state(sim, nullptr, nullptr, nullptr, nullptr, nullptr, c.data()), "mgc_read_state");
+    for (Piece& p : pieces)
+        check(mgc_read_state(p.sim, nullptr, nullptr, nullptr, nullptr, nullptr, c.data() + p.first), "mgc_read_state");
     return c;
 }
 
 std::vector<real> MGSimulator::get_weights()
 {
-    mgc_info info;
-    check(mgc_get_info(sim, &info), "mgc_get_info");
-    std::vector<real> w(info.n_synapses);
-    check(mgc_read_weights(sim, w.data()), "mgc_read_weights");
+    if (pieces.size() == 1) {
+        mgc_info info;
+        check(mgc_get_info(sim, &info), "mgc_get_info");
+        std::vector<real> w(info.n_synapses);
+        if (!w.empty()) check(mgc_read_weights(sim, w.data()), "mgc_read_weights");
+        return w;
+    }
+    // a partition holds the synapses that target its neurons, in synapse order
+    std::vector<real> w(syn_tar.size());
+    for (Piece& p : pieces) {
+        mgc_info info;
+        check(mgc_get_info(p.sim, &info), "mgc_get_info");
+        if (info.n_synapses == 0) continue;
+        std::vector<real> wp(info.n_synapses);
+        check(mgc_read_weights(p.sim, wp.data()), "mgc_read_weights");
+        size_t j = 0;
+        for (size_t k = 0; k < syn_tar.size(); ++k)
+            if (syn_tar[k] >= p.first && syn_tar[k] < p.first + p.count) w[k] = wp[j++];
+    }
     return w;
 }
 
 void MGSimulator::set_rates(const std::vector<real>& rate)
 {
-    check(mgc_set_rates(sim, rate.data(), (int32_t)rate.size()), "mgc_set_rates");
-    check(mgc_sync(sim), "mgc_sync");
+    if (rate.size() != (size_t)n_neurons) check(MGC_ERR_INVALID, "set_rates: one rate per neuron");
+    for (Piece& p : pieces) {
+        check(mgc_set_rates(p.sim, rate.data() + p.first, p.count), "mgc_set_rates");
+        check(mgc_sync(p.sim), "mgc_sync");
+    }
 }
 
 long long MGSimulator::get_events()
 {
-    mgc_info info;
-    check(mgc_get_info(sim, &info), "mgc_get_info");
-    return info.events;
+    long long e = 0;
+    for (Piece& p : pieces) {
+        mgc_info info;
+        check(mgc_get_info(p.sim, &info), "mgc_get_info");
+        e += info.events;
+    }
+    return e;
 }
 
 }  // namespace MGBrain

@@ -3,8 +3,9 @@
 // model -> netgen::gen_net -> parter::part_network -> mgsim.simulate.
 //
 //   api_driver gen <spec> <out.net>              env MGB_MT_SEED, MGB_RAND_SEED
-//   api_driver simulate <spec> <out_prefix> <seconds> <v0.f32|-> <stdp 0|1>
+//   api_driver simulate <spec> <out_prefix> <seconds> <v0.f32|-> <stdp 0|1> [npart [single|multi]]
 //                                                env MGB_MT_SEED, MGB_RAND_SEED, MGB_SEED
+//   (npart > 1: SIMPLE partitions; "single" calls config::enable_single_gpu())
 // simulate writes <out_prefix>.state (V, fire_cnt, weights) and .raster.
 #include <cstdio>
 #include <cstdlib>
@@ -50,7 +51,7 @@ int main(int argc, char** argv)
         printf("neurons %zu synapses %zu\n", net.neurons.size(), net.synapses.size());
         return 0;
     }
-    if (argc == 7 && std::string(argv[1]) == "simulate") {
+    if ((argc == 7 || argc == 9) && std::string(argv[1]) == "simulate") {
         network net;
         build(argv[2], net);
         if (std::string(argv[5]) != "-") {
@@ -62,8 +63,10 @@ int main(int argc, char** argv)
         if (atoi(argv[6])) config::enable_stdp();
         config::set_seed(env("MGB_SEED", 1));
         config::enable_fire_check();
-        std::vector<int> part = parter::part_network(net, 1, PartType::MODEL);
-        mgsim sim(net, part, 1);
+        const int npart = argc == 9 ? atoi(argv[7]) : 1;
+        if (argc == 9 && std::string(argv[8]) == "single") config::enable_single_gpu();
+        std::vector<int> part = parter::part_network(net, npart, npart > 1 ? PartType::SIMPLE : PartType::MODEL);
+        mgsim sim(net, part, npart);
         sim.simulate((real)atof(argv[4]));
         std::string pre = argv[3];
         FILE* f = fopen((pre + ".state").c_str(), "wb");
@@ -82,7 +85,7 @@ int main(int argc, char** argv)
         fwrite(c.data(), 8, c.size(), f);
         fwrite(ids.data(), 4, ids.size(), f);
         fclose(f);
-        printf("steps %lld time %.6f\n", sim.get_steps(), sim.get_time());
+        printf("steps %lld time %.6f handles %d\n", sim.get_steps(), sim.get_time(), sim.get_handles());
         return 0;
     }
     fprintf(stderr, "usage: api_driver gen|simulate ...\n");

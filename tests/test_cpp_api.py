@@ -74,3 +74,25 @@ def test_cpp_simulate_matches_oracle_and_reference(driver, tmp_path, name):
         rs = T.read_state(sim_state, n, S)
         assert np.array_equal(fc, rs["fire_cnt"])
         assert np.array_equal(v.view(np.int32), rs["V"].view(np.int32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c0s", "brunel_maker"])
+def test_cpp_partitions_run_as_separate_handles(driver, tmp_path, name):
+    """mgsim(net, part, 3) with SIMPLE partitions: without enable_single_gpu
+    each partition is its own handle (exchanging spike ids), with it the
+    network is one handle; both end exactly where npart = 1 ends."""
+    c, net, _ = load(name)
+    v0p = os.path.join(T.GOLDEN, name + ".v0")
+    outs = {}
+    for tag, extra in (("one", []), ("multi", ["3", "multi"]), ("single", ["3", "single"])):
+        pre = str(tmp_path / tag)
+        r = subprocess.run([driver, "simulate", os.path.join(T.GOLDEN, name + ".spec"), pre, "0.2",
+                            v0p if os.path.exists(v0p) else "-", "0"] + extra,
+                           check=True, env=_env(c), capture_output=True, text=True)
+        outs[tag] = (open(pre + ".state", "rb").read(), open(pre + ".raster", "rb").read(), r.stdout)
+    assert "handles 3" in outs["multi"][2] and "run multi-net on" in outs["multi"][2]
+    assert "handles 1" in outs["single"][2] and "run multi-net on single-GPU" in outs["single"][2]
+    for tag in ("multi", "single"):
+        assert outs[tag][0] == outs["one"][0], tag
+        assert outs[tag][1] == outs["one"][1], tag
