@@ -467,7 +467,11 @@ def run_partition(a, ws, rank, local):
                                        conn_seed=1, seed=1, device=local, raster_ids=-1, part=(first, count))
     sim.sync()
     build_s = time.perf_counter() - t0
-    part = DistributedPartition(sim, device=f"cuda:{local}") if ws > 1 else PartitionGroup([sim], [local])
+    cap = None if a.exchange == "exact" else max(256, count // 32)   # ids per step and partition
+    if ws > 1:
+        part = DistributedPartition(sim, device=f"cuda:{local}", cap_per_step=cap)
+    else:
+        part = PartitionGroup([sim], [local], cap_per_step=cap)
     for _ in range(a.warmup):
         part.run(CHUNK)
     torch.cuda.synchronize()
@@ -481,6 +485,7 @@ def run_partition(a, ws, rank, local):
             part.run(CHUNK)
         e1.record(stream)
         e1.synchronize()
+    sim.sync()   # raises if an exchange window was refused (the run would miss spikes)
     ms = allmax(ws, e0.elapsed_time(e1))
     events = allsum(ws, sim.info()["events"] - ev0)
     line = {"workload": "partition", "metric": METRIC, "value": events / (ms / 1e3), "unit": "events/s",
@@ -488,7 +493,9 @@ def run_partition(a, ws, rank, local):
             "scaling": "strong", "window_steps": part.window,
             "sim_s_per_wall_s": a.steps * CHUNK * DT / (ms / 1e3), "build_s": build_s,
             "partition": {"first": first, "neurons": count, "synapses": sim.S},
-            "exchange": "NCCL all-gather of counts, then of ids" if ws > 1 else "none (one partition)",
+            "exchange": ("none (one partition)" if ws == 1 else
+                         "NCCL all-gather of counts, then of ids (host waits)" if cap is None else
+                         f"NCCL all-gather of fixed buffers on the stream, {cap} ids per step"),
             "clocks": clk.summary()}
     if ws == 1:
         whole = make_sim(w, local, seed=1, record=False)
@@ -814,6 +821,8 @@ def main():
                          "parameter sweep; sched: the step scheduler's modes on a periodic drive; refgpu: "
                          "the reference's own simulator and this core on the reference's benchmark network; "
                          "partition: the 1M-neuron network split over the ranks, spike ids exchanged")
+    ap.add_argument("--exchange", choices=["device", "exact"], default="device",
+                    help="partition workload: the device exchange (fixed capacity, no host wait) or the exact one")
     ap.add_argument("--sched-train-groups", type=int, default=200)
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)

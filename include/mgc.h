@@ -194,6 +194,23 @@ mgc_status mgc_part_export(mgc_sim* sim, int32_t count, int32_t* counts, int32_t
 mgc_status mgc_part_import(mgc_sim* sim, int32_t count, int32_t nranks, int32_t self, const int32_t* counts,
                            const int32_t* ids, int64_t stride);
 
+/* The same exchange kept on the device, for callers that gather on the
+ * device (NCCL all-gather on the handle's stream, or device copies): no host
+ * synchronisation, a fixed capacity.  mgc_part_export_dev enqueues on the
+ * handle's stream the window's export into buf (device memory, count + cap
+ * ints): buf[0..count) = spikes per step, buf[count..) = their ids, cut at
+ * cap ids.  mgc_part_import_dev enqueues the import from bufs, nranks such
+ * blocks of count + cap ints side by side (rank r's at bufs + r*(count+cap),
+ * the layout an all-gather of the export buffers gives); nranks = 1 only
+ * closes the window.  The caller orders the gather between the two on the
+ * handle's stream (mgc_get_stream).  A window in which any rank exported
+ * more than cap ids is refused on every rank, and so are invalid counts or
+ * ids: every later mgc_sync returns MGC_ERR_INVALID, since the steps after
+ * a refused window miss its spikes (repeat the run with a larger cap). */
+mgc_status mgc_part_export_dev(mgc_sim* sim, int32_t count, int32_t* buf, int64_t cap);
+mgc_status mgc_part_import_dev(mgc_sim* sim, int32_t count, int32_t nranks, int32_t self, const int32_t* bufs,
+                               int64_t cap);
+
 /* Host-side fault injection for callers' error paths: the n-th device
  * allocation from now (n >= 1) fails as if the device were out of memory;
  * 0 turns it off.  The entry point that meets it returns MGC_ERR_NOMEM and

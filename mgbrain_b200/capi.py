@@ -28,7 +28,8 @@ EXPORTED = (
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
-    "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats",
+    "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats", "mgc_part_export_dev",
+    "mgc_part_import_dev",
 )
 
 
@@ -113,6 +114,10 @@ def lib():
     L.mgc_fault_inject_alloc.argtypes = [i64]
     L.mgc_partition_stats.argtypes = [vp, vp, i32, C.POINTER(i64), vp, vp, vp, vp]
     L.mgc_partition_stats.restype = C.c_int
+    L.mgc_part_export_dev.argtypes = [vp, i32, vp, i64]
+    L.mgc_part_import_dev.argtypes = [vp, i32, i32, i32, vp, i64]
+    L.mgc_part_export_dev.restype = C.c_int
+    L.mgc_part_import_dev.restype = C.c_int
     L.mgc_selftest_wait_timeout.argtypes = [i32, i32, C.POINTER(i32), C.POINTER(C.c_double)]
     for name in ("mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export",
                  "mgc_part_import", "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout"):
@@ -412,6 +417,17 @@ class Simulator:
         c = np.ascontiguousarray(counts, np.int32)
         check(lib().mgc_part_import(self._h, int(count), int(c.shape[0]), int(self_rank), _ptr(c),
                                     C.c_void_p(ids.data_ptr()) if ids is not None else None, int(stride)))
+
+    def part_export_dev(self, count, buf, cap):
+        """Enqueues the window's export into the device tensor buf (count + cap
+        int32: counts, then ids); no host synchronisation."""
+        check(lib().mgc_part_export_dev(self._h, int(count), C.c_void_p(buf.data_ptr()), int(cap)))
+
+    def part_import_dev(self, count, self_rank, nranks, bufs, cap):
+        """Enqueues the import from the device tensor bufs (nranks blocks of
+        count + cap int32, as an all-gather of the export buffers lays them)."""
+        ptr = C.c_void_p(bufs.data_ptr()) if bufs is not None else None
+        check(lib().mgc_part_import_dev(self._h, int(count), int(nranks), int(self_rank), ptr, int(cap)))
 
     def autotune(self, steps_per_trial=640):
         """Times the launch configurations and keeps the fastest; the trial

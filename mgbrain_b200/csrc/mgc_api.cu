@@ -1357,7 +1357,9 @@ mgc_status mgc_sync(mgc_sim* s)
     int32_t st = 0;
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
     if (st & kStatusBarrier) return fail(MGC_ERR_CUDA, "a grid barrier of the persistent step group timed out");
-    if (st & kStatusExchange) return fail(MGC_ERR_INVALID, "an imported spike id was out of range (exchange refused)");
+    if (st & kStatusExchange)
+        return fail(MGC_ERR_INVALID, "a spike exchange was refused: an id outside the network, or a window with more "
+                                     "spikes than the exchange buffer holds");
     if (st) return fail(MGC_ERR_OVERFLOW, "raster buffer overflow (status %d)", st);
     return MGC_OK;
 }
@@ -2275,31 +2277,42 @@ __global__ void k_part_export(StepArgs a, int32_t count, int32_t* counts, int32_
 
 // Block (j, r), r != self: rank r's spikes of step (current - count + j),
 // stored from ids + r * stride after its spikes of the earlier steps, go
-// after the slot's own spikes and those of the ranks before r.  cnt is
-// [nranks][count].  An id outside the network, or a slot that would hold
-// more than every neuron, sets kStatusExchange and the counts stay as they
-// were (k_part_commit), so no delivery reads what was written.
+// after the slot's own spikes and those of the ranks before r.  Rank q's
+// count of step j is cnt[q * cnt_stride + j].  A rank whose window holds
+// more than cap ids (its buffer cut them), a negative count, an id outside
+// the network or a slot that would hold more than every neuron sets
+// kStatusExchange and the counts stay as they were (k_part_commit), so no
+// delivery reads what was written.
 __global__ void k_part_import(StepArgs a, int32_t count, int32_t nranks, int32_t self, const int32_t* cnt,
-                              const int32_t* ids, int64_t stride)
+                              int64_t cnt_stride, const int32_t* ids, int64_t stride, int64_t cap)
 {
     const int32_t j = blockIdx.x, r = blockIdx.y;
-    if (r == self) return;
+    int64_t src = (int64_t)r * stride, rank_total = 0;
+    bool bad = false;
+    for (int32_t q = 0; q < count; ++q) {
+        const int32_t c = cnt[(size_t)r * cnt_stride + q];
+        bad |= c < 0;
+        rank_total += c;
+        if (q < j) src += c;
+    }
+    if (r == self) {  // its own window cut short makes the others refuse: refuse here too
+        if (threadIdx.x == 0 && rank_total > cap) atomicOr(a.status, kStatusExchange);
+        return;
+    }
     const int32_t hs = slot_back(a, count - j);
     const int64_t own = a.hist_cnt[hs];
     int64_t dst = own, total = own;
     for (int32_t q = 0; q < nranks; ++q) {
         if (q == self) continue;
-        const int32_t c = cnt[(size_t)q * count + j];
+        const int32_t c = cnt[(size_t)q * cnt_stride + j];
         if (q < r) dst += c;
         total += c;
     }
-    if (total > a.n_src) {
+    if (bad || rank_total > cap || total > a.n_src) {
         if (threadIdx.x == 0) atomicOr(a.status, kStatusExchange);
         return;
     }
-    int64_t src = (int64_t)r * stride;
-    for (int32_t q = 0; q < j; ++q) src += cnt[(size_t)r * count + q];
-    const int32_t c = cnt[(size_t)r * count + j];
+    const int32_t c = cnt[(size_t)r * cnt_stride + j];
     int32_t* out = a.hist_ids + (size_t)hs * (size_t)a.n_src;
     for (int32_t i = threadIdx.x; i < c; i += blockDim.x) {
         const int32_t id = ids[src + i];
@@ -2312,13 +2325,14 @@ __global__ void k_part_import(StepArgs a, int32_t count, int32_t nranks, int32_t
 }
 
 // The slots' counts grow by the imported spikes, unless the import failed.
-__global__ void k_part_commit(StepArgs a, int32_t count, int32_t nranks, int32_t self, const int32_t* cnt)
+__global__ void k_part_commit(StepArgs a, int32_t count, int32_t nranks, int32_t self, const int32_t* cnt,
+                              int64_t cnt_stride)
 {
     if (*(volatile int32_t*)a.status & kStatusExchange) return;
     for (int32_t j = threadIdx.x; j < count; j += blockDim.x) {
         int32_t add = 0;
         for (int32_t q = 0; q < nranks; ++q)
-            if (q != self) add += cnt[(size_t)q * count + j];
+            if (q != self) add += cnt[(size_t)q * cnt_stride + j];
         a.hist_cnt[slot_back(a, count - j)] += add;
     }
 }
@@ -2404,8 +2418,9 @@ mgc_status mgc_part_import(mgc_sim* s, int32_t count, int32_t nranks, int32_t se
     CKS(xch_reserve(s, (int64_t)nranks * count));
     CK(cudaMemcpyAsync(s->xch, counts, 4 * (size_t)nranks * count, cudaMemcpyHostToDevice, s->stream));
     if (any) {
-        k_part_import<<<dim3(count, nranks), 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch, ids, stride);
-        k_part_commit<<<1, 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch);
+        k_part_import<<<dim3(count, nranks), 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch, count, ids,
+                                                                   stride, stride);
+        k_part_commit<<<1, 256, 0, s->stream>>>(s->a, count, nranks, self, s->xch, count);
         CK(cudaGetLastError());
         s->launches += 2;
     }
@@ -2413,6 +2428,38 @@ mgc_status mgc_part_import(mgc_sim* s, int32_t count, int32_t nranks, int32_t se
     int32_t st = 0;
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
     if (st & kStatusExchange) return fail(MGC_ERR_INVALID, "an imported spike id was out of range (exchange refused)");
+    s->pending = 0;
+    return MGC_OK;
+}
+
+mgc_status mgc_part_export_dev(mgc_sim* s, int32_t count, int32_t* buf, int64_t cap)
+{
+    if (!s || !buf || cap < 0) return fail(MGC_ERR_INVALID, "bad export arguments");
+    CKS(check_window(s, count));
+    CK(cudaSetDevice(s->device));
+    if (!device_accessible(buf, s->device))
+        return fail(MGC_ERR_INVALID, "exchange buffer is not device memory of device %d", s->device);
+    k_part_export<<<count, 256, 0, s->stream>>>(s->a, count, buf, buf + count, cap);
+    CK(cudaGetLastError());
+    s->launches += 1;
+    return MGC_OK;
+}
+
+mgc_status mgc_part_import_dev(mgc_sim* s, int32_t count, int32_t nranks, int32_t self, const int32_t* bufs, int64_t cap)
+{
+    if (!s || nranks < 1 || self < 0 || self >= nranks || cap < 0) return fail(MGC_ERR_INVALID, "bad import arguments");
+    CKS(check_window(s, count));
+    CK(cudaSetDevice(s->device));
+    if (nranks > 1) {
+        if (!bufs || !device_accessible(bufs, s->device))
+            return fail(MGC_ERR_INVALID, "exchange buffer is not device memory of device %d", s->device);
+        const int64_t blk = count + cap;  // one rank's export: counts, then ids
+        k_part_import<<<dim3(count, nranks), 256, 0, s->stream>>>(s->a, count, nranks, self, bufs, blk, bufs + count,
+                                                                   blk, cap);
+        k_part_commit<<<1, 256, 0, s->stream>>>(s->a, count, nranks, self, bufs, blk);
+        CK(cudaGetLastError());
+        s->launches += 2;
+    }
     s->pending = 0;
     return MGC_OK;
 }

@@ -18,9 +18,17 @@ whole network's run.
 Two drivers:
 - PartitionGroup: several partition handles in one process (one device or
   several), the gather done by device copies;
-- DistributedPartition: one handle per rank of a torch.distributed group; the
-  gather is an all-gather of the counts, then of the ids padded to the
-  largest rank's total (NCCL on device buffers, or gloo through host memory).
+- DistributedPartition: one handle per rank of a torch.distributed group.
+
+Two exchanges, by `cap_per_step`:
+- None (exact): an all-gather of the counts, then of the ids padded to the
+  largest rank's total; the host learns the sizes in between, so each window
+  waits for the host (NCCL on device buffers, or gloo through host memory);
+- a number: fixed-capacity buffers of cap_per_step ids per step of the
+  window, exported, gathered (NCCL all-gather, or device copies) and imported
+  on the handles' streams without a host synchronisation.  A window with
+  more spikes than the capacity is refused on every rank and the next sync
+  raises (mgc_part_export_dev / mgc_part_import_dev).
 """
 from __future__ import annotations
 
@@ -63,13 +71,22 @@ def merge_rasters(rasters):
 class PartitionGroup:
     """Partition handles of one network driven together in one process."""
 
-    def __init__(self, sims, devices=None):
+    def __init__(self, sims, devices=None, cap_per_step=None):
         self.sims = list(sims)
         self.devices = [torch.device("cuda", d) for d in (devices or [0] * len(self.sims))]
         self.window = min(window_of(s.info()["min_delay"]) for s in self.sims)
-        # export buffers: a partition emits at most its neurons per step
-        self.bufs = [torch.empty(max(1, self.window * s.n), dtype=torch.int32, device=d)
-                     for s, d in zip(self.sims, self.devices)]
+        R = len(self.sims)
+        self.cap = None if cap_per_step is None else self.window * int(cap_per_step)
+        if self.cap is None:
+            # export buffers: a partition emits at most its neurons per step
+            self.bufs = [torch.empty(max(1, self.window * s.n), dtype=torch.int32, device=d)
+                         for s, d in zip(self.sims, self.devices)]
+        else:
+            blk = self.window + self.cap
+            self.ebufs = [torch.empty(blk, dtype=torch.int32, device=d) for d in self.devices]
+            self.gbufs = [torch.empty(R * blk, dtype=torch.int32, device=d) for d in self.devices] if R > 1 else None
+            self.streams = [torch.cuda.ExternalStream(s.stream, device=d) for s, d in zip(self.sims, self.devices)]
+            self.done = []   # events: the previous window's gathers, before an export buffer is reused
 
     def run(self, steps):
         left = int(steps)
@@ -77,8 +94,15 @@ class PartitionGroup:
             k = min(self.window, left)
             for s in self.sims:
                 s.run(k)
-            self._exchange(k)
+            if self.cap is None:
+                self._exchange(k)
+            else:
+                self._exchange_dev(k)
             left -= k
+
+    def sync(self):
+        for s in self.sims:
+            s.sync()
 
     def _exchange(self, k):
         R = len(self.sims)
@@ -97,6 +121,32 @@ class PartitionGroup:
             torch.cuda.synchronize(d)
             s.part_import(k, r, C, ids, stride)
 
+    def _exchange_dev(self, k):
+        R = len(self.sims)
+        if R == 1:
+            self.sims[0].part_import_dev(k, 0, 1, None, self.cap)   # nothing to gather: closes the window
+            return
+        blk = k + self.cap
+        exported = []
+        for q, s in enumerate(self.sims):
+            for ev in self.done:             # every gather of the last window read this buffer
+                self.streams[q].wait_event(ev)
+            s.part_export_dev(k, self.ebufs[q], self.cap)
+            ev = torch.cuda.Event()
+            ev.record(self.streams[q])
+            exported.append(ev)
+        self.done = []
+        for r, s in enumerate(self.sims):
+            st = self.streams[r]
+            with torch.cuda.stream(st):
+                for q in range(R):   # every block, its own too (its counts are checked against cap)
+                    st.wait_event(exported[q])
+                    self.gbufs[r][q * blk:(q + 1) * blk].copy_(self.ebufs[q][:blk], non_blocking=True)
+            s.part_import_dev(k, r, R, self.gbufs[r], self.cap)
+            ev = torch.cuda.Event()
+            ev.record(st)
+            self.done.append(ev)
+
     def raster(self):
         return merge_rasters([s.read_raster() for s in self.sims])
 
@@ -109,7 +159,7 @@ class DistributedPartition:
     """This rank's partition handle; run() is collective over the group.
     `device`: where the handle's exchange buffers live (its CUDA device)."""
 
-    def __init__(self, sim, device=None, group=None):
+    def __init__(self, sim, device=None, group=None, cap_per_step=None):
         import torch.distributed as dist
         self.dist = dist
         self.sim = sim
@@ -122,15 +172,35 @@ class DistributedPartition:
         w = torch.tensor([window_of(sim.info()["min_delay"])], dtype=torch.int64, device=self.comm_device)
         dist.all_reduce(w, op=dist.ReduceOp.MIN, group=group)
         self.window = int(w.item())
-        self.buf = torch.empty(max(1, self.window * sim.n), dtype=torch.int32, device=self.device)
+        if cap_per_step is not None and not self.nccl:
+            raise ValueError("the device exchange gathers with NCCL (gloo groups use the exact exchange)")
+        self.cap = None if cap_per_step is None else self.window * int(cap_per_step)
+        if self.cap is None:
+            self.buf = torch.empty(max(1, self.window * sim.n), dtype=torch.int32, device=self.device)
+        else:
+            blk = self.window + self.cap
+            self.ebuf = torch.empty(blk, dtype=torch.int32, device=self.device)
+            self.gbuf = torch.empty(self.world * blk, dtype=torch.int32, device=self.device)
+            self.stream = torch.cuda.ExternalStream(sim.stream, device=self.device)
 
     def run(self, steps):
         left = int(steps)
         while left > 0:
             k = min(self.window, left)
             self.sim.run(k)
-            self.exchange(k)
+            if self.cap is None:
+                self.exchange(k)
+            else:
+                self.exchange_dev(k)
             left -= k
+
+    def exchange_dev(self, k):
+        """Export, all-gather and import on the handle's stream; no host wait."""
+        blk = k + self.cap
+        self.sim.part_export_dev(k, self.ebuf, self.cap)
+        with torch.cuda.stream(self.stream):
+            self.dist.all_gather_into_tensor(self.gbuf[:self.world * blk], self.ebuf[:blk], group=self.group)
+        self.sim.part_import_dev(k, self.rank, self.world, self.gbuf, self.cap)
 
     def exchange(self, k):
         dist, R = self.dist, self.world

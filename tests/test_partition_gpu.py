@@ -55,9 +55,10 @@ def compare(whole, group, exact_v):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cap", [None, 64])
 @pytest.mark.parametrize("parts", [2, 3])
 @pytest.mark.parametrize("name", ["c0s", "brunel_maker", "lif_mixed"])
-def test_explicit_partitions_equal_whole(name, parts):
+def test_explicit_partitions_equal_whole(name, parts, cap):
     net, args, kw = explicit_args(name)
     whole = mgb.Simulator.from_arrays(*args, **kw)
     whole.run(2000)
@@ -66,9 +67,10 @@ def test_explicit_partitions_equal_whole(name, parts):
         assert s.first == first and s.n == count and s.n_src == net["n"]
         assert s.info()["mode"] == mgb.MODE_DEFERRED
     assert sum(s.S for s in sims) == len(net["src"])
-    g = PartitionGroup(sims)
+    g = PartitionGroup(sims, cap_per_step=cap)   # exact exchange, or the device one with 64 ids per step
     g.run(700)
     g.run(1300)
+    g.sync()
     compare(whole, g, equal_weights(net["weight"]))
 
 
@@ -78,8 +80,9 @@ def fixed(w, **kw):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("cap", [None, 2048])
 @pytest.mark.parametrize("persistent", [0, 1, 2])
-def test_fixed_indegree_partitions_equal_whole(persistent):
+def test_fixed_indegree_partitions_equal_whole(persistent, cap):
     w = bench.workload(scale=0.02, nu=0.02)
     whole = fixed(w)
     whole.set_persistent(persistent)
@@ -89,9 +92,10 @@ def test_fixed_indegree_partitions_equal_whole(persistent):
     for s in sims:
         s.set_persistent(persistent)
     assert sum(s.S for s in sims) == whole.S
-    g = PartitionGroup(sims)
+    g = PartitionGroup(sims, cap_per_step=cap)
     assert g.window == 9
     g.run(3000)
+    g.sync()
     for s in sims:
         assert s.info()["persistent"] == persistent
     compare(whole, g, True)
@@ -143,6 +147,20 @@ def test_partition_misuse_is_refused():
         a.sync()
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_device_exchange_overflow_is_refused():
+    """A window with more spikes than the device exchange holds is refused on
+    every partition, and the next sync says so."""
+    w = bench.workload(scale=0.02, nu=0.05)
+    sims = [fixed(w, part=p) for p in split(w["n"], 2)]
+    g = PartitionGroup(sims, cap_per_step=1)
+    g.run(200)
+    for s in sims:
+        with pytest.raises(mgb.MgcError) as e:
+            s.sync()
+        assert "exchange" in str(e.value)
 
 
 def free_port():
