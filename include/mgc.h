@@ -249,6 +249,18 @@ mgc_status mgc_set_rates(mgc_sim* sim, const float* rate, int32_t n);
 mgc_status mgc_read_raster(mgc_sim* sim, int64_t* first_step, int64_t* counts, int64_t counts_cap,
                            int32_t* ids, int64_t ids_cap, int64_t* n_steps, int64_t* n_ids);
 
+/* The same readout without stopping the device, for readers that read while
+ * the simulation goes on: mgc_raster_stage enqueues on the handle's stream a
+ * device copy of the raster recorded so far into one of two staging buffers
+ * and starts a new raster (no host wait); mgc_raster_collect waits only for
+ * the oldest staged copy and returns it as mgc_read_raster does, while the
+ * steps enqueued after that stage keep running.  At most two stages are
+ * outstanding; mgc_read_raster refuses while one is.  No reference
+ * counterpart. */
+mgc_status mgc_raster_stage(mgc_sim* sim);
+mgc_status mgc_raster_collect(mgc_sim* sim, int64_t* first_step, int64_t* counts, int64_t counts_cap,
+                              int32_t* ids, int64_t ids_cap, int64_t* n_steps, int64_t* n_ids);
+
 /* Copies neuron state to host arrays of n entries; any pointer may be NULL.
  * Replaces get_subnet_firecnt (mgnet.cpp:148-158) / copy_subnet_cpu
  * (mgnet.cpp:283-300). */

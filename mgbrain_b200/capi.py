@@ -29,7 +29,7 @@ EXPORTED = (
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
     "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats", "mgc_part_export_dev",
-    "mgc_part_import_dev",
+    "mgc_part_import_dev", "mgc_raster_stage", "mgc_raster_collect",
 )
 
 
@@ -114,6 +114,10 @@ def lib():
     L.mgc_fault_inject_alloc.argtypes = [i64]
     L.mgc_partition_stats.argtypes = [vp, vp, i32, C.POINTER(i64), vp, vp, vp, vp]
     L.mgc_partition_stats.restype = C.c_int
+    L.mgc_raster_stage.argtypes = [vp]
+    L.mgc_raster_collect.argtypes = [vp, vp, vp, i64, vp, i64, vp, vp]
+    L.mgc_raster_stage.restype = C.c_int
+    L.mgc_raster_collect.restype = C.c_int
     L.mgc_part_export_dev.argtypes = [vp, i32, vp, i64]
     L.mgc_part_import_dev.argtypes = [vp, i32, i32, i32, vp, i64]
     L.mgc_part_export_dev.restype = C.c_int
@@ -365,6 +369,22 @@ class Simulator:
         check(lib().mgc_read_raster(self._h, C.byref(first), _ptr(counts), max_steps, _ptr(ids),
                                     max_ids, C.byref(ns), C.byref(ni)))
         # copies: the (mostly untouched) capacity buffers are not kept alive
+        return first.value, counts[:ns.value].copy(), ids[:ni.value].copy()
+
+    def stage_raster(self):
+        """Enqueues a device copy of the raster so far and starts a new one
+        (mgc_raster_stage); no host wait."""
+        check(lib().mgc_raster_stage(self._h))
+
+    def collect_raster(self, max_steps=1 << 20, max_ids=None):
+        """The oldest staged raster, as read_raster returns one."""
+        if max_ids is None:
+            max_ids = max(1, self.n) * 64
+        counts = np.empty(max_steps, np.int64)
+        ids = np.empty(max_ids, np.int32)
+        first, ns, ni = C.c_int64(), C.c_int64(), C.c_int64()
+        check(lib().mgc_raster_collect(self._h, C.byref(first), _ptr(counts), max_steps, _ptr(ids),
+                                       max_ids, C.byref(ns), C.byref(ni)))
         return first.value, counts[:ns.value].copy(), ids[:ni.value].copy()
 
     def state(self):

@@ -97,6 +97,15 @@ struct mgc_sim {
     bool partition = false;  // simulates neurons [a.src_base, a.src_base + n) of a larger network
     std::vector<int32_t> pois_idx;  // POISSON neurons, and the V they report (their V slot holds
     std::vector<float> pois_v;      // the per-step probability)
+    struct RasterStage {     // a device copy of the raster, waiting for the host
+        int32_t* ids = nullptr;
+        int32_t* counts = nullptr;
+        int64_t* meta = nullptr;  // first step, steps, ids, raster status bits
+        cudaEvent_t ev = nullptr;
+    };
+    RasterStage stages[2];
+    int stage_head = 0, staged = 0;  // oldest outstanding stage, and how many
+    cudaStream_t copy_stream = nullptr;
     int32_t pending = 0;     // partition: steps run since the last spike import
     int32_t* xch = nullptr;  // partition: device scratch of the exchange (spike counts)
     int64_t xch_cap = 0;
@@ -136,6 +145,9 @@ struct mgc_sim {
         if (device >= 0) cudaSetDevice(device);
         if (graph) cudaGraphExecDestroy(graph);
         if (stream) cudaStreamSynchronize(stream);
+        for (RasterStage& g : stages)
+            if (g.ev) cudaEventDestroy(g.ev);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         for (void* p : allocs) cudaFree(p);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1375,34 +1387,19 @@ mgc_status mgc_set_rates(mgc_sim* s, const float* rate, int32_t n)
     return MGC_OK;
 }
 
-mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int64_t counts_cap, int32_t* ids,
-                           int64_t ids_cap, int64_t* n_steps, int64_t* n_ids)
+}  // extern "C"
+
+namespace {
+
+constexpr int32_t kRasterBits = kStatusRasterIds | kStatusRasterSteps;
+
+// ns steps' counts c32 and their ni ids hid (step after step) into the
+// caller's arrays, each step's ids sorted, the steps split over host threads.
+mgc_status finish_raster(int64_t step0, int64_t ns, int64_t ni, const int32_t* c32, int32_t* hid, bool truncated,
+                         int32_t status, int64_t* first_step, int64_t* counts, int64_t counts_cap, int32_t* ids,
+                         int64_t ids_cap, int64_t* n_steps, int64_t* n_ids)
 {
-    if (!s) return fail(MGC_ERR_INVALID, "null handle");
-    if (!s->a.record) return fail(MGC_ERR_INVALID, "raster recording is off for this handle");
-    CK(cudaSetDevice(s->device));
-    CK(cudaStreamSynchronize(s->stream));
-    int64_t step = 0, step0 = 0, pos = 0;
-    int32_t status = 0;
-    CK(cudaMemcpy(&step, s->a.step, 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&step0, s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&pos, s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&status, s->a.status, 4, cudaMemcpyDeviceToHost));
-    const int64_t ns = std::min(step - step0, s->raster_steps_cap);
-    const int64_t ni = std::min(pos, s->raster_ids_cap);
-    std::vector<int32_t> c32(ns);
-    if (ns) CK(cudaMemcpy(c32.data(), s->a.raster_counts, 4 * ns, cudaMemcpyDeviceToHost));
-    // the ids land in the caller's buffer when it holds them all (else in a
-    // staging buffer), then each step's ids are sorted in place, the steps
-    // split over host threads
-    std::unique_ptr<int32_t[]> staging;
-    int32_t* hid = ids;
-    if (!ids || ids_cap < ni) {
-        staging.reset(new int32_t[std::max<int64_t>(ni, 1)]);
-        hid = staging.get();
-    }
-    if (ni) CK(cudaMemcpy(hid, s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
-    const bool truncated = status != 0 || ns > counts_cap || ni > ids_cap;
+    truncated = truncated || ns > counts_cap || ni > ids_cap;
     std::vector<int64_t> off(ns + 1, 0);
     for (int64_t i = 0; i < ns; ++i) {
         off[i + 1] = off[i] + c32[i];
@@ -1424,13 +1421,125 @@ mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int
     if (first_step) *first_step = step0;
     if (n_steps) *n_steps = std::min(ns, counts_cap);
     if (n_ids) *n_ids = std::min(ni, ids_cap);
-    const int64_t zero = 0;
-    const int32_t zero32 = 0;
-    CK(cudaMemcpy(s->a.raster_step0, &step, 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s->a.raster_pos, &zero, 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s->a.status, &zero32, 4, cudaMemcpyHostToDevice));
     if (truncated) return fail(MGC_ERR_OVERFLOW, "raster truncated (device status %d)", status);
     return MGC_OK;
+}
+
+// The raster so far into a stage (block-strided copies), then the clock of
+// the next raster (k_raster_restart, after every block has read).
+__global__ void k_raster_stage(StepArgs a, int32_t* ids, int32_t* counts, int64_t steps_cap, int64_t ids_cap)
+{
+    const int64_t ns = min(*a.step - *a.raster_step0, steps_cap);
+    const int64_t ni = min(*a.raster_pos, ids_cap);
+    GRID_STRIDE(i, ns) counts[i] = a.raster_counts[i];
+    GRID_STRIDE(i, ni) ids[i] = a.raster_ids[i];
+}
+
+__global__ void k_raster_restart(StepArgs a, int64_t* meta, int64_t steps_cap, int64_t ids_cap)
+{
+    const int64_t step = *a.step, step0 = *a.raster_step0;
+    meta[0] = step0;
+    meta[1] = min(step - step0, steps_cap);
+    meta[2] = min(*a.raster_pos, ids_cap);
+    meta[3] = *a.status & kRasterBits;
+    *a.raster_step0 = step;
+    *a.raster_pos = 0;
+    atomicAnd(a.status, ~kRasterBits);
+}
+
+}  // namespace
+
+extern "C" {
+
+mgc_status mgc_read_raster(mgc_sim* s, int64_t* first_step, int64_t* counts, int64_t counts_cap, int32_t* ids,
+                           int64_t ids_cap, int64_t* n_steps, int64_t* n_ids)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->a.record) return fail(MGC_ERR_INVALID, "raster recording is off for this handle");
+    if (s->staged) return fail(MGC_ERR_INVALID, "collect the staged rasters first (mgc_raster_collect)");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    int64_t step = 0, step0 = 0, pos = 0;
+    int32_t status = 0;
+    CK(cudaMemcpy(&step, s->a.step, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&step0, s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&pos, s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&status, s->a.status, 4, cudaMemcpyDeviceToHost));
+    const int64_t ns = std::min(step - step0, s->raster_steps_cap);
+    const int64_t ni = std::min(pos, s->raster_ids_cap);
+    std::vector<int32_t> c32(ns);
+    if (ns) CK(cudaMemcpy(c32.data(), s->a.raster_counts, 4 * ns, cudaMemcpyDeviceToHost));
+    // the ids land in the caller's buffer when it holds them all (else in a
+    // staging buffer)
+    std::unique_ptr<int32_t[]> staging;
+    int32_t* hid = ids;
+    if (!ids || ids_cap < ni) {
+        staging.reset(new int32_t[std::max<int64_t>(ni, 1)]);
+        hid = staging.get();
+    }
+    if (ni) CK(cudaMemcpy(hid, s->a.raster_ids, 4 * ni, cudaMemcpyDeviceToHost));
+    // the next raster starts here; only the raster's status bits are cleared
+    const int64_t zero = 0;
+    const int32_t kept = status & ~kRasterBits;
+    CK(cudaMemcpy(s->a.raster_step0, &step, 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->a.raster_pos, &zero, 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->a.status, &kept, 4, cudaMemcpyHostToDevice));
+    return finish_raster(step0, ns, ni, c32.data(), hid, (status & kRasterBits) != 0, status, first_step, counts,
+                         counts_cap, ids, ids_cap, n_steps, n_ids);
+}
+
+mgc_status mgc_raster_stage(mgc_sim* s)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->a.record) return fail(MGC_ERR_INVALID, "raster recording is off for this handle");
+    if (s->staged == 2) return fail(MGC_ERR_INVALID, "two rasters are staged already: collect one first");
+    CK(cudaSetDevice(s->device));
+    mgc_sim::RasterStage& g = s->stages[(s->stage_head + s->staged) & 1];
+    if (!g.ids) {
+        CKS(s->alloc(&g.ids, (size_t)s->raster_ids_cap, false));
+        CKS(s->alloc(&g.counts, (size_t)s->raster_steps_cap, false));
+        CKS(s->alloc(&g.meta, 4));
+        CK(cudaEventCreateWithFlags(&g.ev, cudaEventDisableTiming));
+    }
+    if (!s->copy_stream) CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    k_raster_stage<<<grid_for(s->raster_ids_cap), 256, 0, s->stream>>>(s->a, g.ids, g.counts, s->raster_steps_cap,
+                                                                        s->raster_ids_cap);
+    k_raster_restart<<<1, 1, 0, s->stream>>>(s->a, g.meta, s->raster_steps_cap, s->raster_ids_cap);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(g.ev, s->stream));
+    s->launches += 2;
+    s->staged += 1;
+    return MGC_OK;
+}
+
+mgc_status mgc_raster_collect(mgc_sim* s, int64_t* first_step, int64_t* counts, int64_t counts_cap, int32_t* ids,
+                              int64_t ids_cap, int64_t* n_steps, int64_t* n_ids)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->staged) return fail(MGC_ERR_INVALID, "no raster is staged (mgc_raster_stage)");
+    CK(cudaSetDevice(s->device));
+    mgc_sim::RasterStage& g = s->stages[s->stage_head];
+    // the stage's copies are done; the steps enqueued after it keep running
+    CK(cudaStreamWaitEvent(s->copy_stream, g.ev, 0));
+    int64_t meta[4];
+    CK(cudaMemcpyAsync(meta, g.meta, sizeof(meta), cudaMemcpyDeviceToHost, s->copy_stream));
+    CK(cudaStreamSynchronize(s->copy_stream));
+    const int64_t step0 = meta[0], ns = meta[1], ni = meta[2];
+    const int32_t status = (int32_t)meta[3];
+    std::vector<int32_t> c32(ns);
+    std::unique_ptr<int32_t[]> staging;
+    int32_t* hid = ids;
+    if (!ids || ids_cap < ni) {
+        staging.reset(new int32_t[std::max<int64_t>(ni, 1)]);
+        hid = staging.get();
+    }
+    if (ns) CK(cudaMemcpyAsync(c32.data(), g.counts, 4 * ns, cudaMemcpyDeviceToHost, s->copy_stream));
+    if (ni) CK(cudaMemcpyAsync(hid, g.ids, 4 * ni, cudaMemcpyDeviceToHost, s->copy_stream));
+    CK(cudaStreamSynchronize(s->copy_stream));
+    s->stage_head ^= 1;
+    s->staged -= 1;
+    return finish_raster(step0, ns, ni, c32.data(), hid, status != 0, status, first_step, counts, counts_cap, ids,
+                         ids_cap, n_steps, n_ids);
 }
 
 mgc_status mgc_read_state(mgc_sim* s, float* v, float* i_exc, float* i_inh, int32_t* refrac, int32_t* last_fired,
