@@ -2347,6 +2347,7 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
         CK(cudaMemcpy(s->a.ev_mark, &ev, 8, cudaMemcpyHostToDevice));
     }
     s->ahead = h.ahead != 0;
+    s->pending = 0;  // a partition's checkpoint is taken between exchanges
     return MGC_OK;
 }
 
