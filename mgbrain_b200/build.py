@@ -12,6 +12,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 OBJ_DIR = os.path.join(ROOT, "_build", "mgbrain_b200")
 LIB = os.path.join(LIB_DIR, "libmgbrain_b200.so")
+LIB_CHECKED = os.path.join(LIB_DIR, "libmgbrain_b200_checked.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = "/usr/bin/g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -35,28 +36,33 @@ def _run(cmd):
     return r
 
 
-def build(verbose=False):
+def build(verbose=False, checked=False):
+    """The library; checked=True builds libmgbrain_b200_checked.so, whose
+    kernels test every index they read from memory before using it."""
     os.makedirs(LIB_DIR, exist_ok=True)
-    os.makedirs(OBJ_DIR, exist_ok=True)
+    obj_dir = OBJ_DIR + ("_checked" if checked else "")
+    lib = LIB_CHECKED if checked else LIB
+    os.makedirs(obj_dir, exist_ok=True)
     headers = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
                + glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True))
     objs = []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         if _stale(obj, [src] + headers):
-            _run([NVCC] + NVFLAGS + ["-c", src, "-o", obj])
+            _run([NVCC] + NVFLAGS + (["-DMGC_CHECKED"] if checked else []) + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp"))):
-        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         if _stale(obj, [src] + headers):
             _run([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
-    if _stale(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"])
+    if _stale(lib, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"])
     if verbose:
-        print("built", LIB)
-    return LIB
+        print("built", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose=True)
+    import sys
+    build(verbose=True, checked="--checked" in sys.argv)

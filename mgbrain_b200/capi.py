@@ -11,7 +11,12 @@ import os
 
 import numpy as np
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libmgbrain_b200.so")
+# MGBRAIN_LIB=checked selects the index-checking build (every index the
+# kernels read from memory is tested before use; a failure is reported by
+# sync), for debugging a network or the library.
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib",
+                        "libmgbrain_b200_checked.so" if os.environ.get("MGBRAIN_LIB") == "checked"
+                        else "libmgbrain_b200.so")
 
 MGC_OK, MGC_ERR_INVALID, MGC_ERR_CUDA, MGC_ERR_NOMEM, MGC_ERR_OVERFLOW, MGC_ERR_NODEVICE = range(6)
 RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)

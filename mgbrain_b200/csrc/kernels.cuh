@@ -34,7 +34,8 @@ namespace mgc {
 enum : int { kRAW = 0, kLIF0 = 1, kPOISSON = 2, kLIF = 3, kLIFE = 4, kLIFB = 5 };
 
 // Device status bits, read back by mgc_sync / mgc_read_raster.
-enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2, kStatusBarrier = 4, kStatusExchange = 8 };
+enum : int { kStatusRasterIds = 1, kStatusRasterSteps = 2, kStatusBarrier = 4, kStatusExchange = 8,
+             kStatusBounds = 16 };
 
 constexpr int kNeuronBlock = 256;
 constexpr int kPushBlock = 256;
@@ -74,7 +75,7 @@ struct StepArgs {
     int32_t* hist_ids;    //   [H][n_src] spike ids per step
     int32_t* hist_cnt;    //   [H]
     const int64_t* bucket;   // [n_src*D + 1] CSR position of (source, bucket)
-    float* acc_e;         //   [2][ns] input arriving at steps of each parity
+    float* acc_e;         //   [4][ns] input arriving at step s in buffer s % 4
     float* acc_i;
     int32_t pull;         // pull method (per-target pass at emission, STDP fused)
     uint32_t* fired_bits; //   [ns/32] spikes of the current step
@@ -96,6 +97,7 @@ struct StepArgs {
     // synapses: CSR by source; word .x = target | delay << tbits, .y = weight bits
     const int64_t* row_ptr;
     uint2* syn;
+    int64_t n_syn;            // synapses in the CSR
     const int32_t* csr_src;   // STDP only
     const uint8_t* plastic;   // STDP only, may be null (all plastic)
     const int64_t* dend_off;  // STDP only: incoming lists
@@ -125,6 +127,18 @@ struct StepArgs {
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
 
+// Checked build (-DMGC_CHECKED, the library libmgbrain_b200_checked.so): every
+// index the kernels take from memory (a spike id, a CSR position, a target,
+// a delay, a history slot) is tested before it is used; a failed test sets
+// kStatusBounds, which mgc_sync reports, and the access is skipped.  In the
+// normal build the tests compile away.
+#ifdef MGC_CHECKED
+#define MGC_OK_INDEX(cond) mgc_check_index(a, (cond))
+__device__ __forceinline__ bool mgc_check_index(const struct StepArgs& a, bool ok);
+#else
+#define MGC_OK_INDEX(cond) true
+#endif
+
 // Fire-and-forget fp32 reduction into global memory (PTX red.add.f32: the
 // same rounding and subnormal flushing as atomicAdd, but no value comes back,
 // so the issuing warp never waits on it).
@@ -133,6 +147,14 @@ __device__ __forceinline__ void red_add(float* p, float v)
     asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t as_u(float f) { return __float_as_uint(f); }
+
+#ifdef MGC_CHECKED
+__device__ __forceinline__ bool mgc_check_index(const StepArgs& a, bool ok)
+{
+    if (!ok) atomicOr(a.status, kStatusBounds);
+    return ok;
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // Step epilogue: run by the last block to finish the step's last kernel.
@@ -383,6 +405,7 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 const int32_t i0 = (int32_t)((gb + h * 32 + lane) << 2);
                 for (int k = 0; k < 4; ++k) {
                     if (fmask[h] & (1u << k)) {
+                        if (!MGC_OK_INDEX(pos < (a.deferred ? a.n_src : a.n))) break;
                         ids[pos] = a.src_base + i0 + k;
                         if (pop_cnt) atomicAdd(pop_cnt + a.tpop[i0 + k], 1);
                         if (rec && rbase + pos < a.raster_ids_cap) a.raster_ids[rbase + pos] = a.src_base + i0 + k;
@@ -483,7 +506,8 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
             const int32_t src = (int32_t)(e.x & a.tmask);
             const int32_t d = (int32_t)(e.x >> a.tbits);
             const float w = as_f(e.y);
-            const bool pre = ok && bit_of(a.fired_bits, src);
+            const bool in_range = !ok || MGC_OK_INDEX(src < a.n && d >= 1 && d < a.M);
+            const bool pre = ok && in_range && bit_of(a.fired_bits, src);
             const unsigned m = __ballot_sync(0xffffffffu, pre);
             unsigned mm = m;
             while (mm) {  // spiking sources in row order
@@ -520,7 +544,7 @@ __global__ void __launch_bounds__(kPushBlock) k_pull(StepArgs a)
                 }
             }
             if (lane == 0) ev += (unsigned long long)__popc(m);
-            if (a.stdp && ok && (pre || post) && (!a.in_plastic || a.in_plastic[q])) {
+            if (a.stdp && ok && in_range && (pre || post) && (!a.in_plastic || a.in_plastic[q])) {
                 float nw = w;
                 if (pre) nw = stdp_weight((int32_t)s - lfT, nw, a.P);
                 if (post) nw = stdp_weight(a.last_fired[src] - (int32_t)s, nw, a.P);
@@ -625,12 +649,16 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
             int32_t h = hs - (a.dmin + k);
             if (h < 0) h += a.H;
             const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n_src + j];
-            const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
-            const int64_t b0 = __ldg(bk);
-            const int64_t seg = __ldg(bk + 1) - b0;
-            const int64_t c0 = (int64_t)c * a.chunk_len;
-            b = b0 + c0;
-            len = seg > c0 ? (int32_t)(seg - c0 < a.chunk_len ? seg - c0 : a.chunk_len) : 0;
+            if (MGC_OK_INDEX(h >= 0 && h < a.H && j < a.n_src && src >= 0 && src < a.n_src)) {
+                const int64_t* bk = a.bucket + (size_t)src * D + k;  // segment [bk[0], bk[1])
+                const int64_t b0 = __ldg(bk);
+                const int64_t seg = __ldg(bk + 1) - b0;
+                const int64_t c0 = (int64_t)c * a.chunk_len;
+                if (MGC_OK_INDEX(b0 >= 0 && seg >= 0 && b0 + seg <= a.n_syn)) {
+                    b = b0 + c0;
+                    len = seg > c0 ? (int32_t)(seg - c0 < a.chunk_len ? seg - c0 : a.chunk_len) : 0;
+                }
+            }
         }
         // 2. segments end to end: exclusive offsets
         int32_t incl = len;
@@ -661,6 +689,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
 #pragma unroll
             for (int u = 0; u < kDeliverUnroll; ++u) {
                 if (base + u * 32 + lane >= tot) continue;
+                if (!MGC_OK_INDEX((w[u].x & a.tmask) < (uint32_t)a.ns)) continue;
                 const float wt = as_f(w[u].y);
                 red_add((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
             }
@@ -1006,8 +1035,10 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
         const int32_t j = (int32_t)(task / a.chunks_per_spike);
         const int32_t c = (int32_t)(task - (int64_t)j * a.chunks_per_spike);
         const int32_t nid = a.spk[j];
+        if (!MGC_OK_INDEX(nid >= 0 && nid < a.n)) continue;
         if (c == 0 && lane == 0 && a.record && rpos + j < a.raster_ids_cap) a.raster_ids[rpos + j] = nid;
         const int64_t rb = a.row_ptr[nid], re = a.row_ptr[nid + 1];
+        if (!MGC_OK_INDEX(rb >= 0 && rb <= re && re <= a.n_syn)) continue;
         const int64_t b = rb + (int64_t)c * kChunk;
         if (b >= re) continue;
         const int64_t e = min(re, b + (int64_t)kChunk);
@@ -1024,6 +1055,7 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
             const uint32_t tgt = w[u].x & a.tmask;
             int32_t slot = slot0 + (int32_t)(w[u].x >> a.tbits);
             if (slot >= a.M) slot -= a.M;
+            if (!MGC_OK_INDEX(tgt < (uint32_t)a.ns && slot >= 0 && slot < a.M)) continue;
             const float wt = as_f(w[u].y);
             float* ring = wt > 0.0f ? a.ring_e : a.ring_i;
             red_add(ring + (size_t)slot * (size_t)a.ns + tgt, wt);
@@ -1051,15 +1083,18 @@ __global__ void __launch_bounds__(kPushBlock) k_stdp(StepArgs a)
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t j = warp; j < cnt; j += nwarps) {
         const int32_t nid = a.spk[j];
+        if (!MGC_OK_INDEX(nid >= 0 && nid < a.n)) continue;
         const int32_t lfn = a.last_fired[nid];
         for (int64_t k = a.row_ptr[nid] + lane; k < a.row_ptr[nid + 1]; k += 32) {
             if (a.plastic && !a.plastic[k]) continue;
             const uint2 e = a.syn[k];
+            if (!MGC_OK_INDEX(k < a.n_syn && (e.x & a.tmask) < (uint32_t)a.n)) continue;
             const int32_t dt = lfn - a.last_fired[e.x & a.tmask];
             a.syn[k].y = as_u(stdp_weight(dt, as_f(e.y), a.P));
         }
         for (int64_t q = a.dend_off[nid] + lane; q < a.dend_off[nid + 1]; q += 32) {
             const int64_t k = a.dend_pos[q];
+            if (!MGC_OK_INDEX(k >= 0 && k < a.n_syn && a.csr_src[k] >= 0 && a.csr_src[k] < a.n)) continue;
             if (a.plastic && !a.plastic[k]) continue;
             const int32_t dt = a.last_fired[a.csr_src[k]] - lfn;
             a.syn[k].y = as_u(stdp_weight(dt, as_f(a.syn[k].y), a.P));

@@ -1023,6 +1023,7 @@ mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim*
     uint2* syn;
     CKS(s->alloc(&syn, S, false));
     a.syn = syn;
+    a.n_syn = S;
     CKS(s->alloc(&s->csr_syn64, S, false));
     DevTmp t_keys2;
     uint32_t* keys2 = nullptr;
@@ -1251,6 +1252,7 @@ mgc_status create_fixed_indegree(const mgc_fixed_indegree_desc* blocks, int32_t 
     uint2* syn;
     CKS(s->alloc(&syn, S, false));
     a.syn = syn;
+    a.n_syn = S;
     if (S > 0) {
         DevTmp t_pt;
         ProjEntry* dpt;
@@ -1369,6 +1371,8 @@ mgc_status mgc_sync(mgc_sim* s)
     int32_t st = 0;
     CK(cudaMemcpy(&st, s->a.status, 4, cudaMemcpyDeviceToHost));
     if (st & kStatusBarrier) return fail(MGC_ERR_CUDA, "a grid barrier of the persistent step group timed out");
+    if (st & kStatusBounds)
+        return fail(MGC_ERR_CUDA, "an index check of the checked build failed (an index outside its array)");
     if (st & kStatusExchange)
         return fail(MGC_ERR_INVALID, "a spike exchange was refused: an id outside the network, or a window with more "
                                      "spikes than the exchange buffer holds");
