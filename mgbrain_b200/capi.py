@@ -367,7 +367,7 @@ class Simulator:
     def read_raster(self, max_steps=1 << 20, max_ids=None):
         """(first step, spikes per step, ids per step in ascending order)."""
         if max_ids is None:
-            max_ids = max(1, self.n) * 64
+            max_ids = max(1 << 20, max(1, self.n) * 64)   # the device raster's default capacity
         counts = np.empty(max_steps, np.int64)
         ids = np.empty(max_ids, np.int32)
         first, ns, ni = C.c_int64(), C.c_int64(), C.c_int64()
@@ -384,7 +384,7 @@ class Simulator:
     def collect_raster(self, max_steps=1 << 20, max_ids=None):
         """The oldest staged raster, as read_raster returns one."""
         if max_ids is None:
-            max_ids = max(1, self.n) * 64
+            max_ids = max(1 << 20, max(1, self.n) * 64)   # the device raster's default capacity
         counts = np.empty(max_steps, np.int64)
         ids = np.empty(max_ids, np.int32)
         first, ns, ni = C.c_int64(), C.c_int64(), C.c_int64()
