@@ -852,6 +852,64 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
 }
 
 // ---------------------------------------------------------------------------
+// Step group for a minimum delay of one step, where the arrivals of step s
+// include the spikes of step s-1: per step the delivery of its arrivals, a
+// grid barrier, the neuron update, a grid barrier.  The group starts and
+// ends in the state the single-step kernels (k_deliver, then k_neuron)
+// start from, so the two forms mix.  Its grid is sized to the neurons, so a
+// small network takes few blocks and cheap barriers.  Waits are bounded
+// (kStatusBarrier).
+// ---------------------------------------------------------------------------
+template <bool CUR>
+__global__ void __launch_bounds__(kPushBlock, 2) k_steps1(StepArgs a, int32_t nsteps)
+{
+    __shared__ int64_t pre[kMaxBuckets + 1];
+    __shared__ int abort_flag;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    int64_t s = *a.step;
+    int32_t slot = a.slots[0], hslot = a.slots[1];
+    int64_t rbase = a.record ? *a.raster_pos : 0;
+    const int64_t rstep0 = *a.raster_step0;
+    if (threadIdx.x == 0) abort_flag = 0;
+    for (int32_t i = 0; i < nsteps; ++i) {
+        const int32_t next_h = hslot + 1 == a.H ? 0 : hslot + 1;
+        // the arrivals of step s: spikes of steps <= s-1, complete at the last barrier
+        if (threadIdx.x < 32) deliver_prefix(a, s, s, hslot, pre);
+        __syncthreads();
+        deliver_tasks(a, s, s, hslot, pre, warp, nwarps);
+        if (!grid_barrier(a, &abort_flag)) return;
+        // step s+1's slot held step s+1-H, which no delivery reads any more
+        if (lead) a.hist_cnt[next_h] = 0;
+        neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+                              a.record ? rbase : 0);
+        if (!grid_barrier(a, &abort_flag)) return;
+        // step s is complete on every block
+        const int32_t nspk = *(volatile int32_t*)(a.hist_cnt + hslot);
+        if (lead && a.record) {
+            const int64_t idx = s - rstep0;
+            if (idx < a.raster_steps_cap)
+                a.raster_counts[idx] = nspk;
+            else
+                atomicOr(a.status, kStatusRasterSteps);
+            if (rbase + nspk > a.raster_ids_cap) atomicOr(a.status, kStatusRasterIds);
+        }
+        if (a.record) rbase += nspk;
+        s += 1;
+        hslot = next_h;
+        slot = slot + 1 == a.M ? 0 : slot + 1;
+    }
+    if (lead) {
+        if (a.record) *a.raster_pos = rbase;
+        a.slots[0] = slot;
+        a.slots[1] = hslot;
+        __threadfence();
+        *a.step = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Pipelined step group (minimum delay >= 4): during step s every block
 // updates its neurons of step s and delivers the arrivals of step s+2 (they
 // depend only on spikes of steps <= s-2), so a block waits only until every

@@ -137,6 +137,7 @@ struct mgc_sim {
     int persistent = 0;               // fused method as cooperative step groups: 1 barrier per
                                       // step, 2 pipelined (min delay >= 4)
     int group_grid_v[2][2] = {{1, 1}, {1, 1}};  // [persistent-1][variant] co-resident grids
+    int group_grid1 = 1;              // minimum delay 1: the step group's grid
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
 
@@ -580,6 +581,7 @@ StepKernel fused_kernel(const mgc_sim* s, int v)
 using GroupKernel = void (*)(StepArgs, int32_t);
 GroupKernel steps_kernel(const mgc_sim* s, int p, int v)
 {
+    if (!s->fused) return s->a.has_cur ? k_steps1<true> : k_steps1<false>;  // minimum delay 1
     if (p == 2) {
         if (s->a.has_cur) return v == 0 ? k_pipe<true, 2> : k_pipe<true, 3>;
         return v == 0 ? k_pipe<false, 2> : k_pipe<false, 3>;
@@ -688,7 +690,16 @@ mgc_status finish_build(mgc_sim* s)
         s->fused_grid = s->fused_grid_v[1];
         // step groups by default (faster than one launch per step on every
         // measured load); the pipelined form needs a minimum delay >= 4
-        s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 0;
+        s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 1;
+        if (!s->fused) {
+            // minimum delay 1: a barrier-per-phase step group sized to the
+            // neurons (8 warps x 64 neuron groups a block per pass)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, 1, 0), kPushBlock, 0));
+            const int64_t wave = (int64_t)prop.multiProcessorCount * std::max(1, occ);
+            const int64_t want = ((int64_t)a.ns / 4 + 511) / 512;
+            s->group_grid1 = (int)std::max<int64_t>(1, std::min(wave, want));
+            CKS(s->alloc(&a.bar, 4));  // the grid barrier's arrivals and generation
+        }
         if (s->fused) {
             for (int p = 1; p <= 2; ++p)
                 for (int v = 0; v < 2; ++v) {
@@ -1322,7 +1333,7 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
         CKS(enqueue_step(s));  // catches up the delivery, leaves ahead = true
         --left;
     }
-    if (s->persistent && s->fused && !sched_wanted(s)) {
+    if (s->persistent && s->a.deferred && !sched_wanted(s)) {
         // one cooperative launch per group: every block resident, a grid
         // barrier between steps (or the pipelined arrive/wait) instead of a launch
         const int p = s->persistent, v = s->fused_variant;
@@ -1333,9 +1344,9 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
             ga.trace = nullptr;
             void* args[] = {&ga, &n};
             CK(cudaMemsetAsync(s->a.bar, 0, 4 * sizeof(unsigned int), s->stream));  // clean barriers
-            const cudaError_t e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v),
-                                                              dim3(s->group_grid_v[p - 1][v]), dim3(kPushBlock),
-                                                              args, 0, s->stream);
+            const int grid = s->fused ? s->group_grid_v[p - 1][v] : s->group_grid1;
+            const cudaError_t e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(grid),
+                                                              dim3(kPushBlock), args, 0, s->stream);
             if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
                 // the blocks cannot all be resident here (e.g. a shared
                 // device): fall back to the graphs of single-step kernels
@@ -1717,7 +1728,7 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->mode = s->mode;
     info->graph_steps = s->graph_steps ? s->graph_steps : kGraphSteps;
     info->device_bytes = (int64_t)s->bytes;
-    info->persistent = s->fused && !sched_wanted(s) ? s->persistent : 0;
+    info->persistent = s->a.deferred && !sched_wanted(s) ? s->persistent : 0;
     info->first_neuron = s->a.src_base;
     info->total_neurons = s->n_src;
     return MGC_OK;
@@ -1865,7 +1876,8 @@ mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
 {
     if (!s) return fail(MGC_ERR_INVALID, "null handle");
     if (mode < 0 || mode > 2) return fail(MGC_ERR_INVALID, "step-group mode %d (0, 1 or 2)", mode);
-    if (mode && !s->fused) return fail(MGC_ERR_INVALID, "step groups need the fused deferred method");
+    if (mode && !s->a.deferred) return fail(MGC_ERR_INVALID, "step groups need the deferred method");
+    if (mode == 2 && !s->fused) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
     if (mode == 2 && s->dmin < 4) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
     if (s->graph && s->persistent != mode) {  // the scheduler's graph holds step groups of the old mode
         CK(cudaStreamSynchronize(s->stream));
@@ -1940,13 +1952,14 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
         rep->trials += 1;
     }
     TuneCand best_c = cands[best_i];
-    for (int t = 0; t < 4 && st == MGC_OK && s->fused && !sched_wanted(s); ++t) {
+    for (int t = 0; t < (s->fused ? 4 : 1) && st == MGC_OK && s->a.deferred && !sched_wanted(s); ++t) {
         // the best chunking once more as step groups (p = 2: pipelined) of
         // each kernel instantiation: their best register budget can differ
-        // from the single-step kernel's
+        // from the single-step kernel's (a minimum delay of 1: the one
+        // step-group form, k_steps1)
         const int p = 1 + t / 2;
         if (p == 2 && s->dmin < 4) break;
-        const TuneCand c{cands[best_i].chunk_target, t % 2 == 0 ? 2 : 3};
+        const TuneCand c = s->fused ? TuneCand{cands[best_i].chunk_target, t % 2 == 0 ? 2 : 3} : cands[best_i];
         st = apply_cand(s, c, sms);
         s->persistent = p;
         if (st == MGC_OK) st = mgc_run(s, kGraphSteps);

@@ -59,3 +59,42 @@ def test_pipelined_needs_min_delay_four():
     with pytest.raises(mgb.MgcError):
         sim.set_persistent(2)
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nu", [0.002, 0.02])
+def test_one_step_delay_group_equals_graphs(nu):
+    """A minimum delay of one step (the arrivals of step s include step s-1's
+    spikes): the step group with a barrier after the delivery and after the
+    update gives the rasters and state of the single-step kernels, also when
+    the two forms alternate."""
+    w = bench.workload(scale=0.03, nu=nu)
+    projs = [(s, t, k, wt, 1, 6) for (s, t, k, wt, _, _) in w["projs"]]
+
+    def mk():
+        return mgb.Simulator.fixed_indegree(w["pops"], projs, w["lif"], rate=w["rate"], v_init=w["v0"],
+                                            conn_seed=8, seed=9)
+    ref = mk()
+    ref.set_persistent(0)
+    ref.run(2500)
+    _, cr, ir = ref.read_raster()
+    vr = ref.state()["V"]
+    ev = ref.info()["events"]
+    ref.close()
+    sim = mk()
+    assert sim.info()["persistent"] == 1          # the default for this method
+    sim.run(1000)
+    sim.set_persistent(0)
+    sim.run(77)
+    sim.set_persistent(1)
+    sim.run(1)
+    sim.run(1422)
+    sim.sync()
+    _, c, i = sim.read_raster()
+    assert np.array_equal(c, cr) and np.array_equal(i, ir)
+    assert np.array_equal(sim.state()["V"], vr)
+    assert sim.info()["events"] == ev
+    assert c.sum() > 0
+    with pytest.raises(mgb.MgcError):
+        sim.set_persistent(2)
+    sim.close()
