@@ -1,5 +1,6 @@
 """The index-checking build (libmgbrain_b200_checked.so, selected with
-MGBRAIN_LIB=checked): the GPU parity suites pass with every index the kernels
+MGBRAIN_LIB=checked): the GPU parity, step-group, partition, STDP, failure,
+batch, checkpoint, edge-case and staged-readout suites pass with every index the kernels
 read from memory tested before use, and no test fires (a fired test would
 make sync raise).  This is the project's stand-in for a memory checker, which
 is not available on the GPU machines here."""
@@ -11,7 +12,8 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SUITES = ["tests/test_parity_gpu.py", "tests/test_persistent_gpu.py", "tests/test_partition_gpu.py",
-          "tests/test_stdp_net.py", "tests/test_faults_gpu.py"]
+          "tests/test_stdp_net.py", "tests/test_faults_gpu.py", "tests/test_batch.py",
+          "tests/test_checkpoint_gpu.py", "tests/test_edge_cases_gpu.py", "tests/test_raster_stage_gpu.py"]
 
 PROBE = """
 import mgbrain_b200 as mgb, bench

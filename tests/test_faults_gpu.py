@@ -5,6 +5,8 @@ uses them; a raster buffer too small for the run reported as an overflow
 while the simulation itself is unaffected; the step groups' bounded waits
 run out on a counter nothing advances and leave the device usable; and
 run-twice determinism, bit for bit, of the methods that promise it."""
+import gc
+
 import numpy as np
 import pytest
 import torch
@@ -42,6 +44,7 @@ def test_every_allocation_failure_is_reported_and_freed(build):
         return mgb.Simulator.from_arrays(*args, **kw, part=(100, 300))
 
     make().close()                   # warm: library, context, allocator pools
+    gc.collect()                     # handles other tests left to the garbage collector go first
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info()[0]
     k = 1
@@ -61,8 +64,11 @@ def test_every_allocation_failure_is_reported_and_freed(build):
         s.close()
         break
     assert k > 5                     # the build allocates in several places
+    gc.collect()
     torch.cuda.synchronize()
-    assert abs(torch.cuda.mem_get_info()[0] - free0) < (64 << 20)
+    # nothing leaked: free memory did not shrink (it may grow, when memory
+    # other code held is released meanwhile)
+    assert torch.cuda.mem_get_info()[0] > free0 - (64 << 20)
 
 
 @pytest.mark.gpu
