@@ -69,7 +69,7 @@ struct StepArgs {
     int32_t deferred;     // deferred delivery (else ring)
     int32_t dmin;         // deferred: delay of bucket 0
     int32_t D;            //   number of delay buckets per row
-    int32_t H;            //   history slots (>= dmax + 1)
+    int32_t H;            //   history slots: dmax + 3 (the pipelined group clears a slot two steps ahead)
     int32_t bucket_chunks;//   delivery tasks per (spike, delay) segment
     int32_t chunk_len;    //   synapses per task: segment positions [c*len, (c+1)*len)
     int32_t* hist_ids;    //   [H][n_src] spike ids per step
@@ -121,7 +121,7 @@ struct StepArgs {
     const uint8_t* tpop;      // [ns] trace population of each neuron (< kTracePops)
     float* trace;             // [kTraceSteps][kTraceCols]
     unsigned long long* ev_mark;  // events counter at the previous step's end
-    unsigned int* bar;        // [4] step-group barriers: arrivals + generation (k_steps),
+    unsigned int* bar;        // [4] step-group barriers: arrivals + generation (k_steps, k_steps1),
                               //     phase arrival counters (k_pipe)
 };
 
