@@ -122,10 +122,11 @@ typedef struct mgc_info {
     int32_t mode;
     int32_t graph_steps;       /* steps per captured CUDA graph */
     int64_t device_bytes;      /* device memory held by the handle */
-    int32_t persistent;        /* steps run as step groups: 0 no (graphs), 1 barrier per step, 2 pipelined */
+    int32_t persistent;        /* steps run as step groups: 0 no (graphs), 1 barrier per step, 2 pipelined,
+                                  3 windowed */
     int32_t first_neuron;      /* partition handles: whole-network id of neuron 0 (else 0) */
     int32_t total_neurons;     /* partition handles: neurons of the whole network (else n_neurons) */
-    int32_t reserved;
+    int32_t window;            /* steps per window of the windowed step group (0: minimum delay 1) */
 } mgc_info;
 
 /* Replaces MGSimulator::MGSimulator(Network&, std::vector<int>&, int)
@@ -301,6 +302,8 @@ typedef struct mgc_tune_report {
     int32_t chunk_len;            /* chosen synapses per delivery task (deferred method) */
     int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
     int32_t persistent;           /* chosen step-group mode of the fused method (mgc_set_persistent) */
+    int32_t window;               /* chosen window of the windowed step group (mgc_set_window) */
+    int32_t reserved;
     double ms_per_step;           /* time per step of the chosen configuration */
     double default_ms_per_step;   /* time per step of the builder's configuration */
     int64_t steps;                /* steps simulated by the trials */
@@ -321,7 +324,10 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * cooperative step groups of up to
  * 1024 steps with a grid barrier between steps; 2 pipelined step groups
  * (minimum delay >= 4): during step s each block delivers the arrivals of
- * step s+2 and waits only until every block has finished step s-2.
+ * step s+2 and waits only until every block has finished step s-2; 3
+ * windowed step groups (minimum delay >= 2): the arrivals of a window of W
+ * steps (mgc_set_window) are delivered before it, then every neuron advances
+ * the W steps with its state in registers, two grid barriers per window.
  * Default: 2 when the minimum delay is >= 4, else 1; the autotuner may pick
  * another.  If the device cannot keep all blocks of a group resident, the
  * call falls back to 0.  Results are the same in every mode; while a schedule mode other than
@@ -329,6 +335,12 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * bounded (a time-out makes mgc_sync return MGC_ERR_CUDA).  No reference
  * counterpart. */
 mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
+
+/* Steps per window of the windowed step group (mode 3 of
+ * mgc_set_persistent): 1 <= steps <= min(4, minimum delay); default the
+ * largest.  Results are the same for every window.  No reference
+ * counterpart. */
+mgc_status mgc_set_window(mgc_sim* sim, int32_t steps);
 
 /* ---- Step scheduler (fused deferred method: minimum delay >= 2) ----------
  * Each CUDA graph of 64 steps starts with a decision kernel that picks which

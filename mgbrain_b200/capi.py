@@ -29,7 +29,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_checkpoint_size",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_set_window", "mgc_checkpoint_size",
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
@@ -71,8 +71,8 @@ class FixedInDegreeDesc(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [
         ("trials", C.c_int32), ("chunk_len", C.c_int32), ("blocks_per_sm", C.c_int32),
-        ("persistent", C.c_int32), ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double),
-        ("steps", C.c_int64),
+        ("persistent", C.c_int32), ("window", C.c_int32), ("reserved", C.c_int32),
+        ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double), ("steps", C.c_int64),
     ]
 
 
@@ -91,7 +91,7 @@ class Info(C.Structure):
         ("max_delay", C.c_int32), ("n_synapses", C.c_int64), ("step", C.c_int64),
         ("events", C.c_int64), ("mode", C.c_int32), ("graph_steps", C.c_int32),
         ("device_bytes", C.c_int64), ("persistent", C.c_int32), ("first_neuron", C.c_int32),
-        ("total_neurons", C.c_int32), ("reserved", C.c_int32),
+        ("total_neurons", C.c_int32), ("window", C.c_int32),
     ]
 
 
@@ -156,6 +156,8 @@ def lib():
     L.mgc_autotune.restype = C.c_int
     L.mgc_set_persistent.argtypes = [vp, i32]
     L.mgc_set_persistent.restype = C.c_int
+    L.mgc_set_window.argtypes = [vp, i32]
+    L.mgc_set_window.restype = C.c_int
     L.mgc_checkpoint_size.argtypes = [vp, C.POINTER(i64)]
     L.mgc_checkpoint_save.argtypes = [vp, vp, i64]
     L.mgc_checkpoint_load.argtypes = [vp, vp, i64]
@@ -459,7 +461,7 @@ class Simulator:
         steps advance the simulation (report["steps"] of them)."""
         r = TuneReport()
         check(lib().mgc_autotune(self._h, int(steps_per_trial), C.byref(r)))
-        return {k: getattr(r, k) for k, _ in TuneReport._fields_}
+        return {k: getattr(r, k) for k, _ in TuneReport._fields_ if k != "reserved"}
 
     # ---- step scheduler ---------------------------------------------------
     def sched_mode(self, mode):
@@ -503,8 +505,13 @@ class Simulator:
 
     def set_persistent(self, mode=1):
         """0: CUDA graphs of single-step kernels; 1: cooperative step groups
-        with a grid barrier per step; 2: pipelined step groups."""
+        with a grid barrier per step; 2: pipelined step groups; 3: windowed
+        step groups (set_window)."""
         check(lib().mgc_set_persistent(self._h, int(mode)))
+
+    def set_window(self, steps):
+        """Steps per window of the windowed step group (1..min(4, min delay))."""
+        check(lib().mgc_set_window(self._h, int(steps)))
 
     def profile(self, steps):
         """Milliseconds spent in (neuron update, event push, STDP) over `steps`

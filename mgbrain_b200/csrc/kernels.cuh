@@ -69,7 +69,7 @@ struct StepArgs {
     int32_t deferred;     // deferred delivery (else ring)
     int32_t dmin;         // deferred: delay of bucket 0
     int32_t D;            //   number of delay buckets per row
-    int32_t H;            //   history slots: dmax + 3 (the pipelined group clears a slot two steps ahead)
+    int32_t H;            //   history slots: dmax + 4 (step groups clear slots up to four steps ahead)
     int32_t bucket_chunks;//   delivery tasks per (spike, delay) segment
     int32_t chunk_len;    //   synapses per task: segment positions [c*len, (c+1)*len)
     int32_t* hist_ids;    //   [H][n_src] spike ids per step
@@ -588,7 +588,7 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 {
     const int D = a.D;
     const int32_t hs = hist_slot(a, sa, s, hslot);
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     int64_t carry = 0;
     if (lane == 0) pre[0] = 0;
     for (int base = 0; base < D; base += 32) {
@@ -611,17 +611,22 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 
 // The tasks themselves, after deliver_prefix and a block barrier.
 // blk_ev: when given, the warps add their delivered events into this block
-// counter (shared memory) instead of the global one.
+// counter (shared memory) instead of the global one.  NMAX > 1: the tasks of
+// the n <= NMAX consecutive arrival steps sa, sa+1, ... as one task space
+// (step k's prefixes at pre + k*(D+1)), so that a warp's lanes fetch the
+// segments of several steps in one batch.
+template <int NMAX = 1>
 __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot,
                                               const int64_t* pre, int64_t warp, int64_t nwarps,
-                                              unsigned long long* blk_ev = nullptr)
+                                              unsigned long long* blk_ev = nullptr, int n = 1)
 {
     const int D = a.D;
-    const int32_t hs = hist_slot(a, sa, s, hslot);
     const int CH = a.bucket_chunks;
-    const int64_t total = pre[D] * CH;  // (spike, delay) segments x chunks
-    float* acc_e = acc_buf(a, a.acc_e, sa);
-    float* acc_i = acc_buf(a, a.acc_i, sa);
+    int64_t first[NMAX + 1];  // task offset of each step
+    first[0] = 0;
+#pragma unroll
+    for (int k = 0; k < NMAX; ++k) first[k + 1] = first[k] + (k < n ? pre[(size_t)k * (D + 1) + D] * CH : 0);
+    const int64_t total = first[NMAX];  // (spike, delay) segments x chunks
     const int lane = threadIdx.x & 31;
     unsigned long long ev = 0;
     // tasks per warp: 32, or fewer when the grid has more lanes than tasks,
@@ -636,16 +641,27 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
         const int64_t f = fb + lane;
         int64_t b = 0;
         int32_t len = 0;
+        int step = 0;  // arrival step sa + step of the lane's task
         if (lane < per && f < total) {
-            const int64_t fs = f / CH;               // segment task
-            const int32_t c = (int32_t)(f - fs * CH);  // chunk of it
-            int lo = 0, hi = D - 1;  // last k with pre[k] <= fs
+            int64_t f0 = 0;
+#pragma unroll
+            for (int k = 1; k < NMAX; ++k)
+                if (f >= first[k]) {
+                    step = k;
+                    f0 = first[k];
+                }
+            const int64_t* pk = pre + (size_t)step * (D + 1);
+            const int32_t hs = hist_slot(a, sa + step, s, hslot);
+            const int64_t fl = f - f0;
+            const int64_t fs = fl / CH;               // segment task
+            const int32_t c = (int32_t)(fl - fs * CH);  // chunk of it
+            int lo = 0, hi = D - 1;  // last k with pk[k] <= fs
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
-                if (pre[mid] <= fs) lo = mid; else hi = mid - 1;
+                if (pk[mid] <= fs) lo = mid; else hi = mid - 1;
             }
             const int k = lo;
-            const int32_t j = (int32_t)(fs - pre[k]);
+            const int32_t j = (int32_t)(fs - pk[k]);
             int32_t h = hs - (a.dmin + k);
             if (h < 0) h += a.H;
             const int32_t src = a.hist_ids[(size_t)h * (size_t)a.n_src + j];
@@ -673,6 +689,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
         // 3. all lanes over the concatenated synapses
         for (int32_t base = 0; base < tot; base += 32 * kDeliverUnroll) {
             uint2 w[kDeliverUnroll];
+            int st_of[kDeliverUnroll];
 #pragma unroll
             for (int u = 0; u < kDeliverUnroll; ++u) {
                 const int32_t idx = base + u * 32 + lane;
@@ -684,6 +701,7 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
                 }
                 const int64_t bl = __shfl_sync(0xffffffffu, b, L);
                 const int32_t el = __shfl_sync(0xffffffffu, excl, L);
+                if (NMAX > 1) st_of[u] = __shfl_sync(0xffffffffu, step, L);
                 w[u] = idx < tot ? __ldcs(a.syn + bl + (idx - el)) : make_uint2(0u, 0u);
             }
 #pragma unroll
@@ -691,7 +709,8 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
                 if (base + u * 32 + lane >= tot) continue;
                 if (!MGC_OK_INDEX((w[u].x & a.tmask) < (uint32_t)a.ns)) continue;
                 const float wt = as_f(w[u].y);
-                red_add((wt > 0.0f ? acc_e : acc_i) + (w[u].x & a.tmask), wt);
+                const int64_t sx = sa + (NMAX > 1 ? st_of[u] : 0);
+                red_add(acc_buf(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
             }
         }
     }
@@ -793,6 +812,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
     __shared__ int64_t pre[kMaxBuckets + 1];
     __shared__ int pop_cnt[kTracePops];
     __shared__ int abort_flag;
+    __shared__ unsigned long long blk_ev;  // without the trace: the block's events, added once at the end
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
@@ -800,7 +820,10 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
     int32_t slot = a.slots[0], hslot = a.slots[1];
     int64_t rbase = a.record ? *a.raster_pos : 0;
     const int64_t rstep0 = *a.raster_step0;
-    if (threadIdx.x == 0) abort_flag = 0;
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        blk_ev = 0;
+    }
     for (int32_t i = 0; i < nsteps; ++i) {
         const int32_t next_h = hslot + 1 == a.H ? 0 : hslot + 1;
         if (lead) {
@@ -818,7 +841,11 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
         __syncthreads();
         if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
             atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
-        deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps);
+        deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps, a.trace ? nullptr : &blk_ev);
+        if (!a.trace && i == nsteps - 1) {  // the block's events, before the last barrier
+            __syncthreads();
+            if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);
+        }
         if (!grid_barrier(a, &abort_flag)) return;
         // step s is complete on every block
         const int32_t nspk = *(volatile int32_t*)(a.hist_cnt + hslot);
@@ -844,10 +871,190 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
     }
     if (lead) {
         if (a.record) *a.raster_pos = rbase;
+        *a.ev_mark = *(volatile unsigned long long*)a.events;  // every block's events are in
         a.slots[0] = slot;
         a.slots[1] = hslot;
         __threadfence();
         *a.step = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Windowed step group (window W <= minimum delay, W <= 4).  The inputs of
+// the W steps of a window arrive from spikes of steps before the window, so
+// all of them are delivered before it, and then every neuron advances W
+// steps in registers: its state is loaded and stored once per window, its W
+// input slots are loaded together, and the blocks meet twice per window (after
+// the update, after the next window's deliveries) instead of at every step.
+// The arithmetic of each step is that of the single-step update, step by
+// step, so the results are the same bits.  Accumulator buffers: step x in
+// x & 3, as for the other kernels (W <= 4 keeps a window's buffers distinct);
+// history: H >= max delay + 4, so the slots cleared for the next window hold
+// steps no delivery of this window reads.  The group starts and ends in the
+// state of the single-step kernels (arrivals of its first step delivered,
+// nothing later).  Waits are bounded (kStatusBarrier).
+// ---------------------------------------------------------------------------
+constexpr int kMaxWindow = 4;
+
+// Neurons [first group, ...) advanced through the window's wl steps.  One
+// group of four neurons per lane per pass: its state and its wl input slots
+// are loaded at once, the steps run in registers, the state is stored once.
+template <bool CUR>
+__device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int wl, int32_t hs0, int64_t warp,
+                                              int64_t nwarps)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t ngroups = a.ns >> 2;
+    for (int64_t gb = warp * 32; gb < ngroups; gb += nwarps * 32) {
+        const int64_t g = gb + lane;
+        const bool have = g < ngroups;
+        char4 t4 = make_char4(0, 0, 0, 0);
+        float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), ce4 = v4, ci4 = v4;
+        int4 r4 = make_int4(0, 0, 0, 0);
+        float4 e4[kMaxWindow], i4[kMaxWindow];
+        if (have) {
+            t4 = __ldg(reinterpret_cast<const char4*>(a.type) + g);
+            v4 = reinterpret_cast<float4*>(a.V)[g];
+            r4 = reinterpret_cast<int4*>(a.refrac)[g];
+            if (CUR) {
+                ce4 = reinterpret_cast<float4*>(a.Iexc)[g];
+                ci4 = reinterpret_cast<float4*>(a.Iinh)[g];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kMaxWindow; ++k) {
+            e4[k] = i4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (have && k < wl) {
+                e4[k] = reinterpret_cast<float4*>(acc_buf(a, a.acc_e, w0 + k))[g];
+                i4[k] = reinterpret_cast<float4*>(acc_buf(a, a.acc_i, w0 + k))[g];
+            }
+        }
+        const int32_t i0 = (int32_t)(g << 2);
+        const bool pois = t4.x == kPOISSON || t4.y == kPOISSON || t4.z == kPOISSON || t4.w == kPOISSON;
+#pragma unroll
+        for (int k = 0; k < kMaxWindow; ++k) {
+            if (k >= wl) break;
+            const int64_t s = w0 + k;
+            unsigned fm = 0;
+            if (have) {
+                float u[4] = {0.f, 0.f, 0.f, 0.f};
+                if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
+                fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e4[k].x, i4[k].x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
+                fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e4[k].y, i4[k].y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
+                fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e4[k].z, i4[k].z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
+                fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e4[k].w, i4[k].w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                // the step's input was used: its slot is cleared for step s+4
+                reinterpret_cast<float4*>(acc_buf(a, a.acc_e, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                reinterpret_cast<float4*>(acc_buf(a, a.acc_i, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            // the step's spikes into its history slot, in neuron order within the warp
+            const int c = __popc(fm);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            if (total) {
+                int32_t hs = hs0 + k;
+                if (hs >= a.H) hs -= a.H;
+                int32_t base = 0;
+                if (lane == 31) base = atomicAdd(a.hist_cnt + hs, total);
+                base = __shfl_sync(0xffffffffu, base, 31);
+                int32_t pos = base + incl - c;
+                int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
+                for (int q = 0; q < 4; ++q)
+                    if (fm & (1u << q)) {
+                        if (!MGC_OK_INDEX(pos < a.n_src)) break;
+                        ids[pos++] = a.src_base + i0 + q;
+                    }
+            }
+        }
+        if (have) {
+            reinterpret_cast<float4*>(a.V)[g] = v4;
+            reinterpret_cast<int4*>(a.refrac)[g] = r4;
+            if (CUR) {
+                reinterpret_cast<float4*>(a.Iexc)[g] = ce4;
+                reinterpret_cast<float4*>(a.Iinh)[g] = ci4;
+            }
+        }
+    }
+}
+
+// The arrivals of steps [sa0, sa0 + n) (n <= kMaxWindow), from spikes of steps
+// before sa0: the prefixes of the n steps by the first n warps, then every
+// warp through the n steps' tasks without a barrier between them.  s, hslot:
+// a step and its history slot, for the slot arithmetic.
+__device__ __forceinline__ void deliver_window(const StepArgs& a, int64_t sa0, int n, int64_t s, int32_t hslot,
+                                               int64_t* pre, int64_t warp, int64_t nwarps, unsigned long long* blk_ev)
+{
+    const int wib = threadIdx.x >> 5;
+    for (int k = wib; k < n; k += blockDim.x >> 5) deliver_prefix(a, sa0 + k, s, hslot, pre + (size_t)k * (a.D + 1));
+    __syncthreads();
+    deliver_tasks<kMaxWindow>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
+}
+
+__device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0,
+                                            int64_t& rbase);
+
+template <bool CUR, int MINB>
+__global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t nsteps, int32_t W)
+{
+    extern __shared__ int64_t wpre[];   // [kMaxWindow][D + 1]
+    __shared__ int abort_flag;
+    __shared__ unsigned long long blk_ev;  // the block's delivered events, added once at the end
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+    const int64_t s0 = *a.step;
+    const int32_t slot0 = a.slots[0], h0 = a.slots[1];
+    const bool rec = a.record != 0;
+    int64_t rbase = rec ? *a.raster_pos : 0;
+    const int64_t rstep0 = *a.raster_step0;
+    const int64_t s_end = s0 + nsteps;
+    auto hs_of = [&](int64_t x) { return (int32_t)((h0 + (x - s0)) % a.H); };
+    if (threadIdx.x == 0) {
+        abort_flag = 0;
+        blk_ev = 0;
+    }
+    // prologue: the arrivals of the first window's later steps (its first
+    // step's are delivered), their history slots cleared
+    {
+        const int n = (int)(nsteps < W ? nsteps - 1 : W - 1);
+        if (lead)
+            for (int k = 1; k <= n; ++k) a.hist_cnt[hs_of(s0 + k)] = 0;
+        __syncthreads();
+        if (n > 0) deliver_window(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
+        if (!grid_barrier(a, &abort_flag)) return;
+    }
+    for (int64_t w0 = s0; w0 < s_end;) {
+        const int wl = (int)(s_end - w0 < W ? s_end - w0 : W);
+        neuron_window<CUR>(a, w0, wl, hs_of(w0), warp, nwarps);
+        if (!grid_barrier(a, &abort_flag)) return;
+        // the window's spikes are complete: its raster, then the next
+        // window's arrivals (only those of s_end after the last window)
+        if (rec && blockIdx.x == 0)
+            for (int k = 0; k < wl; ++k) raster_copy(a, w0 + k, hs_of(w0 + k), rstep0, rbase);
+        const int64_t next = w0 + wl;
+        const int nn = (int)(next < s_end ? (s_end - next < W ? s_end - next : W) : 1);
+        if (lead)
+            for (int k = 0; k < nn; ++k) a.hist_cnt[hs_of(next + k)] = 0;
+        deliver_window(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
+        if (next >= s_end) {  // the block's events, before the last barrier
+            __syncthreads();
+            if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);
+        }
+        if (!grid_barrier(a, &abort_flag)) return;
+        w0 = next;
+    }
+    if (lead) {
+        if (rec) *a.raster_pos = rbase;
+        *a.ev_mark = *(volatile unsigned long long*)a.events;
+        a.slots[0] = (int32_t)((slot0 + nsteps) % a.M);
+        a.slots[1] = hs_of(s_end);
+        __threadfence();
+        *a.step = s_end;
     }
 }
 

@@ -135,8 +135,11 @@ struct mgc_sim {
     float* sched_data = nullptr;      // device [kMaxDataset][kTraceCols]
     bool sched_graph = false;         // the step-group graph branches on the scheduler's choice
     int persistent = 0;               // fused method as cooperative step groups: 1 barrier per
-                                      // step, 2 pipelined (min delay >= 4)
+                                      // step, 2 pipelined (min delay >= 4), 3 windowed
     int group_grid_v[2][2] = {{1, 1}, {1, 1}};  // [persistent-1][variant] co-resident grids
+    int window = 1;                   // steps per window of the windowed group (<= min delay, <= 4)
+    int window_grid_v[2] = {1, 1};    // its co-resident grids by variant
+    size_t window_smem = 0;           // its dynamic shared memory: the window's delivery prefixes
     int group_grid1 = 1;              // minimum delay 1: the step group's grid
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
@@ -534,7 +537,7 @@ mgc_status choose_mode(mgc_sim* s, int requested)
         a.deferred = 1;
         a.D = D;
         a.dmin = s->dmin;
-        a.H = s->dmax + 3;  // + 2: the pipelined step group clears a slot two steps ahead
+        a.H = s->dmax + 4;  // + 3: the windowed step group clears the next window's slots
     }
     return MGC_OK;
 }
@@ -589,6 +592,20 @@ GroupKernel steps_kernel(const mgc_sim* s, int p, int v)
     if (s->a.has_cur) return v == 0 ? k_steps<true, 2> : k_steps<true, 3>;
     return v == 0 ? k_steps<false, 2> : k_steps<false, 3>;
 }
+
+// The windowed step group of variant v (templates over the update's
+// current arrays and the register budget, as the other step groups).
+using WindowKernel = void (*)(StepArgs, int32_t, int32_t);
+WindowKernel window_kernel(const mgc_sim* s, int v)
+{
+    if (s->a.has_cur) return v == 0 ? k_window<true, 2> : k_window<true, 3>;
+    return v == 0 ? k_window<false, 2> : k_window<false, 3>;
+}
+
+// The step-group mode the scheduler's graph runs for mode p: the windowed
+// group keeps no schedule trace, so the graph takes the pipelined group (or
+// the barrier per step, for a minimum delay below 4) in its place.
+int graph_group_mode(const mgc_sim* s, int p) { return p == 3 ? (s->dmin >= 4 ? 2 : 1) : p; }
 
 constexpr int32_t kPersistentSteps = 1024;  // steps per cooperative launch
 
@@ -706,6 +723,16 @@ mgc_status finish_build(mgc_sim* s)
                     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, p, v), kPushBlock, 0));
                     s->group_grid_v[p - 1][v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
                 }
+            // windowed group: prefixes of up to kMaxWindow steps in dynamic shared memory
+            s->window = std::min(kMaxWindow, s->dmin);
+            s->window_smem = (size_t)kMaxWindow * (size_t)(a.D + 1) * sizeof(int64_t);
+            for (int v = 0; v < 2; ++v) {
+                CK(cudaFuncSetAttribute((const void*)window_kernel(s, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)s->window_smem));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, window_kernel(s, v), kPushBlock,
+                                                                 s->window_smem));
+                s->window_grid_v[v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+            }
             CKS(init_sched(s));
         }
     } else {
@@ -836,7 +863,7 @@ mgc_status build_sched_graph(mgc_sim* s)
         if (s->persistent) {
             // the group as one cooperative step-group kernel of variant v,
             // after a node that clears its barrier counters
-            const int p = s->persistent;
+            const int p = graph_group_mode(s, s->persistent);
             cudaMemsetParams mp = {};
             mp.dst = s->a.bar;
             mp.value = 0;
@@ -1344,9 +1371,17 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
             ga.trace = nullptr;
             void* args[] = {&ga, &n};
             CK(cudaMemsetAsync(s->a.bar, 0, 4 * sizeof(unsigned int), s->stream));  // clean barriers
-            const int grid = s->fused ? s->group_grid_v[p - 1][v] : s->group_grid1;
-            const cudaError_t e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(grid),
-                                                              dim3(kPushBlock), args, 0, s->stream);
+            cudaError_t e;
+            if (p == 3) {
+                int32_t w = s->window;
+                void* wargs[] = {&ga, &n, &w};
+                e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v), dim3(s->window_grid_v[v]),
+                                                dim3(kPushBlock), wargs, s->window_smem, s->stream);
+            } else {
+                const int grid = s->fused ? s->group_grid_v[p - 1][v] : s->group_grid1;
+                e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(grid), dim3(kPushBlock),
+                                                args, 0, s->stream);
+            }
             if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
                 // the blocks cannot all be resident here (e.g. a shared
                 // device): fall back to the graphs of single-step kernels
@@ -1731,6 +1766,7 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->persistent = s->a.deferred && !sched_wanted(s) ? s->persistent : 0;
     info->first_neuron = s->a.src_base;
     info->total_neurons = s->n_src;
+    info->window = s->fused ? s->window : 0;
     return MGC_OK;
 }
 
@@ -1875,10 +1911,11 @@ mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
 mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
 {
     if (!s) return fail(MGC_ERR_INVALID, "null handle");
-    if (mode < 0 || mode > 2) return fail(MGC_ERR_INVALID, "step-group mode %d (0, 1 or 2)", mode);
+    if (mode < 0 || mode > 3) return fail(MGC_ERR_INVALID, "step-group mode %d (0, 1, 2 or 3)", mode);
     if (mode && !s->a.deferred) return fail(MGC_ERR_INVALID, "step groups need the deferred method");
     if (mode == 2 && !s->fused) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
     if (mode == 2 && s->dmin < 4) return fail(MGC_ERR_INVALID, "the pipelined step group needs a minimum delay >= 4");
+    if (mode == 3 && !s->fused) return fail(MGC_ERR_INVALID, "the windowed step group needs a minimum delay >= 2");
     if (s->graph && s->persistent != mode) {  // the scheduler's graph holds step groups of the old mode
         CK(cudaStreamSynchronize(s->stream));
         cudaGraphExecDestroy(s->graph);
@@ -1886,6 +1923,16 @@ mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
         s->sched_graph = false;
     }
     s->persistent = mode;
+    return MGC_OK;
+}
+
+mgc_status mgc_set_window(mgc_sim* s, int32_t steps)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (!s->fused) return fail(MGC_ERR_INVALID, "the windowed step group needs a minimum delay >= 2");
+    const int most = std::min(kMaxWindow, s->dmin);
+    if (steps < 1 || steps > most) return fail(MGC_ERR_INVALID, "window of %d steps (1 to %d)", steps, most);
+    s->window = steps;
     return MGC_OK;
 }
 
@@ -1952,16 +1999,28 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
         rep->trials += 1;
     }
     TuneCand best_c = cands[best_i];
-    for (int t = 0; t < (s->fused ? 4 : 1) && st == MGC_OK && s->a.deferred && !sched_wanted(s); ++t) {
-        // the best chunking once more as step groups (p = 2: pipelined) of
-        // each kernel instantiation: their best register budget can differ
-        // from the single-step kernel's (a minimum delay of 1: the one
-        // step-group form, k_steps1)
-        const int p = 1 + t / 2;
-        if (p == 2 && s->dmin < 4) break;
+    const int window0 = s->window;
+    int best_window = window0;
+    // step-group trials: p = 1, 2 of both instantiations, then the windows
+    // 2..min(4, min delay) of the windowed group (p = 3) of both
+    std::vector<std::pair<int, int>> groups;  // (mode, window)
+    if (s->fused) {
+        for (int p = 1; p <= 2; ++p)
+            if (p == 1 || s->dmin >= 4) groups.push_back({p, window0}), groups.push_back({p, window0});
+        for (int w = 2; w <= std::min(kMaxWindow, s->dmin); ++w) groups.push_back({3, w}), groups.push_back({3, w});
+    } else {
+        groups.push_back({1, window0});
+    }
+    for (size_t t = 0; t < groups.size() && st == MGC_OK && s->a.deferred && !sched_wanted(s); ++t) {
+        // the best chunking once more as step groups of each kernel
+        // instantiation: their best register budget can differ from the
+        // single-step kernel's (a minimum delay of 1: the one step-group
+        // form, k_steps1)
+        const int p = groups[t].first;
         const TuneCand c = s->fused ? TuneCand{cands[best_i].chunk_target, t % 2 == 0 ? 2 : 3} : cands[best_i];
         st = apply_cand(s, c, sms);
         s->persistent = p;
+        s->window = groups[t].second;
         if (st == MGC_OK) st = mgc_run(s, kGraphSteps);
         if (st == MGC_OK) {
             cudaEventRecord(e0, s->stream);
@@ -1976,11 +2035,14 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
                 best = per;
                 rep->persistent = p;
                 best_c = c;
+                best_window = groups[t].second;
             }
         }
         if (st == MGC_OK) st = mgc_sync(s);
     }
     s->persistent = rep->persistent;
+    s->window = best_window;
+    rep->window = s->fused ? s->window : 0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st != MGC_OK) return st;

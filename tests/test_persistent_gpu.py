@@ -98,3 +98,95 @@ def test_one_step_delay_group_equals_graphs(nu):
     with pytest.raises(mgb.MgcError):
         sim.set_persistent(2)
     sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nu", [0.002, 0.02])
+@pytest.mark.parametrize("window", [1, 2, 3, 4])
+def test_windowed_group_equals_graphs(nu, window):
+    """The windowed step group (arrivals of W steps delivered before the
+    window, then W updates with the state in registers) gives the rasters,
+    state and event count of the graph path, also when group lengths are no
+    multiple of the window and the modes are mixed."""
+    ref = make(nu)
+    ref.set_persistent(0)
+    ref.run(3001)
+    _, cr, ir = ref.read_raster()
+    vr = ref.state()["V"]
+    st = ref.state()
+    ev = ref.info()["events"]
+    ref.close()
+
+    sim = make(nu)
+    sim.set_persistent(3)
+    sim.set_window(window)
+    info = sim.info()
+    assert info["persistent"] == 3 and info["window"] == window
+    sim.run(1001)
+    sim.set_persistent(0)
+    sim.run(37)
+    sim.set_persistent(3)
+    sim.run(1)
+    sim.run(2)
+    sim.run(3)
+    sim.set_persistent(2)
+    sim.run(5)
+    sim.set_persistent(3)
+    sim.run(1952)
+    sim.sync()
+    _, c, i = sim.read_raster()
+    assert sim.info()["step"] == 3001
+    assert np.array_equal(c, cr) and np.array_equal(i, ir)
+    s2 = sim.state()
+    assert np.array_equal(s2["V"], vr)
+    for k in st:
+        assert np.array_equal(s2[k], st[k]), k
+    assert sim.info()["events"] == ev
+    assert c.sum() > 0
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_windowed_group_min_delay_two():
+    """Minimum delay 2: windows of 1 and 2 steps; 3 is refused."""
+    w = bench.workload(scale=0.03, nu=0.02)
+    projs = [(s, t, k, wt, 2, 7) for (s, t, k, wt, _, _) in w["projs"]]
+
+    def mk():
+        return mgb.Simulator.fixed_indegree(w["pops"], projs, w["lif"], rate=w["rate"], v_init=w["v0"],
+                                            conn_seed=5, seed=3)
+    ref = mk()
+    ref.set_persistent(0)
+    ref.run(1500)
+    _, cr, ir = ref.read_raster()
+    vr = ref.state()["V"]
+    ref.close()
+    for window in (1, 2):
+        sim = mk()
+        sim.set_persistent(3)
+        sim.set_window(window)
+        sim.run(777)
+        sim.run(723)
+        sim.sync()
+        _, c, i = sim.read_raster()
+        assert np.array_equal(c, cr) and np.array_equal(i, ir)
+        assert np.array_equal(sim.state()["V"], vr)
+        assert c.sum() > 0
+        with pytest.raises(mgb.MgcError):
+            sim.set_window(3)
+        with pytest.raises(mgb.MgcError):
+            sim.set_window(0)
+        sim.close()
+
+
+@pytest.mark.gpu
+def test_windowed_group_refused_for_min_delay_one():
+    w = bench.workload(scale=0.03)
+    projs = [(s, t, k, wt, 1, 5) for (s, t, k, wt, _, _) in w["projs"]]
+    sim = mgb.Simulator.fixed_indegree(w["pops"], projs, w["lif"], rate=w["rate"], v_init=w["v0"], conn_seed=4)
+    with pytest.raises(mgb.MgcError):
+        sim.set_persistent(3)
+    with pytest.raises(mgb.MgcError):
+        sim.set_window(1)
+    assert sim.info()["window"] == 0
+    sim.close()
