@@ -332,12 +332,13 @@ def run_ours(a, ws, rank, local):
         v["share"] = kms[0 if k_ == "neuron_update" else 1] / max(1e-9, sum(kms))
     steps_timed = a.steps * CHUNK
     group_mode = sim.info()["persistent"]
+    sim_window = sim.info()["window"] if group_mode == 3 else None
     if 0 < launches <= steps_timed and steps_timed % launches == 0:
         # the fused method: one kernel per step (k_fused) or one per step group
-        # (k_steps / k_pipe); each launch covers steps_timed / launches steps
-        # and its average duration is the timed region over its launches
+        # (k_steps / k_pipe / k_window); each launch covers steps_timed /
+        # launches steps and its average duration is the timed region over its launches
         per_launch = steps_timed // launches
-        dom = {0: "k_fused", 1: "k_steps", 2: "k_pipe"}[group_mode]
+        dom = {0: "k_fused", 1: "k_steps", 2: "k_pipe", 3: "k_window"}[group_mode]
         dur_us = 1e3 * ms / launches
         dbytes = per_launch * (neuron_bytes + 8.0 * events / steps_timed)
         achieved = dbytes / (dur_us * 1e-6) / 1e9
@@ -441,7 +442,8 @@ def run_ours(a, ws, rank, local):
                                    "dt 0.1 ms",
                        "scale": a.scale, "synapses": info["n_synapses"], "bench_step": "1 s simulated "
                        "(10,000 timesteps)", "l2": "inputs larger than L2 (8.8 GB CSR)",
-                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+                       "parallelism": "replicas" if ws > 1 else "single GPU",
+                       "step_group": {"mode": group_mode, "kernel": dom, "window": sim_window}},
             "sim_s_per_wall_s": sim_s_wall,
             "events_per_step": ev_all / (a.steps * CHUNK * ws),
             "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
@@ -834,9 +836,9 @@ def main():
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
     ap.add_argument("--sweep-steps", type=int, default=2048)
-    ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2],
+    ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2, 3],
                     help="with --kernel-profile or --no-autotune: 0 graphs of k_fused, 1 k_steps groups, "
-                         "2 k_pipe groups")
+                         "2 k_pipe groups, 3 k_window groups (window of 4 steps)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner and run --group-mode (for launch lists)")
     ap.add_argument("--kernel-profile", choices=["quiet", "driven"],

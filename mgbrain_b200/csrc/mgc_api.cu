@@ -706,8 +706,9 @@ mgc_status finish_build(mgc_sim* s)
         s->fused_variant = 1;
         s->fused_grid = s->fused_grid_v[1];
         // step groups by default (faster than one launch per step on every
-        // measured load); the pipelined form needs a minimum delay >= 4
-        s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 1;
+        // measured load); windows of 4 steps (the fastest measured form)
+        // need a minimum delay >= 4
+        s->persistent = s->fused ? (s->dmin >= 4 ? 3 : 1) : 1;
         if (!s->fused) {
             // minimum delay 1: a barrier-per-phase step group sized to the
             // neurons (8 warps x 64 neuron groups a block per pass)

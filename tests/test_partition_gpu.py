@@ -81,7 +81,7 @@ def fixed(w, **kw):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("cap", [None, 2048])
-@pytest.mark.parametrize("persistent", [0, 1, 2])
+@pytest.mark.parametrize("persistent", [0, 1, 2, 3])
 def test_fixed_indegree_partitions_equal_whole(persistent, cap):
     w = bench.workload(scale=0.02, nu=0.02)
     whole = fixed(w)

@@ -147,10 +147,12 @@ def test_windowed_group_equals_graphs(nu, window):
 
 
 @pytest.mark.gpu
-def test_windowed_group_min_delay_two():
-    """Minimum delay 2: windows of 1 and 2 steps; 3 is refused."""
+@pytest.mark.parametrize("dmin", [2, 5])
+def test_windowed_group_short_min_delay(dmin):
+    """Minimum delays 2 and 5: every window up to min(4, dmin) steps gives
+    the rasters and state of the graph path; a longer window is refused."""
     w = bench.workload(scale=0.03, nu=0.02)
-    projs = [(s, t, k, wt, 2, 7) for (s, t, k, wt, _, _) in w["projs"]]
+    projs = [(s, t, k, wt, dmin, dmin + 5) for (s, t, k, wt, _, _) in w["projs"]]
 
     def mk():
         return mgb.Simulator.fixed_indegree(w["pops"], projs, w["lif"], rate=w["rate"], v_init=w["v0"],
@@ -161,7 +163,7 @@ def test_windowed_group_min_delay_two():
     _, cr, ir = ref.read_raster()
     vr = ref.state()["V"]
     ref.close()
-    for window in (1, 2):
+    for window in range(1, min(4, dmin) + 1):
         sim = mk()
         sim.set_persistent(3)
         sim.set_window(window)
@@ -173,7 +175,7 @@ def test_windowed_group_min_delay_two():
         assert np.array_equal(sim.state()["V"], vr)
         assert c.sum() > 0
         with pytest.raises(mgb.MgcError):
-            sim.set_window(3)
+            sim.set_window(min(4, dmin) + 1)
         with pytest.raises(mgb.MgcError):
             sim.set_window(0)
         sim.close()
