@@ -328,8 +328,8 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * windowed step groups (minimum delay >= 2): the arrivals of a window of W
  * steps (mgc_set_window) are delivered before it, then every neuron advances
  * the W steps with its state in registers, two grid barriers per window.
- * Default: 3 (windows of 4 steps) when the minimum delay is >= 4, else 1;
- * the autotuner may pick another.  If the device cannot keep all blocks of a group resident, the
+ * Default: 2 when the minimum delay is >= 4, else 1; the autotuner may pick
+ * another.  If the device cannot keep all blocks of a group resident, the
  * call falls back to 0.  Results are the same in every mode; while a schedule mode other than
  * static, recording or calibration is on, graphs are used.  All waits are
  * bounded (a time-out makes mgc_sync return MGC_ERR_CUDA).  No reference

@@ -706,9 +706,12 @@ mgc_status finish_build(mgc_sim* s)
         s->fused_variant = 1;
         s->fused_grid = s->fused_grid_v[1];
         // step groups by default (faster than one launch per step on every
-        // measured load); windows of 4 steps (the fastest measured form)
-        // need a minimum delay >= 4
-        s->persistent = s->fused ? (s->dmin >= 4 ? 3 : 1) : 1;
+        // measured load); the pipelined form needs a minimum delay >= 4.
+        // The windowed form is faster on the measured loads, but it changes
+        // the order of the fp32 additions into one neuron's input (with
+        // unequal weights per sign the last bits of V differ from the
+        // reference's), so only the autotuner or the caller selects it
+        s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 1;
         if (!s->fused) {
             // minimum delay 1: a barrier-per-phase step group sized to the
             // neurons (8 warps x 64 neuron groups a block per pass)

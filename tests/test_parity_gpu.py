@@ -14,13 +14,15 @@ from cases import NAMES, load, ref_outputs, run_oracle
 W_RTOL = 1e-5
 
 
-def run_cuda(name, mode=mgb.MODE_AUTO):
+def run_cuda(name, mode=mgb.MODE_AUTO, persistent=None):
     c, net, v0 = load(name)
     dsteps, dmin, dmax = T.quantize_delays(net["delay"], net["step"])
     sim = mgb.Simulator.from_arrays(
         net["n"], net["type"], net["src"], net["tar"], net["weight"], dsteps,
         T.default_lifconst(net), T.default_stdpconst(net), rate=net["rate"], v_init=v0,
         stdp=bool(c["stdp"]), seed=c["seed"], mode=mode)
+    if persistent is not None:
+        sim.set_persistent(persistent)
     off = c.get("rates_off")
     if off:
         sim.run(off)
@@ -92,6 +94,38 @@ def test_cuda_matches_reference_kernels(name):
         assert np.array_equal(gst["V"].view(np.int32), rst["V"].view(np.int32))
     for k in ("fire_cnt", "last_fired", "refrac"):
         assert np.array_equal(gst[k], rst[k]), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_windowed_group_matches_reference_kernels(name):
+    """The windowed step group (mgc_set_persistent mode 3, windows of up to 4
+    steps) against the reference kernels' outputs: rasters and integer state
+    bit-exact; V bit-exact with one weight per sign, else within 1e-5
+    relative (it adds a neuron's inputs of one step in another order than the
+    pipelined group, and with unequal weights of one sign fp32 sums depend on
+    that order)."""
+    ref = ref_outputs(name)
+    if ref is None:
+        pytest.skip("no golden reference outputs for " + name)
+    c, net, _ = load(name)
+    if c["stdp"]:
+        pytest.skip("STDP networks run the pull method (no step groups)")
+    dsteps, dmin, _ = T.quantize_delays(net["delay"], net["step"])
+    if dmin < 2:
+        pytest.skip("a minimum delay of one step has one step-group form")
+    rc, ri, rst = ref
+    gc, gi, gst, gsim = run_cuda(name, persistent=3)
+    assert gsim.info()["persistent"] == 3 and gsim.info()["window"] == min(4, dmin)
+    assert np.array_equal(gc, rc)
+    assert np.array_equal(gi, ri)
+    for k in ("fire_cnt", "last_fired", "refrac"):
+        assert np.array_equal(gst[k], rst[k]), k
+    wt = net["weight"]
+    if len(np.unique(wt[wt > 0])) <= 1 and len(np.unique(wt[wt <= 0])) <= 1:
+        assert np.array_equal(gst["V"].view(np.int32), rst["V"].view(np.int32))
+    else:
+        np.testing.assert_allclose(gst["V"], rst["V"], rtol=W_RTOL, atol=1e-8)
 
 
 @pytest.mark.gpu
