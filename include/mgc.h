@@ -316,8 +316,12 @@ typedef struct mgc_tune_report {
  * cooperative launch of up to 1024 steps with a bounded grid barrier between
  * steps — starting with the builder's choice, and keeps the fastest.  The trials are
  * real steps: the simulation advances by report->steps.  The configuration
- * changes no result (it only changes which warp adds which synapse).  No
- * reference counterpart (its launch shapes are fixed, mgcore.cu:535-554). */
+ * changes which warp adds which synapse, and so the order of the fp32
+ * additions into a neuron's input: no result changes with one weight per
+ * sign; with unequal weights of one sign the last bits of V may (as between
+ * two runs of the reference's atomics).  The windowed step group
+ * (mgc_set_persistent mode 3) is among the trials.  No reference counterpart
+ * (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 
 /* How the fused method runs: 0 CUDA graphs of single-step kernels; 1
