@@ -379,10 +379,12 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             }
         }
         // compaction in neuron order: one warp scan of the per-pass counts
-        // (pass h in bits 8h.., at most 128 spikes each)
+        // (pass h in bits 8h.., at most 128 spikes each); none when no lane
+        // of the warp spiked (most passes of a quiet step)
         int c = 0;
 #pragma unroll
         for (int h = 0; h < G; ++h) c |= __popc(fmask[h]) << (8 * h);
+        if (!__any_sync(0xffffffffu, c != 0)) continue;
         int incl = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -947,7 +949,9 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                 reinterpret_cast<float4*>(acc_buf(a, a.acc_e, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
                 reinterpret_cast<float4*>(acc_buf(a, a.acc_i, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            // the step's spikes into its history slot, in neuron order within the warp
+            // the step's spikes into its history slot, in neuron order within
+            // the warp (no scan when no lane spiked)
+            if (!__any_sync(0xffffffffu, fm != 0)) continue;
             const int c = __popc(fm);
             int incl = c;
 #pragma unroll
