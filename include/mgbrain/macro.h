@@ -59,6 +59,11 @@ public:
     static int DEVICE;
     static bool THROW_ON_ERROR;
     static bool STDP_BY_TYPE;    // addition: only STDP-typed projections learn
+    // additions: NetGen's fixed-probability rule draws its candidate pairs on
+    // this many host threads (0: all hardware threads) once a projection has
+    // at least NETGEN_PARALLEL_PAIRS pairs; the network is the same
+    static int NETGEN_THREADS;
+    static long long NETGEN_PARALLEL_PAIRS;
 
     static void set_timestep(real time_step)
     {
@@ -84,6 +89,11 @@ public:
     static void set_seed(long long seed) { SEED = seed; }
     static void set_netgen_seed(long long seed) { NETGEN_SEED = seed; }
     static void set_device(int device) { DEVICE = device; }
+    static void set_netgen_threads(int threads, long long min_pairs = 1LL << 24)
+    {
+        NETGEN_THREADS = threads;
+        NETGEN_PARALLEL_PAIRS = min_pairs;
+    }
     static void throw_on_error(bool on) { THROW_ON_ERROR = on; }
     // With STDP on, the reference updates every synapse (mgcore.cu:365-412)
     // whatever its projection's SynapseType; this restricts it to STDP ones.

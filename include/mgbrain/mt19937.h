@@ -1,0 +1,70 @@
+// MGBrain C++ API addition: the 32-bit Mersenne Twister NetGen draws from
+// (the reference seeds a std::mt19937 in src/model/netgen.cpp:47), with its
+// state open and a jump-ahead, so that one stretch of its output can be cut
+// into pieces that threads generate at once and the result is the stream's.
+//
+// Mt19937 is MT19937 as published by Matsumoto and Nishimura (1998) and as
+// the C++ standard defines std::mt19937: the same seed gives the same
+// outputs.  It advances one word per output (the 624-word block twist
+// computed word by word), so one output is one step of the linear map T on
+// the state.
+//
+// Jump-ahead (Haramoto, Matsumoto, Nishimura, Panneton and L'Ecuyer, 2008,
+// "Efficient jump ahead for F2-linear random number generators"): the
+// characteristic polynomial phi of T, of degree 19937, is found once with the
+// Berlekamp-Massey algorithm from 2 x 19937 output bits; advancing J outputs
+// is T^J = sum a_i T^i where x^J mod phi = sum a_i x^i, evaluated on the state
+// by Horner's rule (19937 steps of T).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace MGBrain {
+
+class Mt19937 {
+public:
+    static constexpr int N = 624;
+    explicit Mt19937(uint32_t seed = 5489u) { seed_with(seed); }
+    void seed_with(uint32_t seed);
+    uint32_t operator()()
+    {
+        step();
+        return temper(x_[i_ == 0 ? N - 1 : i_ - 1]);
+    }
+    void discard(uint64_t n)
+    {
+        for (uint64_t k = 0; k < n; ++k) step();
+    }
+    // One step of T: the word at the ring position is replaced by the next.
+    void step();
+    // this ^= o, word by word in logical order (linear combination of states)
+    void add(const Mt19937& o);
+    void clear();
+
+private:
+    static uint32_t temper(uint32_t y)
+    {
+        y ^= y >> 11;
+        y ^= (y << 7) & 0x9d2c5680u;
+        y ^= (y << 15) & 0xefc60000u;
+        return y ^ (y >> 18);
+    }
+    uint32_t x_[N];
+    int i_ = 0;  // ring position of the oldest word (the next to be replaced)
+};
+
+// x^J mod phi as a bit vector (bit i: coefficient of x^i), 19937 bits.
+class MtJump {
+public:
+    explicit MtJump(uint64_t steps);
+    uint64_t steps() const { return steps_; }
+    // g advanced by steps() outputs
+    void apply(Mt19937& g) const;
+
+private:
+    uint64_t steps_;
+    std::vector<uint64_t> poly_;
+};
+
+}  // namespace MGBrain

@@ -1,8 +1,11 @@
 // MGBrain C++ API: Config storage, Model, NetGen.
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
+#include <thread>
 
 #include "mgbrain/constgen.h"
+#include "mgbrain/mt19937.h"
 #include "mgbrain/netgen.h"
 
 #ifndef __CUDACC__  // the core's Philox header, here compiled for the host only
@@ -32,6 +35,8 @@ long long Config::NETGEN_SEED = -1;
 int Config::DEVICE = 0;
 bool Config::THROW_ON_ERROR = false;
 bool Config::STDP_BY_TYPE = false;
+int Config::NETGEN_THREADS = 0;
+long long Config::NETGEN_PARALLEL_PAIRS = 1LL << 24;
 
 Model::Model() { indexer = 0; }
 
@@ -143,6 +148,60 @@ real NetGen::rand_delay(real floor, real ceil)
 
 namespace {
 
+// The fixed-probability rule's candidate pairs (netgen.cpp): pair k of the
+// row-major order is taken, while fewer than gen_num are taken, when the
+// k-th draw of rng satisfies draw % max_num < limit.  Returns the taken
+// pairs (the first gen_num in order) and leaves rng after the draws the rule
+// consumed (one per pair until the gen_num-th is taken).  With more than one
+// thread the pairs are cut into equal stretches, each thread starts from the
+// generator jumped ahead to its stretch (MtJump) and takes its pairs as if
+// none had been taken before; the stretches' pairs are then joined in order
+// and cut at gen_num, which is the sequential result.
+std::vector<size_t> draw_pairs(Mt19937& rng, size_t max_num, size_t gen_num, double limit)
+{
+    std::vector<size_t> picked;
+    picked.reserve(gen_num);
+    unsigned threads = Config::NETGEN_THREADS > 0 ? (unsigned)Config::NETGEN_THREADS
+                                                  : std::max(1u, std::thread::hardware_concurrency());
+    if (threads <= 1 || gen_num == 0 || max_num == 0 || (long long)max_num < Config::NETGEN_PARALLEL_PAIRS) {
+        for (size_t k = 0; k < max_num && picked.size() < gen_num; ++k)
+            if ((double)(rng() % max_num) < limit) picked.push_back(k);
+        return picked;
+    }
+    const size_t T = std::min<size_t>(threads, max_num);
+    const size_t C = (max_num + T - 1) / T;
+    std::vector<Mt19937> start(T, rng);
+    const MtJump jump(C);
+    for (size_t k = 1; k < T; ++k) {
+        start[k] = start[k - 1];
+        jump.apply(start[k]);
+    }
+    std::vector<std::vector<size_t>> local(T);
+    std::vector<std::thread> pool;
+    for (size_t k = 0; k < T; ++k)
+        pool.emplace_back([&, k] {
+            Mt19937 g = start[k];
+            const size_t lo = k * C, hi = std::min(max_num, lo + C);
+            std::vector<size_t>& out = local[k];
+            for (size_t idx = lo; idx < hi && out.size() < gen_num; ++idx)
+                if ((double)(g() % max_num) < limit) out.push_back(idx);
+        });
+    for (auto& th : pool) th.join();
+    size_t consumed = max_num;  // draws the sequential rule makes
+    for (size_t k = 0; k < T && picked.size() < gen_num; ++k)
+        for (size_t idx : local[k]) {
+            picked.push_back(idx);
+            if (picked.size() == gen_num) {
+                consumed = idx + 1;
+                break;
+            }
+        }
+    const size_t kc = (consumed - 1) / C;  // the stretch of the last draw consumed
+    rng = start[kc];
+    rng.discard(consumed - kc * C);
+    return picked;
+}
+
 void add_synapse(Network& net, int src, int tar, real w, real d, SynapseType stype)
 {
     net.synapses.emplace_back(src, tar, w, d);
@@ -159,7 +218,7 @@ void NetGen::gen_net(Network& net, Model& model)
     const unsigned long seed = Config::NETGEN_SEED >= 0
                                    ? (unsigned long)Config::NETGEN_SEED
                                    : (unsigned long)std::chrono::system_clock::now().time_since_epoch().count();
-    std::mt19937 rng(seed);
+    Mt19937 rng((uint32_t)seed);  // std::mt19937's outputs for the same seed
     net.nlifconst = model.nlifconst;
     net.nstdpconst = model.nstdpconst;
     net.lifconst = model.lifconst;
@@ -256,11 +315,8 @@ void NetGen::gen_net(Network& net, Model& model)
                 const size_t max_num = (size_t)sn * (size_t)tn;
                 const size_t gen_num = static_cast<size_t>(std::round(max_num * pr.ctype));
                 const double limit = gen_num * 1.1;
-                std::vector<size_t> picked(gen_num, 0);
-                size_t count = 0;
-                for (size_t m = 0; m < (size_t)sn; ++m)
-                    for (size_t n = 0; n < (size_t)tn; ++n)
-                        if (count < gen_num && (double)(rng() % max_num) < limit) picked[count++] = m * tn + n;
+                std::vector<size_t> picked = draw_pairs(rng, max_num, gen_num, limit);
+                picked.resize(gen_num, 0);
                 net.synapses.reserve(net.synapses.size() + gen_num);
                 for (size_t t = 0; t < gen_num; ++t) {
                     const int m = (int)(picked[t] / tn);
