@@ -32,12 +32,18 @@ public:
         step();
         return temper(x_[i_ == 0 ? N - 1 : i_ - 1]);
     }
-    void discard(uint64_t n)
-    {
-        for (uint64_t k = 0; k < n; ++k) step();
-    }
+    // the next n outputs (the same as n calls), whole blocks of 624 at once
+    void generate(uint32_t* out, size_t n);
+    void discard(uint64_t n);
     // One step of T: the word at the ring position is replaced by the next.
-    void step();
+    void step()
+    {
+        const int i1 = i_ + 1 == N ? 0 : i_ + 1;
+        const int im = i_ + 397 >= N ? i_ + 397 - N : i_ + 397;
+        const uint32_t y = (x_[i_] & 0x80000000u) | (x_[i1] & 0x7fffffffu);
+        x_[i_] = x_[im] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+        i_ = i1;
+    }
     // this ^= o, word by word in logical order (linear combination of states)
     void add(const Mt19937& o);
     void clear();
@@ -50,6 +56,7 @@ private:
         y ^= (y << 15) & 0xefc60000u;
         return y ^ (y >> 18);
     }
+    void twist_block();  // 624 steps from ring position 0, in three loops
     uint32_t x_[N];
     int i_ = 0;  // ring position of the oldest word (the next to be replaced)
 };

@@ -148,6 +148,53 @@ real NetGen::rand_delay(real floor, real ceil)
 
 namespace {
 
+// draw % max_num for 32-bit draws: the draw itself when max_num exceeds
+// every draw, else Lemire's remainder by multiplication ("Faster remainder by
+// direct computation", 2019), exact for 32-bit operands.
+struct DrawMod {
+    explicit DrawMod(size_t max_num)
+        : big(max_num > 0xffffffffull), d((uint32_t)max_num), M(big ? 0 : UINT64_MAX / (uint32_t)max_num + 1)
+    {
+    }
+    uint64_t operator()(uint32_t a) const
+    {
+        if (big) return a;
+        const uint64_t low = M * a;
+        return (uint64_t)(((unsigned __int128)low * d) >> 64);
+    }
+    bool big;
+    uint32_t d;
+    uint64_t M;
+};
+
+// Pairs [lo, hi) of the fixed-probability rule, drawing from g: pair k is
+// taken when its draw % max_num < limit, until out holds cap pairs.  Leaves g
+// after the draws consumed (one per pair up to the cap-th taken).  Draws come
+// in blocks; the block that reaches the cap is redrawn from its start up to
+// the last pair it took.
+void scan_pairs(Mt19937& g, size_t lo, size_t hi, size_t max_num, double limit, size_t cap,
+                std::vector<size_t>& out)
+{
+    constexpr size_t kBlock = 4096;
+    uint32_t buf[kBlock];
+    const DrawMod mod(max_num);
+    for (size_t k = lo; k < hi && out.size() < cap;) {
+        const size_t n = std::min(kBlock, hi - k);
+        const Mt19937 at_start = g;
+        g.generate(buf, n);
+        for (size_t j = 0; j < n; ++j)
+            if ((double)mod(buf[j]) < limit) {
+                out.push_back(k + j);
+                if (out.size() == cap) {
+                    g = at_start;
+                    g.discard(j + 1);
+                    return;
+                }
+            }
+        k += n;
+    }
+}
+
 // The fixed-probability rule's candidate pairs (netgen.cpp): pair k of the
 // row-major order is taken, while fewer than gen_num are taken, when the
 // k-th draw of rng satisfies draw % max_num < limit.  Returns the taken
@@ -164,8 +211,7 @@ std::vector<size_t> draw_pairs(Mt19937& rng, size_t max_num, size_t gen_num, dou
     unsigned threads = Config::NETGEN_THREADS > 0 ? (unsigned)Config::NETGEN_THREADS
                                                   : std::max(1u, std::thread::hardware_concurrency());
     if (threads <= 1 || gen_num == 0 || max_num == 0 || (long long)max_num < Config::NETGEN_PARALLEL_PAIRS) {
-        for (size_t k = 0; k < max_num && picked.size() < gen_num; ++k)
-            if ((double)(rng() % max_num) < limit) picked.push_back(k);
+        scan_pairs(rng, 0, max_num, max_num, limit, gen_num, picked);
         return picked;
     }
     const size_t T = std::min<size_t>(threads, max_num);
@@ -182,9 +228,7 @@ std::vector<size_t> draw_pairs(Mt19937& rng, size_t max_num, size_t gen_num, dou
         pool.emplace_back([&, k] {
             Mt19937 g = start[k];
             const size_t lo = k * C, hi = std::min(max_num, lo + C);
-            std::vector<size_t>& out = local[k];
-            for (size_t idx = lo; idx < hi && out.size() < gen_num; ++idx)
-                if ((double)(g() % max_num) < limit) out.push_back(idx);
+            if (lo < hi) scan_pairs(g, lo, hi, max_num, limit, gen_num, local[k]);
         });
     for (auto& th : pool) th.join();
     size_t consumed = max_num;  // draws the sequential rule makes
@@ -318,6 +362,23 @@ void NetGen::gen_net(Network& net, Model& model)
                 std::vector<size_t> picked = draw_pairs(rng, max_num, gen_num, limit);
                 picked.resize(gen_num, 0);
                 net.synapses.reserve(net.synapses.size() + gen_num);
+                net.plastic.reserve(net.plastic.size() + gen_num);
+                {  // the per-neuron lists grow once each instead of by doubling
+                    std::vector<uint32_t> out_n(sn, 0), in_n(tn, 0);
+                    for (size_t t = 0; t < gen_num; ++t) {
+                        ++out_n[picked[t] / tn];
+                        ++in_n[picked[t] % tn];
+                    }
+                    for (int m = 0; m < sn; ++m) {
+                        Neuron& nm = net.neurons[sp.neurons[m]];
+                        nm.nxt.reserve(nm.nxt.size() + out_n[m]);
+                        nm.syns.reserve(nm.syns.size() + out_n[m]);
+                    }
+                    for (int n = 0; n < tn; ++n) {
+                        Neuron& nn = net.neurons[tp.neurons[n]];
+                        nn.pre.reserve(nn.pre.size() + in_n[n]);
+                    }
+                }
                 for (size_t t = 0; t < gen_num; ++t) {
                     const int m = (int)(picked[t] / tn);
                     const int n = (int)(picked[t] % tn);

@@ -161,13 +161,35 @@ void Mt19937::seed_with(uint32_t seed)
     i_ = 0;
 }
 
-void Mt19937::step()
+void Mt19937::twist_block()
 {
-    const int i1 = i_ + 1 == N ? 0 : i_ + 1;
-    const int im = i_ + kM >= N ? i_ + kM - N : i_ + kM;
-    const uint32_t y = (x_[i_] & kUpper) | (x_[i1] & kLower);
-    x_[i_] = x_[im] ^ (y >> 1) ^ ((y & 1u) ? kMatrixA : 0u);
-    i_ = i1;
+    auto next = [](uint32_t a, uint32_t b, uint32_t c) {
+        const uint32_t y = (a & kUpper) | (b & kLower);
+        return c ^ (y >> 1) ^ ((y & 1u) ? kMatrixA : 0u);
+    };
+    int j = 0;
+    for (; j < N - kM; ++j) x_[j] = next(x_[j], x_[j + 1], x_[j + kM]);
+    for (; j < N - 1; ++j) x_[j] = next(x_[j], x_[j + 1], x_[j + kM - N]);
+    x_[N - 1] = next(x_[N - 1], x_[0], x_[kM - 1]);
+}
+
+void Mt19937::generate(uint32_t* out, size_t n)
+{
+    size_t k = 0;
+    for (; k < n && i_ != 0; ++k) out[k] = (*this)();
+    for (; n - k >= (size_t)N; k += N) {
+        twist_block();
+        for (int j = 0; j < N; ++j) out[k + j] = temper(x_[j]);
+    }
+    for (; k < n; ++k) out[k] = (*this)();
+}
+
+void Mt19937::discard(uint64_t n)
+{
+    uint64_t k = 0;
+    for (; k < n && i_ != 0; ++k) step();
+    for (; n - k >= (uint64_t)N; k += N) twist_block();
+    for (; k < n; ++k) step();
 }
 
 void Mt19937::add(const Mt19937& o)
