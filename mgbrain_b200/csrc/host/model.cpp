@@ -255,6 +255,60 @@ void add_synapse(Network& net, int src, int tar, real w, real d, SynapseType sty
     net.plastic.push_back(stype == SynapseType::STDP ? 1 : 0);
 }
 
+// add_synapse for the pairs (m, n) = (picked[t] / tn, picked[t] % tn) of
+// populations sp -> tp, in order: the synapses and their weight and delay
+// draws (glibc rand(), in the reference's order) one after the other; then
+// the per-neuron lists, each reserved once, filled by threads that own the
+// neurons by id, each neuron's entries in synapse order.  The same Network
+// as calling add_synapse pair by pair.
+void add_pairs(Network& net, const Pop& sp, const Pop& tp, const std::vector<size_t>& picked, real w0, real w1,
+               real d0, real d1, SynapseType stype)
+{
+    const size_t G = picked.size(), base = net.synapses.size();
+    const size_t tn = (size_t)tp.num;
+    net.synapses.reserve(base + G);
+    net.plastic.reserve(net.plastic.size() + G);
+    for (size_t t = 0; t < G; ++t) {
+        const real w = NetGen::rand_weight(w0, w1);
+        const real d = NetGen::rand_delay(d0, d1);
+        net.synapses.emplace_back(sp.neurons[picked[t] / tn], tp.neurons[picked[t] % tn], w, d);
+        net.plastic.push_back(stype == SynapseType::STDP ? 1 : 0);
+    }
+    std::vector<uint32_t> out_n(net.neurons.size(), 0), in_n(net.neurons.size(), 0);
+    for (size_t t = 0; t < G; ++t) {
+        ++out_n[net.synapses[base + t].src];
+        ++in_n[net.synapses[base + t].tar];
+    }
+    for (size_t i = 0; i < net.neurons.size(); ++i) {
+        Neuron& nr = net.neurons[i];
+        if (out_n[i]) {
+            nr.nxt.reserve(nr.nxt.size() + out_n[i]);
+            nr.syns.reserve(nr.syns.size() + out_n[i]);
+        }
+        if (in_n[i]) nr.pre.reserve(nr.pre.size() + in_n[i]);
+    }
+    unsigned T = Config::NETGEN_THREADS > 0 ? (unsigned)Config::NETGEN_THREADS
+                                            : std::max(1u, std::thread::hardware_concurrency());
+    if ((long long)G < Config::NETGEN_PARALLEL_PAIRS / 16) T = 1;
+    auto fill = [&](unsigned part) {
+        for (size_t t = 0; t < G; ++t) {
+            const Synapse& s = net.synapses[base + t];
+            if ((unsigned)s.src % T == part) {
+                net.neurons[s.src].nxt.push_back(s.tar);
+                net.neurons[s.src].syns.push_back(base + t + 1);
+            }
+            if ((unsigned)s.tar % T == part) net.neurons[s.tar].pre.push_back(s.src);
+        }
+    };
+    if (T == 1) {
+        fill(0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (unsigned p = 0; p < T; ++p) pool.emplace_back(fill, p);
+    for (auto& th : pool) th.join();
+}
+
 }  // namespace
 
 void NetGen::gen_net(Network& net, Model& model)
@@ -361,31 +415,7 @@ void NetGen::gen_net(Network& net, Model& model)
                 const double limit = gen_num * 1.1;
                 std::vector<size_t> picked = draw_pairs(rng, max_num, gen_num, limit);
                 picked.resize(gen_num, 0);
-                net.synapses.reserve(net.synapses.size() + gen_num);
-                net.plastic.reserve(net.plastic.size() + gen_num);
-                {  // the per-neuron lists grow once each instead of by doubling
-                    std::vector<uint32_t> out_n(sn, 0), in_n(tn, 0);
-                    for (size_t t = 0; t < gen_num; ++t) {
-                        ++out_n[picked[t] / tn];
-                        ++in_n[picked[t] % tn];
-                    }
-                    for (int m = 0; m < sn; ++m) {
-                        Neuron& nm = net.neurons[sp.neurons[m]];
-                        nm.nxt.reserve(nm.nxt.size() + out_n[m]);
-                        nm.syns.reserve(nm.syns.size() + out_n[m]);
-                    }
-                    for (int n = 0; n < tn; ++n) {
-                        Neuron& nn = net.neurons[tp.neurons[n]];
-                        nn.pre.reserve(nn.pre.size() + in_n[n]);
-                    }
-                }
-                for (size_t t = 0; t < gen_num; ++t) {
-                    const int m = (int)(picked[t] / tn);
-                    const int n = (int)(picked[t] % tn);
-                    const real w = rand_weight(w0, w1);
-                    const real d = rand_delay(d0, d1);
-                    add_synapse(net, sp.neurons[m], tp.neurons[n], w, d, pr.stype);
-                }
+                add_pairs(net, sp, tp, picked, w0, w1, d0, d1, pr.stype);
             }
         }
     }
