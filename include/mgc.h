@@ -455,7 +455,8 @@ mgc_status mgc_measure_scatter(int32_t device, int64_t n_events, int32_t n_targe
  * mgc_create builds and mgc_export_csr returns for the same list.  src
  * (n_synapses int32) and row_ptr (n_neurons+1 int64) are device pointers on
  * the current device; the work is enqueued on `stream` (a cudaStream_t, NULL
- * for the legacy default stream) and the call waits for it before returning.
+ * for the legacy default stream), and every call waits for that stream before
+ * it returns (it reads back a count of out-of-range sources).
  *
  * For callers that cannot allocate device memory at this point: a caller whose
  * memory pool owns the device (cudaMalloc can fail there although the pool
@@ -467,9 +468,11 @@ mgc_status mgc_measure_scatter(int32_t device, int64_t n_events, int32_t n_targe
  * initial contents (the call zeroes it and its own counters).  The first call
  * on a device does a one-time set-up (it looks up the scratch array's address,
  * cudaGetSymbolAddress), so make that first call before any stream capture
- * begins.  All calls on one device share the one scratch array, so calls that
- * overlapped would race on it; the library serialises them with a lock per
- * device.  Sources outside [0, n_neurons) are skipped and reported as
+ * begins.  All calls on one device share the one scratch array, which keeps
+ * the last call's contents, so calls that overlapped on the GPU would race on
+ * it; the library serialises them with a lock per device, held until the
+ * call's work on the stream has finished, on success and on failure alike.
+ * Sources outside [0, n_neurons) are skipped and reported as
  * MGC_ERR_INVALID.  No reference counterpart (the reference computes its row
  * offsets, axon_offs, on the host: src/simulator/mgsim/adj/mgsim.cpp:115-122). */
 mgc_status mgc_row_offsets_static(const int32_t* src, int64_t n_synapses, int32_t n_neurons, int64_t* row_ptr,

@@ -2946,17 +2946,28 @@ extern "C" mgc_status mgc_row_offsets_static(const int32_t* src, int64_t n_synap
     const int64_t tiles = (count + kRoTile - 1) / kRoTile;
     unsigned long long* cnt = reinterpret_cast<unsigned long long*>(row_ptr);
     unsigned long long* bad = scratch + kRoMaxTiles;
-    // must start at zero: the row counts (kept in row_ptr) and the bad-source count
-    CK(cudaMemsetAsync(cnt, 0, sizeof(int64_t) * count, st));
-    CK(cudaMemsetAsync(bad, 0, sizeof(unsigned long long), st));
-    if (n_synapses) k_ro_count<<<grid_for(n_synapses), 256, 0, st>>>(src, n_synapses, n_neurons, cnt, bad);
-    k_ro_tile_sums<<<(unsigned)tiles, kRoThreads, 0, st>>>(cnt, count, scratch);
-    k_ro_scan_tiles<<<1, 1024, 0, st>>>(scratch, tiles);
-    k_ro_apply<<<(unsigned)tiles, kRoThreads, 0, st>>>(cnt, count, scratch);
-    CK(cudaGetLastError());
     unsigned long long nbad = 0;
-    CK(cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    // Once the first operation is enqueued, every exit waits for the stream
+    // (whatever that wait returns) before the lock is released, so that no
+    // work of this call can still write the shared scratch array when the
+    // next call on this device starts.
+    const mgc_status rc = [&]() -> mgc_status {
+        // must start at zero: the row counts (kept in row_ptr) and the bad-source count
+        CK(cudaMemsetAsync(cnt, 0, sizeof(int64_t) * count, st));
+        CK(cudaMemsetAsync(bad, 0, sizeof(unsigned long long), st));
+        if (n_synapses) k_ro_count<<<grid_for(n_synapses), 256, 0, st>>>(src, n_synapses, n_neurons, cnt, bad);
+        k_ro_tile_sums<<<(unsigned)tiles, kRoThreads, 0, st>>>(cnt, count, scratch);
+        k_ro_scan_tiles<<<1, 1024, 0, st>>>(scratch, tiles);
+        k_ro_apply<<<(unsigned)tiles, kRoThreads, 0, st>>>(cnt, count, scratch);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return MGC_OK;
+    }();
+    if (rc != MGC_OK) {
+        cudaStreamSynchronize(st);
+        return rc;
+    }
     if (nbad)
         return fail(MGC_ERR_INVALID, "mgc_row_offsets_static: %llu synapse sources outside [0, %d)", nbad,
                     n_neurons);

@@ -94,6 +94,19 @@ int main(int argc, char** argv)
             return 1;
         }
     }
+    // the per-neuron lists, filled by threads that own neurons by id, in
+    // the order add_synapse would have appended them
+    if (a.neurons.size() != b.neurons.size()) {
+        printf("neuron counts differ: %zu vs %zu\n", a.neurons.size(), b.neurons.size());
+        return 1;
+    }
+    for (size_t i = 0; i < a.neurons.size(); ++i) {
+        const auto &x = a.neurons[i], &y = b.neurons[i];
+        if (x.nxt != y.nxt || x.pre != y.pre || x.syns != y.syns) {
+            printf("neuron %zu: nxt/pre/syns lists differ\n", i);
+            return 1;
+        }
+    }
     printf("ok %zu\n", a.synapses.size());
     return 0;
 }

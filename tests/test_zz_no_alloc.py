@@ -51,6 +51,36 @@ def test_static_row_offsets_equal_create(n, S):
 
 
 @pytest.mark.gpu
+def test_static_row_offsets_allocate_nothing():
+    """The library's allocation-failure injector is armed for the very next
+    device allocation; two static calls still succeed, and the injected
+    failure is still pending afterwards (the next builder meets it), so
+    neither call allocated through the library."""
+    import torch
+    n, S = 50_000, 400_000
+    src, _, _, _ = network(n, S, seed=3)
+    src_d = torch.from_numpy(src).cuda()
+    out_d = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    expect = np.concatenate([[0], np.cumsum(np.bincount(src, minlength=n))]).astype(np.int64)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    mgb.capi.fault_inject_alloc(1)
+    try:
+        for _ in range(2):
+            assert row_offsets_static(src_d, n, out_d, stream) == capi.MGC_OK, capi.lib().mgc_last_error()
+            assert np.array_equal(out_d.cpu().numpy(), expect)
+        assert torch.cuda.mem_get_info()[0] >= free0 - (2 << 20)
+        with pytest.raises(capi.MgcError) as e:   # the pending failure: this builder's first allocation
+            mgb.Simulator.from_arrays(4, np.full(4, mgb.LIF0, np.int8), np.zeros(1, np.int32),
+                                      np.ones(1, np.int32), np.ones(1, np.float32), np.ones(1, np.int32),
+                                      brunel.brunel_lifconst())
+        assert e.value.status == capi.MGC_ERR_NOMEM
+    finally:
+        mgb.capi.fault_inject_alloc(0)
+
+
+@pytest.mark.gpu
 def test_static_row_offsets_reject_bad_input():
     import torch
     out_d = torch.zeros(8, dtype=torch.int64, device="cuda")
