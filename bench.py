@@ -208,15 +208,57 @@ def oracle_rate(L, h, steps):
 
 
 def cpu_baseline(w, sample_steps):
+    """The oracle on one thread over the first `sample_steps` steps of the
+    network: its events/s, and its raster and V after those steps (kept for
+    the parity check of the GPU run)."""
+    import ctypes as C
     L, h, T = oracle_sim(w, os.cpu_count() or 1)
+    cap = 1 << 24
+    counts = np.zeros(sample_steps, np.int64)
+    ids = np.zeros(cap, np.int32)
+    v = np.zeros(w["n"], np.float32)
+    fc = np.zeros(w["n"], np.int32)
     try:
         L.mgbo_set_threads(h, 1)
-        v, dt = oracle_rate(L, h, sample_steps)
+        e0 = L.mgbo_events(h)
+        nid = C.c_int64()
+        t0 = time.perf_counter()
+        rc = L.mgbo_run(h, sample_steps, T._p(counts), T._p(ids), cap, C.byref(nid))
+        dt = time.perf_counter() - t0
+        ev = L.mgbo_events(h) - e0
+        L.mgbo_read_state_f32(h, T._p(v), None)
+        L.mgbo_read_state(h, None, None, None, None, None, T._p(fc), None)
     finally:
         L.mgbo_destroy(h)
-    return {"value": v, "unit": "events/s", "cores": 1, "kind": "port",
+    base = {"value": ev / dt, "unit": "events/s", "cores": 1, "kind": "port",
             "sample": f"oracle (C restatement of the reference kernels), 1 thread, first "
                       f"{sample_steps} timesteps of the same network ({dt:.1f} s)"}
+    ref = dict(counts=counts, ids=ids[:nid.value] if rc == 0 else None, v=v, fire_cnt=fc)
+    return base, ref
+
+
+def parity_check(w, local, ref, steps, group_mode, window):
+    """The GPU's first `steps` steps of the bench network, run from the same
+    seeds in the step-group form the timed run used, against the oracle's."""
+    sim = make_sim(w, local, seed=1, record=True)
+    try:
+        sim.set_persistent(group_mode)
+        if group_mode == 3 and window:
+            sim.set_window(window)
+        sim.run(steps)
+        sim.sync()
+        _, counts, ids = sim.read_raster(max_steps=steps + 1, max_ids=1 << 24)
+        st = sim.state()
+    finally:
+        sim.close()
+    v_o = ref["v"]
+    raster_equal = ref["ids"] is not None and np.array_equal(counts, ref["counts"]) and np.array_equal(ids, ref["ids"])
+    rel = np.abs(st["V"].astype(np.float64) - v_o) / np.maximum(np.abs(v_o.astype(np.float64)), 1e-30)
+    return {"steps": steps, "spikes": int(counts.sum()), "raster_equal": bool(raster_equal),
+            "v_bit_equal": bool(np.array_equal(st["V"].view(np.int32), v_o.view(np.int32))),
+            "v_max_rel": float(rel.max()), "fire_cnt_equal": bool(np.array_equal(st["fire_cnt"], ref["fire_cnt"])),
+            "step_group": {"mode": group_mode, "window": window},
+            "against": "oracle fp32 (C restatement of the reference kernels), same network and seeds"}
 
 
 def run_reference(a, ws, rank):
@@ -424,13 +466,15 @@ def run_ours(a, ws, rank, local):
                   "whole_step_frac_of_reduction_ceiling": dev / (dms / 1e3) / ws / red_ceiling}
         simd.close()
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and not a.no_cpu:
         try:
-            cpu = cpu_baseline(w, a.cpu_sample)
+            cpu, ref = cpu_baseline(w, a.cpu_sample)
         except Exception as e:  # the host may lack the memory for the full network
-            cpu = {"value": None, "unit": "events/s", "cores": 1, "kind": "port",
-                   "sample": f"not run: {e}"}
+            cpu, ref = {"value": None, "unit": "events/s", "cores": 1, "kind": "port",
+                        "sample": f"not run: {e}"}, None
+        if ref is not None:
+            parity = parity_check(w, local, ref, a.cpu_sample, group_mode, sim_window)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": ws,
@@ -447,7 +491,7 @@ def run_ours(a, ws, rank, local):
             "sim_s_per_wall_s": sim_s_wall,
             "events_per_step": ev_all / (a.steps * CHUNK * ws),
             "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
-            "clocks": clk.summary(), "gpu_launches": int(launches),
+            "clocks": clk.summary(), "gpu_launches": int(launches), "parity": parity,
             "build_s": build_s, "autotune": tune, "driven_variant": driven,
             "delivery_ceiling": {"reductions_per_s": red_ceiling, "stream_read_gbs": read_ceiling / 1e9,
                                  "how": "mgc_measure_scatter: 1e8 random fp32 red.add into 2^20 "

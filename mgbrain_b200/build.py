@@ -5,6 +5,7 @@ from __future__ import annotations
 import glob
 import os
 import subprocess
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -45,17 +46,21 @@ def build(verbose=False, checked=False):
     os.makedirs(obj_dir, exist_ok=True)
     headers = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
                + glob.glob(os.path.join(ROOT, "include", "**", "*.h"), recursive=True))
-    objs = []
+    jobs, objs = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         if _stale(obj, [src] + headers):
-            _run([NVCC] + NVFLAGS + (["-DMGC_CHECKED"] if checked else []) + ["-c", src, "-o", obj])
+            jobs.append([NVCC] + NVFLAGS + (["-DMGC_CHECKED"] if checked else []) + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in sorted(glob.glob(os.path.join(CSRC, "host", "*.cpp"))):
         obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
         if _stale(obj, [src] + headers):
-            _run([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
+            jobs.append([CXX] + CXXFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
+    # translation units compile in parallel (the step-kernel instantiations
+    # are the long ones)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        list(pool.map(_run, jobs))
     if _stale(lib, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"])
     if verbose:

@@ -341,3 +341,41 @@ def ref_gen(spec_text, mt_seed, rand_seed, out_path):
     subprocess.run([REF_GEN, "gen", spec_path, out_path], check=True, env=env,
                    capture_output=True)
     return read_netfile(out_path)
+
+
+def ref_steps(net, v0, seed, steps, workdir, stdp=0, rates_off=None):
+    """The reference kernels (oracle/_ref/ref_sim, its own sm_100a build) run
+    for exactly `steps` steps on `net` (written as a network file), POISSON
+    draws keyed by `seed`; from step rates_off on every POISSON rate is 0.
+    Returns (counts, ids, state), or None when the reference build is absent."""
+    if not os.path.exists(REF_SIM):
+        return None
+    netp = os.path.join(workdir, "net.mgbnet")
+    write_netfile(netp, net)
+    v0p = "-"
+    if v0 is not None:
+        v0p = os.path.join(workdir, "v0.f32")
+        np.ascontiguousarray(v0, np.float32).tofile(v0p)
+    out = os.path.join(workdir, "ref")
+    args = [REF_SIM, "steps", netp, out, str(int(steps)), v0p, str(int(stdp))]
+    if rates_off is not None:
+        args.append(str(int(rates_off)))
+    env = dict(os.environ, MGB_REF_SEED=str(int(seed)))
+    subprocess.run(args, check=True, env=env, capture_output=True)
+    counts, ids = read_raster(out + ".raster")
+    return counts, ids, read_state(out + ".state", int(net["n"]), len(net["src"]))
+
+
+def rate_and_cv(counts, ids, n, steps, dt):
+    """Mean rate (Hz) over all n neurons, and the mean CV of the inter-spike
+    intervals over the neurons with at least three spikes (and how many)."""
+    step_of = np.repeat(np.arange(len(counts)), counts)
+    order = np.lexsort((step_of, ids))
+    sid, sst = ids[order], step_of[order]
+    cvs = []
+    bounds = np.flatnonzero(np.diff(sid)) + 1
+    for a, b in zip(np.r_[0, bounds], np.r_[bounds, len(sid)]):
+        if b - a >= 3:
+            isi = np.diff(sst[a:b]).astype(np.float64)
+            cvs.append(isi.std() / isi.mean())
+    return len(ids) / (n * steps * dt), (float(np.mean(cvs)) if cvs else 0.0), len(cvs)

@@ -59,3 +59,23 @@ def test_rand_weight_subtracts_for_nonnegative_floor():
                         "conn 0 1 0.2 0.5 0.001 0.001 1 STATIC\n")
     net = T.oracle_netgen(spec, 1, 3)
     assert net["weight"].max() <= np.float32(0.2) and net["weight"].min() < 0.0
+
+
+@pytest.mark.parametrize("cfg", ["C0", "C1"])
+def test_netgen_matches_reference_at_config_size(cfg, tmp_path):
+    """The benchmark configurations at their stated sizes (C0: 1.1e7
+    synapses; C1: 3.2e5): the oracle's gen_net against the reference's own
+    (oracle/_ref/ref_gen), synapse for synapse."""
+    import os
+
+    import configs
+    if not os.path.exists(T.REF_GEN):
+        pytest.skip("the reference build (oracle/_ref) is absent")
+    c = getattr(configs, cfg)
+    ref = T.ref_gen(c["spec"], c["mt"], c["rnd"], str(tmp_path / "ref.net"))
+    net = T.oracle_netgen(T.parse_spec(c["spec"]), c["mt"], c["rnd"])
+    assert net["n"] == ref["n"] and len(net["src"]) == len(ref["src"]) > 0
+    for k in ("src", "tar", "weight", "delay"):
+        assert np.array_equal(net[k], ref[k]), k
+    assert np.array_equal(net["type"], ref["type"]) and np.array_equal(net["rate"], ref["rate"])
+    assert np.array_equal(ref["lifconst"], configs.lifconst(*c["lif"]))

@@ -12,19 +12,7 @@ import stdp_net
 EPOCHS = 8
 
 
-def rate_and_cv(counts, ids, n, steps, dt):
-    """Mean rate (Hz) over all neurons, and the mean CV-ISI over the neurons
-    with at least three spikes."""
-    step_of = np.repeat(np.arange(len(counts)), counts)
-    order = np.lexsort((step_of, ids))
-    sid, sst = ids[order], step_of[order]
-    cvs = []
-    bounds = np.flatnonzero(np.diff(sid)) + 1
-    for a, b in zip(np.r_[0, bounds], np.r_[bounds, len(sid)]):
-        if b - a >= 3:
-            isi = np.diff(sst[a:b]).astype(np.float64)
-            cvs.append(isi.std() / isi.mean())
-    return len(ids) / (n * steps * dt), float(np.mean(cvs)), len(cvs)
+rate_and_cv = T.rate_and_cv
 
 
 @pytest.mark.gpu
