@@ -475,6 +475,12 @@ def run_ours(a, ws, rank, local):
                         "sample": f"not run: {e}"}, None
         if ref is not None:
             parity = parity_check(w, local, ref, a.cpu_sample, group_mode, sim_window)
+    reference_gpu = None
+    if rank == 0 and not a.no_refgpu:
+        try:
+            reference_gpu = refgpu_compare(a, local)
+        except Exception as e:  # a baseline leg: its failure does not void the line
+            reference_gpu = {"workload": "refgpu", "unavailable": f"{type(e).__name__}: {e}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": ws,
@@ -492,6 +498,7 @@ def run_ours(a, ws, rank, local):
             "events_per_step": ev_all / (a.steps * CHUNK * ws),
             "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
             "clocks": clk.summary(), "gpu_launches": int(launches), "parity": parity,
+            "reference_gpu": reference_gpu,
             "build_s": build_s, "autotune": tune, "driven_variant": driven,
             "delivery_ceiling": {"reductions_per_s": red_ceiling, "stream_read_gbs": read_ceiling / 1e9,
                                  "how": "mgc_measure_scatter: 1e8 random fp32 red.add into 2^20 "
@@ -780,14 +787,19 @@ def run_sched(a, ws, rank, local):
 
 
 def run_refgpu(a, ws, rank, local):
+    if rank != 0:
+        return
+    print(json.dumps(refgpu_compare(a, local)), flush=True)
+
+
+def refgpu_compare(a, local):
     """The reference's own benchmark network (ModelMaker::make_brunel with
     --ref-syn synapses, Poisson inputs at 20 Hz, generated by the reference's
     gen_net) simulated for --ref-seconds by the reference's own
     MGSimulator::simulate on this GPU (its kernels built for sm_100a in
     oracle/_ref, Poisson draws through the shared counter-based generator)
-    and by this core; wall times, and whether the end states agree."""
-    if rank != 0:
-        return
+    and by this core; wall times, and whether the end states agree.  A
+    baseline leg: the reference's kernels are measured, not shipped."""
     import shutil
     import tempfile
 
@@ -796,8 +808,7 @@ def run_refgpu(a, ws, rank, local):
     ref_gen = os.path.join(ROOT, "oracle", "_ref", "ref_gen")
     ref_sim = os.path.join(ROOT, "oracle", "_ref", "ref_sim")
     if not (os.path.exists(ref_gen) and os.path.exists(ref_sim)):
-        print(json.dumps({"workload": "refgpu", "unavailable": "oracle/_ref is not built (make -C oracle ref)"}))
-        return
+        return {"workload": "refgpu", "unavailable": "oracle/_ref is not built (make -C oracle ref)"}
     tmp = tempfile.mkdtemp()
     try:
         spec = os.path.join(tmp, "net.spec")
@@ -810,8 +821,9 @@ def run_refgpu(a, ws, rank, local):
         gen_s = time.perf_counter() - t0
         net = netfile.read_netfile(path)
         prefix = os.path.join(tmp, "ref")
-        r = subprocess.run([ref_sim, "simulate", path, prefix, str(a.ref_seconds), "-", "0"], check=True, env=env,
-                           capture_output=True, text=True)
+        with ClockSampler(local) as clk_ref:
+            r = subprocess.run([ref_sim, "simulate", path, prefix, str(a.ref_seconds), "-", "0"], check=True,
+                               env=env, capture_output=True, text=True)
         ref_wall = float(r.stdout.split("wall")[1].split()[0])
         n, S = net["n"], len(net["src"])
         b = open(prefix + ".state", "rb").read()
@@ -829,17 +841,18 @@ def run_refgpu(a, ws, rank, local):
         import torch
         stream = torch.cuda.ExternalStream(sim.stream)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0 = time.perf_counter()
-        e0.record(stream)
-        sim.run(steps)
-        e1.record(stream)
-        sim.sync()
-        ours_wall = time.perf_counter() - t0
+        with ClockSampler(local) as clk_ours:
+            t0 = time.perf_counter()
+            e0.record(stream)
+            sim.run(steps)
+            e1.record(stream)
+            sim.sync()
+            ours_wall = time.perf_counter() - t0
         ours_dev = e0.elapsed_time(e1) / 1e3
         st = sim.state()
         events = sim.info()["events"]
         sim.close()
-        print(json.dumps({
+        return {
             "workload": "refgpu",
             "config": {"network": f"the reference's make_brunel, {S} synapses, {n} neurons, inputs 20 Hz, "
                                   f"dt 0.1 ms, generated by the reference's gen_net",
@@ -850,7 +863,8 @@ def run_refgpu(a, ws, rank, local):
             "fire_cnt_identical": bool(np.array_equal(st["fire_cnt"], ref_cnt)),
             "V_identical": bool(np.array_equal(st["V"].view(np.int32), ref_v.view(np.int32))),
             "spikes": int(st["fire_cnt"].sum()),
-        }), flush=True)
+            "clocks": {"reference": clk_ref.summary(), "ours": clk_ours.summary()},
+        }
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
@@ -867,6 +881,8 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
+    ap.add_argument("--no-refgpu", action="store_true",
+                    help="skip the reference's own kernels on this GPU (reference_gpu key)")
     ap.add_argument("--ref-syn", type=float, default=1e8)
     ap.add_argument("--ref-seconds", type=float, default=1.0)
     ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched", "refgpu", "partition"],
@@ -879,7 +895,7 @@ def main():
     ap.add_argument("--sched-train-groups", type=int, default=200)
     ap.add_argument("--sched-eval-groups", type=int, default=300)
     ap.add_argument("--sweep-count", type=int, default=256)
-    ap.add_argument("--sweep-steps", type=int, default=2048)
+    ap.add_argument("--sweep-steps", type=int, default=10000)
     ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2, 3],
                     help="with --kernel-profile or --no-autotune: 0 graphs of k_fused, 1 k_steps groups, "
                          "2 k_pipe groups, 3 k_window groups (window of 4 steps)")

@@ -127,7 +127,29 @@ typedef struct mgc_info {
     int32_t first_neuron;      /* partition handles: whole-network id of neuron 0 (else 0) */
     int32_t total_neurons;     /* partition handles: neurons of the whole network (else n_neurons) */
     int32_t window;            /* steps per window of the windowed step group (0: minimum delay 1) */
+    int32_t accumulation;      /* MGC_ACC_FLOAT or MGC_ACC_FIXED (mgc_set_accumulation) */
+    int32_t fx_shift;          /* fixed-point accumulation: weights are added as rint(w * 2^fx_shift) */
 } mgc_info;
+
+/* How a neuron's input of one step is summed.  FLOAT: fp32 additions, as the
+ * reference's atomicAdd does them (mgcore.cu:112-115); the sum of unequal
+ * weights of one sign then depends on the order in which they land, which
+ * the scattered reductions do not fix (nor do the reference's atomics), so
+ * the last bits of V can differ from run to run.  FIXED: each weight is
+ * added as the integer rint(w * 2^fx_shift) into a 64-bit accumulator, and
+ * the neuron update converts the sum to fp32 once (round to nearest) and
+ * scales it by 2^-fx_shift: the sum does not depend on the order, so every
+ * run gives the same bits.  The builder picks fx_shift so that every weight
+ * is an exact multiple of 2^-fx_shift while any neuron's sum of one step
+ * still fits the integer (with plastic weights only the second); the input
+ * is then the exact sum of the fp32 weights, rounded once.  A new handle
+ * takes FIXED when some neuron receives unequal weights of one sign (or
+ * weights are plastic) and the method is DEFERRED or PUSH, else FLOAT (with
+ * one weight per sign, fp32 sums of the same value are the same in any
+ * order, and equal the reference's bit for bit).  The PULL method always
+ * adds in a fixed order in fp32.  FIXED doubles the accumulators' memory
+ * (8 bytes per neuron and buffer). */
+enum { MGC_ACC_FLOAT = 0, MGC_ACC_FIXED = 1 };
 
 /* Replaces MGSimulator::MGSimulator(Network&, std::vector<int>&, int)
  * (src/simulator/mgsim/adj/mgsim.cpp:337-363) for npart=1: build_multinet
@@ -339,6 +361,11 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * bounded (a time-out makes mgc_sync return MGC_ERR_CUDA).  No reference
  * counterpart. */
 mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
+
+/* Chooses how inputs are summed (MGC_ACC_FLOAT or MGC_ACC_FIXED, see
+ * above), before the handle's first step (MGC_ERR_INVALID after it, or for
+ * FIXED with the pull method).  No reference counterpart. */
+mgc_status mgc_set_accumulation(mgc_sim* sim, int32_t mode);
 
 /* Steps per window of the windowed step group (mode 3 of
  * mgc_set_persistent): 1 <= steps <= min(4, minimum delay); default the

@@ -22,6 +22,7 @@ MGC_OK, MGC_ERR_INVALID, MGC_ERR_CUDA, MGC_ERR_NOMEM, MGC_ERR_OVERFLOW, MGC_ERR_
 RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)
 MODE_AUTO, MODE_PUSH, MODE_DEFERRED, MODE_PULL = 0, 1, 2, 3
 SCHED_STATIC, SCHED_THRESHOLD, SCHED_LEARNED = 0, 1, 2
+ACC_FLOAT, ACC_FIXED = 0, 1
 MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_PARAMS = 20, 32, 5, 837
 
 EXPORTED = (
@@ -34,7 +35,7 @@ EXPORTED = (
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
     "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats", "mgc_part_export_dev",
-    "mgc_part_import_dev", "mgc_raster_stage", "mgc_raster_collect",
+    "mgc_part_import_dev", "mgc_raster_stage", "mgc_raster_collect", "mgc_set_accumulation",
 )
 
 
@@ -91,7 +92,8 @@ class Info(C.Structure):
         ("max_delay", C.c_int32), ("n_synapses", C.c_int64), ("step", C.c_int64),
         ("events", C.c_int64), ("mode", C.c_int32), ("graph_steps", C.c_int32),
         ("device_bytes", C.c_int64), ("persistent", C.c_int32), ("first_neuron", C.c_int32),
-        ("total_neurons", C.c_int32), ("window", C.c_int32),
+        ("total_neurons", C.c_int32), ("window", C.c_int32), ("accumulation", C.c_int32),
+        ("fx_shift", C.c_int32),
     ]
 
 
@@ -158,6 +160,8 @@ def lib():
     L.mgc_set_persistent.restype = C.c_int
     L.mgc_set_window.argtypes = [vp, i32]
     L.mgc_set_window.restype = C.c_int
+    L.mgc_set_accumulation.argtypes = [vp, i32]
+    L.mgc_set_accumulation.restype = C.c_int
     L.mgc_checkpoint_size.argtypes = [vp, C.POINTER(i64)]
     L.mgc_checkpoint_save.argtypes = [vp, vp, i64]
     L.mgc_checkpoint_load.argtypes = [vp, vp, i64]
@@ -508,6 +512,11 @@ class Simulator:
         with a grid barrier per step; 2: pipelined step groups; 3: windowed
         step groups (set_window)."""
         check(lib().mgc_set_persistent(self._h, int(mode)))
+
+    def set_accumulation(self, mode):
+        """ACC_FLOAT (fp32 additions) or ACC_FIXED (order-independent 64-bit
+        fixed point), before the first step (mgc_set_accumulation)."""
+        check(lib().mgc_set_accumulation(self._h, int(mode)))
 
     def set_window(self, steps):
         """Steps per window of the windowed step group (1..min(4, min delay))."""

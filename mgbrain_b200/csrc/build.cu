@@ -6,6 +6,7 @@
 // mgcore.cu:665-669, 685-748).
 #include <cub/cub.cuh>
 
+#include <cmath>
 #include <memory>
 
 #include "sim.h"
@@ -79,11 +80,6 @@ __global__ void k_inverse(const int64_t* csr_syn, int64_t S, uint32_t* pos_of)
 __global__ void k_widen(const uint32_t* in, int64_t S, int64_t* out)
 {
     GRID_STRIDE(p, S) out[p] = in[p];
-}
-
-__global__ void k_iota(uint32_t* v, int64_t S)
-{
-    GRID_STRIDE(p, S) v[p] = (uint32_t)p;
 }
 
 __global__ void k_cast_keys(const int32_t* in, int64_t S, uint32_t* out)
@@ -396,9 +392,7 @@ mgc_status finish_build(mgc_sim* s)
     CK(cudaStreamSynchronize(s->stream));
     if (s->S > 0) CKS(max_row(row_ptr, s->n_src, &max_len));
     a.chunks_per_spike = (int32_t)std::max<int64_t>(1, (max_len + kChunk - 1) / kChunk);
-    cudaDeviceProp prop;
-    CK(cudaGetDeviceProperties(&prop, s->device));
-    int occ = 0;
+    const size_t words = a.fx ? 2 : 1;  // accumulator entries: fp32, or 64-bit fixed point
     if (a.deferred) {
         const int64_t nb = (int64_t)s->n_src * a.D;
         int64_t* bucket = const_cast<int64_t*>(a.bucket);
@@ -417,73 +411,35 @@ mgc_status finish_build(mgc_sim* s)
         s->max_gap = (int64_t)gap;
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n_src, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
-        CKS(s->alloc(&a.acc_e, kAccBuffers * (size_t)a.ns));  // step buffers, s % kAccBuffers
-        CKS(s->alloc(&a.acc_i, kAccBuffers * (size_t)a.ns));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, deliver_kernel(s), kPushBlock, 0));
-        s->deliver_grid = prop.multiProcessorCount * std::max(1, occ);
+        CKS(s->alloc(&a.acc_e, kAccBuffers * (size_t)a.ns * words));  // step buffers, s % kAccBuffers
+        CKS(s->alloc(&a.acc_i, kAccBuffers * (size_t)a.ns * words));
         // fused step kernel: one resident wave, every warp updates then delivers
         s->fused = s->dmin >= 2;
-        for (int v = 0; v < 2; ++v) {
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_kernel(s, v), kPushBlock, 0));
-            s->fused_grid_v[v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
-        }
         s->fused_variant = 1;
-        s->fused_grid = s->fused_grid_v[1];
         // step groups by default (faster than one launch per step on every
         // measured load); the pipelined form needs a minimum delay >= 4.
-        // The windowed form is faster on the measured loads, but it changes
-        // the order of the fp32 additions into one neuron's input (with
-        // unequal weights per sign the last bits of V differ from the
-        // reference's), so only the autotuner or the caller selects it
+        // The windowed form is faster on the measured loads; the autotuner
+        // or the caller selects it
         s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 1;
-        if (!s->fused) {
-            // minimum delay 1: a barrier-per-phase step group sized to the
-            // neurons (8 warps x 64 neuron groups a block per pass)
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, 1, 0), kPushBlock, 0));
-            const int64_t wave = (int64_t)prop.multiProcessorCount * std::max(1, occ);
-            const int64_t want = ((int64_t)a.ns / 4 + 511) / 512;
-            s->group_grid1 = (int)std::max<int64_t>(1, std::min(wave, want));
-            CKS(s->alloc(&a.bar, 4));  // the grid barrier's arrivals and generation
-        }
+        if (!s->fused) CKS(s->alloc(&a.bar, 4));  // the grid barrier's arrivals and generation
         if (s->fused) {
-            for (int p = 1; p <= 2; ++p)
-                for (int v = 0; v < 2; ++v) {
-                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, p, v), kPushBlock, 0));
-                    s->group_grid_v[p - 1][v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
-                }
             // windowed group: prefixes of up to kMaxWindow steps in dynamic shared memory
             s->window = std::min(kMaxWindow, s->dmin);
             s->window_smem = (size_t)kMaxWindow * (size_t)(a.D + 1) * sizeof(int64_t);
-            for (int v = 0; v < 2; ++v) {
-                CK(cudaFuncSetAttribute((const void*)window_kernel(s, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)s->window_smem));
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, window_kernel(s, v), kPushBlock,
-                                                                 s->window_smem));
-                s->window_grid_v[v] = prop.multiProcessorCount * std::min(std::max(1, occ), v == 0 ? 2 : 3);
-            }
             CKS(init_sched(s));
         }
     } else {
         a.M = s->M;
-        CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns));
-        CKS(s->alloc(&a.ring_i, (size_t)s->M * a.ns));
+        CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns * words));
+        CKS(s->alloc(&a.ring_i, (size_t)s->M * a.ns * words));
         CKS(s->alloc(&a.spk, s->n));
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, push_kernel(s), kPushBlock, 0));
-        s->push_grid = prop.multiProcessorCount * std::max(1, occ);
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stdp_kernel(s), kPushBlock, 0));
-        s->stdp_grid = prop.multiProcessorCount * std::max(1, occ);
         if (a.pull) {
             const int64_t groups = a.ns / 4;
             CKS(s->alloc(&a.fired_bits, (size_t)((groups + 31) / 32) * 4));
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pull_kernel(s), kPushBlock, 0));
-            s->pull_grid = prop.multiProcessorCount * std::max(1, occ);
         }
     }
     a.M = s->M;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, neuron_kernel(s), kNeuronBlock, 0));
-    s->neuron_grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>((int64_t)prop.multiProcessorCount * std::max(1, occ),
-                             (a.ns / 4 + kNeuronBlock - 1) / kNeuronBlock));
+    CKS(launch_shapes(s));
     CK(cudaStreamSynchronize(s->stream));
     return MGC_OK;
 }
@@ -507,7 +463,112 @@ mgc_status check_tbits(mgc_sim* s)
 // exchange window.
 struct PartSpec {
     int32_t n_src, first, count, dmin, dmax;
+    bool fx_given;   // the accumulation plan of the whole network (fx), not of the partition's synapses
+    struct FxPlan {
+        bool hetero;     // some neuron receives unequal weights of one sign
+        int32_t shift;   // fixed-point shift for the network's weights
+    } fx;
 };
+using FxPlan = PartSpec::FxPlan;
+
+// Shift of the fixed-point accumulation: the largest for which any neuron's
+// sum of one step fits 61 bits (bound = the largest sum of |w| over one
+// neuron's incoming synapses; a synapse delivers at most once per arrival
+// step), and no larger than needed to make every weight an exact multiple
+// of 2^-shift (min_exp: the smallest frexp exponent of a nonzero |w|; the
+// 24-bit mantissa's last bit is 2^(e-24)).  Kept within the range where
+// 2^shift and 2^-shift are normal floats.
+int32_t fx_shift_for(double bound, int min_exp, bool exact)
+{
+    int k = 0;
+    if (bound > 0.0) {
+        int e = 0;
+        std::frexp(bound, &e);  // bound < 2^e
+        k = 61 - e;
+        if (exact) k = std::min(k, 24 - min_exp);
+    }
+    return std::max(-100, std::min(120, k));
+}
+
+// The plan of a synapse list (targets, weights); plastic synapses may take
+// any weight up to wlim in magnitude.
+FxPlan fx_plan_list(int32_t n, int64_t S, const int32_t* tar, const float* w, const uint8_t* plastic, bool stdp,
+                    float wlim)
+{
+    std::vector<float> first_e(n, 0.0f), first_i(n, 1.0f);  // 1.0: no inhibitory weight seen yet
+    std::vector<double> sum(n, 0.0);
+    bool hetero = false, any_plastic = false;
+    int min_exp = 1 << 20;
+    for (int64_t k = 0; k < S; ++k) {
+        const int32_t t = tar[k];
+        if (t < 0 || t >= n) continue;  // refused later by validation
+        const float x = w[k];
+        const bool pl = stdp && (!plastic || plastic[k]);
+        any_plastic |= pl;
+        sum[t] += pl ? std::max((double)std::fabs(x), (double)wlim) : (double)std::fabs(x);
+        if (x != 0.0f) {
+            int e = 0;
+            std::frexp(x, &e);
+            min_exp = std::min(min_exp, e);
+        }
+        if (x > 0.0f) {
+            if (first_e[t] == 0.0f) first_e[t] = x;
+            else hetero |= first_e[t] != x;
+        } else {
+            if (first_i[t] == 1.0f) first_i[t] = x;
+            else hetero |= first_i[t] != x;
+        }
+    }
+    double bound = 0.0;
+    for (int32_t t = 0; t < n; ++t) bound = std::max(bound, sum[t]);
+    return FxPlan{hetero || any_plastic, fx_shift_for(bound, min_exp, !any_plastic)};
+}
+
+// The plan of fixed in-degree blocks: projection r gives each neuron of its
+// target population pr_k[r] synapses of weight pr_w[r].
+FxPlan fx_plan_blocks(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks)
+{
+    bool hetero = false;
+    double bound = 0.0;
+    int min_exp = 1 << 20;
+    for (int b = 0; b < n_blocks; ++b) {
+        const mgc_fixed_indegree_desc& d = blocks[b];
+        for (int tp = 0; tp < d.n_pops; ++tp) {
+            double sum = 0.0;
+            float we = 0.0f, wi = 1.0f;
+            for (int r = 0; r < d.n_proj; ++r) {
+                if (d.pr_tar[r] != tp || d.pr_k[r] <= 0) continue;
+                const float x = d.pr_w[r];
+                sum += (double)d.pr_k[r] * std::fabs((double)x);
+                if (x != 0.0f) {
+                    int e = 0;
+                    std::frexp(x, &e);
+                    min_exp = std::min(min_exp, e);
+                }
+                if (x > 0.0f) {
+                    hetero |= we != 0.0f && we != x;
+                    we = x;
+                } else {
+                    hetero |= wi != 1.0f && wi != x;
+                    wi = x;
+                }
+            }
+            bound = std::max(bound, sum);
+        }
+    }
+    return FxPlan{hetero, fx_shift_for(bound, min_exp, true)};
+}
+
+// Turns fixed-point accumulation on when some neuron receives unequal
+// weights of one sign (their fp32 sum would depend on the arrival order),
+// except for the pull method, whose per-target pass adds in a fixed order.
+void apply_fx(mgc_sim* s, const FxPlan& p)
+{
+    s->fx_shift = p.shift;
+    s->a.fx = p.hetero && !s->a.pull ? 1 : 0;
+    s->a.fx_scale = std::ldexp(1.0f, p.shift);
+    s->a.fx_unscale = std::ldexp(1.0f, -p.shift);
+}
 
 // Applies a partition spec to a handle whose neuron arrays are built.
 void apply_part(mgc_sim* s, const PartSpec& p)
@@ -525,6 +586,62 @@ mgc_status create_fixed_indegree(const mgc_fixed_indegree_desc* blocks, int32_t 
 }  // namespace
 
 namespace mgc {
+
+// Grids of the kernels this handle launches, from their occupancy (which
+// depends on the instantiation: current arrays, register budget, fp32 or
+// fixed-point accumulation).  Step groups are cooperative launches whose
+// blocks must all be resident.
+mgc_status launch_shapes(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, s->device));
+    const int sms = prop.multiProcessorCount;
+    int occ = 0;
+    if (a.deferred) {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, deliver_kernel(s), kPushBlock, 0));
+        s->deliver_grid = sms * std::max(1, occ);
+        if (s->fused) {
+            for (int v = 0; v < 2; ++v) {
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fused_kernel(s, v), kPushBlock, 0));
+                s->fused_grid_v[v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+            }
+            s->fused_grid = s->fused_grid_v[s->fused_variant];
+            for (int p = 1; p <= 2; ++p)
+                for (int v = 0; v < 2; ++v) {
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, p, v), kPushBlock, 0));
+                    s->group_grid_v[p - 1][v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+                }
+            for (int v = 0; v < 2; ++v) {
+                CK(cudaFuncSetAttribute((const void*)window_kernel(s, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)s->window_smem));
+                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, window_kernel(s, v), kPushBlock,
+                                                                 s->window_smem));
+                s->window_grid_v[v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+            }
+        } else {
+            // minimum delay 1: a barrier-per-phase step group sized to the
+            // neurons (8 warps x 64 neuron groups a block per pass)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, 1, 0), kPushBlock, 0));
+            const int64_t wave = (int64_t)sms * std::max(1, occ);
+            const int64_t want = ((int64_t)a.ns / 4 + 511) / 512;
+            s->group_grid1 = (int)std::max<int64_t>(1, std::min(wave, want));
+        }
+    } else {
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, push_kernel(s), kPushBlock, 0));
+        s->push_grid = sms * std::max(1, occ);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stdp_kernel(s), kPushBlock, 0));
+        s->stdp_grid = sms * std::max(1, occ);
+        if (a.pull) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pull_kernel(s), kPushBlock, 0));
+            s->pull_grid = sms * std::max(1, occ);
+        }
+    }
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, neuron_kernel(s), kNeuronBlock, 0));
+    s->neuron_grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>((int64_t)sms * std::max(1, occ), (a.ns / 4 + kNeuronBlock - 1) / kNeuronBlock));
+    return MGC_OK;
+}
 
 // Segments of up to `gap` synapses cut into chunks of about `target`
 // (a multiple of 32), at most kMaxChunks per segment.
@@ -559,7 +676,8 @@ mgc_status mgc_create_partition(const mgc_net_desc* d, int32_t first, int32_t co
     if (d->n_synapses < 0 || (d->n_synapses > 0 && (!d->syn_src || !d->syn_tar || !d->syn_weight || !d->syn_delay)))
         return fail(MGC_ERR_INVALID, "synapse arrays missing");
     // the whole network's delay range; the synapses of this partition's targets
-    PartSpec p{d->n_neurons, first, count, 0x7fffffff, 0};
+    PartSpec p{d->n_neurons, first, count, 0x7fffffff, 0, true,
+               fx_plan_list(d->n_neurons, d->n_synapses, d->syn_tar, d->syn_weight, nullptr, false, 0.0f)};
     std::vector<int32_t> src, tar, dl;
     std::vector<float> w;
     const int32_t last = first + count;
@@ -642,6 +760,10 @@ mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim*
     s->M = dmax + 1;
     CKS(check_tbits(s.get()));
     CKS(choose_mode(s.get(), d->mode));
+    apply_fx(s.get(), part && part->fx_given
+                          ? part->fx
+                          : fx_plan_list(s->n, S, d->syn_tar, d->syn_weight, d->syn_plastic, s->stdp,
+                                         std::max(std::fabs(d->stdpconst[4]), std::fabs(d->stdpconst[5]))));
     const int dbits = sort_dbits(s.get());
     CKS(begin_layout(s.get()));
     uint2* syn;
@@ -871,6 +993,7 @@ mgc_status create_fixed_indegree(const mgc_fixed_indegree_desc* blocks, int32_t 
     s->M = dmax + 1;
     CKS(check_tbits(s.get()));
     CKS(choose_mode(s.get(), d0.mode));
+    apply_fx(s.get(), fx_plan_blocks(blocks, n_blocks));
     const int dbits = sort_dbits(s.get());
     CKS(begin_layout(s.get()));
     uint2* syn;
@@ -925,8 +1048,36 @@ mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* d, mgc_sim**
 mgc_status mgc_create_fixed_indegree_partition(const mgc_fixed_indegree_desc* d, int32_t first, int32_t count,
                                                mgc_sim** out)
 {
-    const PartSpec p{0, first, count, 0, 0};  // sizes and delays filled in from the description
+    const PartSpec p{0, first, count, 0, 0, false, {}};  // sizes and delays filled in from the description
     return create_fixed_indegree(d, 1, &p, out);
 }
 
 }  // extern "C"
+
+extern "C" mgc_status mgc_set_accumulation(mgc_sim* s, int32_t mode)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (mode != MGC_ACC_FLOAT && mode != MGC_ACC_FIXED) return fail(MGC_ERR_INVALID, "unknown accumulation %d", mode);
+    const int fx = mode == MGC_ACC_FIXED;
+    if (fx == s->a.fx) return MGC_OK;
+    if (fx && s->a.pull)
+        return fail(MGC_ERR_INVALID, "the pull method adds every input in a fixed order (no fixed-point accumulation)");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    int64_t step = 0;
+    CK(cudaMemcpy(&step, s->a.step, 8, cudaMemcpyDeviceToHost));
+    if (step != 0 || s->graph) return fail(MGC_ERR_INVALID, "the accumulation is chosen before the first step");
+    StepArgs& a = s->a;
+    float** bufs[2] = {a.deferred ? &a.acc_e : &a.ring_e, a.deferred ? &a.acc_i : &a.ring_i};
+    const size_t entries = (a.deferred ? (size_t)kAccBuffers : (size_t)s->M) * (size_t)a.ns;
+    for (float** b : bufs) {
+        float* nb = nullptr;
+        CKS(s->alloc(&nb, entries * (fx ? 2 : 1)));  // zeroed: nothing has arrived before the first step
+        s->release(*b);
+        *b = nb;
+    }
+    a.fx = fx;
+    CKS(launch_shapes(s));
+    CK(cudaStreamSynchronize(s->stream));
+    return MGC_OK;
+}

@@ -14,7 +14,7 @@ constexpr uint64_t kCheckpointMagic = 0x3130545043474d4dull;  // "MMGCPT01"
 struct CheckpointHeader {
     uint64_t magic;
     int64_t n, ns, S;
-    int32_t mode, M, H, D, stdp, ahead;
+    int32_t mode, M, H, D, stdp, ahead, fx, fx_shift;
     int64_t bytes;  // whole checkpoint
 };
 
@@ -28,18 +28,19 @@ std::vector<Segment> state_segments(mgc_sim* s)
 {
     StepArgs& a = s->a;
     const size_t ns = (size_t)a.ns, n = (size_t)s->n;
+    const size_t acc = a.fx ? 8 : 4;  // accumulator entry: fp32 or 64-bit fixed point
     std::vector<Segment> v = {
         {a.V, 4 * ns}, {a.Iexc, 4 * ns}, {a.Iinh, 4 * ns}, {a.refrac, 4 * ns}, {a.last_fired, 4 * ns},
         {a.fire_cnt, 4 * ns}, {const_cast<float*>(a.rate), 4 * ns}, {a.step, 16}, {a.events, 8},
         {a.spk_count, 4}};
     if (a.deferred) {
-        v.push_back({a.acc_e, 4 * kAccBuffers * ns});
-        v.push_back({a.acc_i, 4 * kAccBuffers * ns});
+        v.push_back({a.acc_e, acc * kAccBuffers * ns});
+        v.push_back({a.acc_i, acc * kAccBuffers * ns});
         v.push_back({a.hist_ids, 4 * (size_t)a.H * (size_t)s->n_src});
         v.push_back({a.hist_cnt, 4 * (size_t)a.H});
     } else {
-        v.push_back({a.ring_e, 4 * (size_t)s->M * ns});
-        v.push_back({a.ring_i, 4 * (size_t)s->M * ns});
+        v.push_back({a.ring_e, acc * (size_t)s->M * ns});
+        v.push_back({a.ring_i, acc * (size_t)s->M * ns});
         v.push_back({a.spk, 4 * n});
     }
     if (s->stdp) v.push_back({a.pull ? (void*)a.in_ent : (void*)a.syn, 8 * (size_t)s->S});  // plastic weights
@@ -59,6 +60,8 @@ CheckpointHeader checkpoint_header(mgc_sim* s)
     h.D = s->a.D;
     h.stdp = s->stdp;
     h.ahead = s->ahead;
+    h.fx = s->a.fx;
+    h.fx_shift = s->fx_shift;
     h.bytes = sizeof(CheckpointHeader);
     for (const Segment& g : state_segments(s)) h.bytes += (int64_t)g.bytes;
     return h;
@@ -103,7 +106,8 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
     const CheckpointHeader mine = checkpoint_header(s);
     if (h.magic != kCheckpointMagic) return fail(MGC_ERR_INVALID, "not a checkpoint");
     if (h.n != mine.n || h.S != mine.S || h.mode != mine.mode || h.M != mine.M || h.H != mine.H || h.D != mine.D ||
-        h.stdp != mine.stdp || h.bytes != mine.bytes || bytes < h.bytes)
+        h.stdp != mine.stdp || h.fx != mine.fx || h.fx_shift != mine.fx_shift || h.bytes != mine.bytes ||
+        bytes < h.bytes)
         return fail(MGC_ERR_INVALID, "the checkpoint is of another network or method");
     CK(cudaStreamSynchronize(s->stream));
     const char* p = static_cast<const char*>(buf) + sizeof(h);

@@ -5,12 +5,18 @@
 
 namespace mgc {
 
+template <bool FX>
+static GroupKernel steps_of(bool fused, bool cur, int v)
+{
+    if (!fused) return cur ? k_steps1<true, FX> : k_steps1<false, FX>;  // minimum delay 1
+    if (cur) return v == 0 ? k_steps<true, 2, FX> : k_steps<true, 3, FX>;
+    return v == 0 ? k_steps<false, 2, FX> : k_steps<false, 3, FX>;
+}
+
 GroupKernel steps_kernel(const mgc_sim* s, int p, int v)
 {
-    if (!s->fused) return s->a.has_cur ? k_steps1<true> : k_steps1<false>;  // minimum delay 1
-    if (p == 2) return pipe_kernel(s, v);
-    if (s->a.has_cur) return v == 0 ? k_steps<true, 2> : k_steps<true, 3>;
-    return v == 0 ? k_steps<false, 2> : k_steps<false, 3>;
+    if (s->fused && p == 2) return pipe_kernel(s, v);
+    return s->a.fx ? steps_of<true>(s->fused, s->a.has_cur, v) : steps_of<false>(s->fused, s->a.has_cur, v);
 }
 
 }  // namespace mgc

@@ -75,8 +75,11 @@ struct StepArgs {
     int32_t* hist_ids;    //   [H][n_src] spike ids per step
     int32_t* hist_cnt;    //   [H]
     const int64_t* bucket;   // [n_src*D + 1] CSR position of (source, bucket)
-    float* acc_e;         //   [4][ns] input arriving at step s in buffer s % 4
-    float* acc_i;
+    float* acc_e;         //   [4][ns] input arriving at step s in buffer s % 4 (fixed-point
+    float* acc_i;         //   accumulation: 64-bit integers, 8 bytes an entry)
+    int32_t fx;           // fixed-point accumulation (deferred and ring methods)
+    float fx_scale;       //   2^fx_shift: a weight w is added as the integer rint(w * fx_scale)
+    float fx_unscale;     //   2^-fx_shift: an input sum is float(sum) * fx_unscale
     int32_t pull;         // pull method (per-target pass at emission, STDP fused)
     uint32_t* fired_bits; //   [ns/32] spikes of the current step
     const int64_t* in_ptr;//   [n+1] incoming rows (by target)
@@ -92,8 +95,8 @@ struct StepArgs {
     int32_t* refrac;
     int32_t* last_fired;
     int32_t* fire_cnt;
-    float* ring_e;        // [M][n]
-    float* ring_i;        // [M][n]
+    float* ring_e;        // [M][ns] (fixed-point accumulation: 64-bit integers)
+    float* ring_i;        // [M][ns]
     // synapses: CSR by source; word .x = target | delay << tbits, .y = weight bits
     const int64_t* row_ptr;
     uint2* syn;
@@ -147,6 +150,65 @@ __device__ __forceinline__ void red_add(float* p, float v)
     asm volatile("red.relaxed.gpu.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t as_u(float f) { return __float_as_uint(f); }
+
+// ---------------------------------------------------------------------------
+// Fixed-point accumulation (FX), for networks in which some neuron receives
+// unequal weights of one sign.  fp32 additions of unequal values depend on
+// their order, and the order in which scattered reductions land is not
+// fixed, so such a neuron's input would change in the last bits from run to
+// run (the reference's atomicAdd, mgcore.cu:112-115, has the same property).
+// Instead every weight is added as the integer rint(w * 2^shift) into a
+// 64-bit accumulator: integer addition is associative, so the sum does not
+// depend on the order, and the neuron update converts it to fp32 once
+// (round to nearest) and scales it back by 2^-shift (exact).  The builder
+// picks the shift so that every weight of the network is an exact multiple
+// of 2^-shift whenever the sums still fit 63 bits; the input is then the
+// exact sum of the arriving fp32 weights, rounded once.  Only the final
+// sum must fit: partial sums that wrap cancel in two's complement.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long to_fx(float w, float scale) { return __float2ll_rn(__fmul_rn(w, scale)); }
+__device__ __forceinline__ float from_fx(long long x, float unscale) { return __fmul_rn(__ll2float_rn(x), unscale); }
+__device__ __forceinline__ void red_add_fx(unsigned long long* p, long long v)
+{
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// The accumulator entries of one step: fp32, or 64-bit fixed point.
+template <bool FX> struct AccT { using type = float; };
+template <> struct AccT<true> { using type = unsigned long long; };
+
+// One group of four neurons' input of one step, loaded with the group
+// (16-byte loads; two of them for fixed point) and read as fp32.
+template <bool FX> struct In4;
+template <> struct In4<false> {
+    float4 v;
+    __device__ __forceinline__ void zero() { v = make_float4(0.f, 0.f, 0.f, 0.f); }
+    __device__ __forceinline__ void load(const void* base, int64_t g) { v = reinterpret_cast<const float4*>(base)[g]; }
+    __device__ __forceinline__ float4 get(const StepArgs&) const { return v; }
+    __device__ __forceinline__ static void clear(void* base, int64_t g)
+    {
+        reinterpret_cast<float4*>(base)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+};
+template <> struct In4<true> {
+    longlong2 lo, hi;
+    __device__ __forceinline__ void zero() { lo = hi = make_longlong2(0, 0); }
+    __device__ __forceinline__ void load(const void* base, int64_t g)
+    {
+        lo = reinterpret_cast<const longlong2*>(base)[2 * g];
+        hi = reinterpret_cast<const longlong2*>(base)[2 * g + 1];
+    }
+    __device__ __forceinline__ float4 get(const StepArgs& a) const
+    {
+        return make_float4(from_fx(lo.x, a.fx_unscale), from_fx(lo.y, a.fx_unscale), from_fx(hi.x, a.fx_unscale),
+                           from_fx(hi.y, a.fx_unscale));
+    }
+    __device__ __forceinline__ static void clear(void* base, int64_t g)
+    {
+        reinterpret_cast<longlong2*>(base)[2 * g] = make_longlong2(0, 0);
+        reinterpret_cast<longlong2*>(base)[2 * g + 1] = make_longlong2(0, 0);
+    }
+};
 
 #ifdef MGC_CHECKED
 __device__ __forceinline__ bool mgc_check_index(const StepArgs& a, bool ok)
@@ -310,8 +372,8 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
 // read from (and cleared in) in_e/in_i, which point at the ring slot or the
 // accumulator buffer.  Spiking ids are compacted in neuron order within the
 // pass, one atomic per warp.
-template <int G, bool CUR>
-__device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, float* in_e, float* in_i,
+template <int G, bool CUR, bool FX>
+__device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int32_t hslot, void* in_e, void* in_i,
                                               int64_t warp, int64_t nwarps, int64_t rbase, int* pop_cnt = nullptr,
                                               bool raster = true)
 {
@@ -323,7 +385,8 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     const bool rec = raster && (a.deferred || a.pull) && a.record;  // no push kernel to record
     for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
         char4 t4[G];
-        float4 v4[G], e4[G], i4[G], ce4[G], ci4[G];
+        float4 v4[G], ce4[G], ci4[G];
+        In4<FX> e4[G], i4[G];
         int4 r4[G];
 #pragma unroll
         for (int h = 0; h < G; ++h) {
@@ -333,8 +396,8 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 t4[h] = __ldg(reinterpret_cast<const char4*>(a.type) + g);
                 v4[h] = reinterpret_cast<float4*>(a.V)[g];
                 r4[h] = reinterpret_cast<int4*>(a.refrac)[g];
-                e4[h] = reinterpret_cast<float4*>(in_e)[g];
-                i4[h] = reinterpret_cast<float4*>(in_i)[g];
+                e4[h].load(in_e, g);
+                i4[h].load(in_i, g);
                 if (CUR) {  // in flight with the rest of the group
                     ce4[h] = reinterpret_cast<float4*>(a.Iexc)[g];
                     ci4[h] = reinterpret_cast<float4*>(a.Iinh)[g];
@@ -352,16 +415,17 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 float u[4] = {0.f, 0.f, 0.f, 0.f};
                 if (t4[h].x == kPOISSON || t4[h].y == kPOISSON || t4[h].z == kPOISSON || t4[h].w == kPOISSON)
                     poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
-                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e4[h].x, i4[h].x, ce4[h].x, ci4[h].x, u[0]) ? 1u : 0u;
-                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e4[h].y, i4[h].y, ce4[h].y, ci4[h].y, u[1]) ? 2u : 0u;
-                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e4[h].z, i4[h].z, ce4[h].z, ci4[h].z, u[2]) ? 4u : 0u;
-                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e4[h].w, i4[h].w, ce4[h].w, ci4[h].w, u[3]) ? 8u : 0u;
+                const float4 e = e4[h].get(a), ii = i4[h].get(a);
+                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e.x, ii.x, ce4[h].x, ci4[h].x, u[0]) ? 1u : 0u;
+                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e.y, ii.y, ce4[h].y, ci4[h].y, u[1]) ? 2u : 0u;
+                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e.z, ii.z, ce4[h].z, ci4[h].z, u[2]) ? 4u : 0u;
+                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e.w, ii.w, ce4[h].w, ci4[h].w, u[3]) ? 8u : 0u;
                 // the input is cleared only after it was used: a store issued
                 // while the load of the same line is in flight stalls the
                 // memory pipeline (measured 4-6x slower once the state
                 // leaves L2)
-                reinterpret_cast<float4*>(in_e)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4*>(in_i)[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                In4<FX>::clear(in_e, g);
+                In4<FX>::clear(in_i, g);
                 reinterpret_cast<float4*>(a.V)[g] = v4[h];
                 reinterpret_cast<int4*>(a.refrac)[g] = r4[h];
                 if (CUR) {
@@ -430,9 +494,10 @@ __device__ __forceinline__ int64_t raster_base(const StepArgs& a)
 // is still being read.
 constexpr int kAccBuffers = 4;
 
-__device__ __forceinline__ float* acc_buf(const StepArgs& a, float* base, int64_t s)
+template <bool FX = false>
+__device__ __forceinline__ typename AccT<FX>::type* acc_buf(const StepArgs& a, float* base, int64_t s)
 {
-    return base + (size_t)(s & (kAccBuffers - 1)) * (size_t)a.ns;
+    return reinterpret_cast<typename AccT<FX>::type*>(base) + (size_t)(s & (kAccBuffers - 1)) * (size_t)a.ns;
 }
 
 template <bool FX>
@@ -440,20 +505,20 @@ __global__ void __launch_bounds__(kNeuronBlock) k_neuron(StepArgs a)
 {
     const int64_t s = *a.step;
     const int32_t slot = a.slots[0], hslot = a.slots[1];
-    float *in_e, *in_i;
+    void *in_e, *in_i;
     if (a.deferred) {
-        in_e = acc_buf(a, a.acc_e, s);
-        in_i = acc_buf(a, a.acc_i, s);
+        in_e = acc_buf<FX>(a, a.acc_e, s);
+        in_i = acc_buf<FX>(a, a.acc_i, s);
     } else {
-        in_e = a.ring_e + (size_t)slot * (size_t)a.ns;
-        in_i = a.ring_i + (size_t)slot * (size_t)a.ns;
+        in_e = reinterpret_cast<typename AccT<FX>::type*>(a.ring_e) + (size_t)slot * (size_t)a.ns;
+        in_i = reinterpret_cast<typename AccT<FX>::type*>(a.ring_i) + (size_t)slot * (size_t)a.ns;
     }
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     if (a.has_cur)
-        neuron_groups<1, true>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
+        neuron_groups<1, true, FX>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
     else
-        neuron_groups<1, false>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
+        neuron_groups<1, false, FX>(a, s, hslot, in_e, in_i, warp, nwarps, raster_base(a));
     if (a.deferred) {
         if (last_block(a.done)) step_epilogue(a);
     }
@@ -527,7 +592,7 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 // the n <= NMAX consecutive arrival steps sa, sa+1, ... as one task space
 // (step k's prefixes at pre + k*(D+1)), so that a warp's lanes fetch the
 // segments of several steps in one batch.
-template <int NMAX = 1>
+template <bool FX, int NMAX = 1>
 __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot,
                                               const int64_t* pre, int64_t warp, int64_t nwarps,
                                               unsigned long long* blk_ev = nullptr, int n = 1)
@@ -622,13 +687,18 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
                 if (!MGC_OK_INDEX((w[u].x & a.tmask) < (uint32_t)a.ns)) continue;
                 const float wt = as_f(w[u].y);
                 const int64_t sx = sa + (NMAX > 1 ? st_of[u] : 0);
-                red_add(acc_buf(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
+                if (FX)
+                    red_add_fx(acc_buf<true>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask),
+                               to_fx(wt, a.fx_scale));
+                else
+                    red_add(acc_buf(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
             }
         }
     }
     if (ev) atomicAdd(blk_ev ? blk_ev : a.events, ev);
 }
 
+template <bool FX>
 __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, int64_t* pre, int64_t warp,
                                                  int64_t nwarps)
 {
@@ -636,7 +706,7 @@ __device__ __forceinline__ void deliver_arrivals(const StepArgs& a, int64_t sa, 
     const int32_t hslot = a.slots[1];
     if (threadIdx.x < 32) deliver_prefix(a, sa, s, hslot, pre);
     __syncthreads();
-    deliver_tasks(a, sa, s, hslot, pre, warp, nwarps);
+    deliver_tasks<FX>(a, sa, s, hslot, pre, warp, nwarps);
 }
 
 // Arrivals of the current step (used when the minimum delay is one step).
@@ -646,7 +716,7 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
     __shared__ int64_t pre[kMaxBuckets + 1];
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    deliver_arrivals(a, *a.step, pre, warp, nwarps);
+    deliver_arrivals<FX>(a, *a.step, pre, warp, nwarps);
 }
 
 // One launch per step when the minimum delay is >= 2: the arrivals of step
@@ -656,7 +726,7 @@ __global__ void __launch_bounds__(kPushBlock) k_deliver(StepArgs a)
 // different warps overlap on each SM.
 // MINB: resident blocks per SM the kernel is compiled for (its register
 // budget); the schedule chooses between the instantiations.
-template <bool CUR, int MINB>
+template <bool CUR, int MINB, bool FX>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_fused(StepArgs a)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
@@ -670,12 +740,12 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_fused(StepArgs a)
     // their neurons; the barrier then publishes the sums for the delivery
     const int32_t hslot = a.slots[1];
     if (threadIdx.x < 32) deliver_prefix(a, s + 1, s, hslot, pre);
-    neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, raster_base(a),
+    neuron_groups<2, CUR, FX>(a, s, hslot, acc_buf<FX>(a, a.acc_e, s), acc_buf<FX>(a, a.acc_i, s), warp, nwarps, raster_base(a),
                           a.trace ? pop_cnt : nullptr);
     __syncthreads();
     if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
         atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
-    deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps);
+    deliver_tasks<FX>(a, s + 1, s, hslot, pre, warp, nwarps);
     if (last_block(a.done)) step_epilogue(a);
 }
 
@@ -719,7 +789,7 @@ __device__ __forceinline__ bool grid_barrier(const StepArgs& a, int* abort_flag)
     return *abort_flag == 0;
 }
 
-template <bool CUR, int MINB>
+template <bool CUR, int MINB, bool FX>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t nsteps)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
@@ -749,12 +819,12 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
         if (threadIdx.x < kTracePops) pop_cnt[threadIdx.x] = 0;
         __syncthreads();
         if (threadIdx.x < 32) deliver_prefix(a, s + 1, s, hslot, pre);
-        neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+        neuron_groups<2, CUR, FX>(a, s, hslot, acc_buf<FX>(a, a.acc_e, s), acc_buf<FX>(a, a.acc_i, s), warp, nwarps,
                               a.record ? rbase : 0, a.trace ? pop_cnt : nullptr);
         __syncthreads();
         if (a.trace && threadIdx.x < kTracePops && pop_cnt[threadIdx.x])
             atomicAdd(a.trace + (s & (kTraceSteps - 1)) * kTraceCols + threadIdx.x, (float)pop_cnt[threadIdx.x]);
-        deliver_tasks(a, s + 1, s, hslot, pre, warp, nwarps, a.trace ? nullptr : &blk_ev);
+        deliver_tasks<FX>(a, s + 1, s, hslot, pre, warp, nwarps, a.trace ? nullptr : &blk_ev);
         if (!a.trace && i == nsteps - 1) {  // the block's events, before the last barrier
             __syncthreads();
             if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);
@@ -812,7 +882,7 @@ constexpr int kMaxWindow = 4;
 // Neurons [first group, ...) advanced through the window's wl steps.  One
 // group of four neurons per lane per pass: its state and its wl input slots
 // are loaded at once, the steps run in registers, the state is stored once.
-template <bool CUR>
+template <bool CUR, bool FX>
 __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int wl, int32_t hs0, int64_t warp,
                                               int64_t nwarps)
 {
@@ -824,7 +894,7 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         char4 t4 = make_char4(0, 0, 0, 0);
         float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), ce4 = v4, ci4 = v4;
         int4 r4 = make_int4(0, 0, 0, 0);
-        float4 e4[kMaxWindow], i4[kMaxWindow];
+        In4<FX> e4[kMaxWindow], i4[kMaxWindow];
         if (have) {
             t4 = __ldg(reinterpret_cast<const char4*>(a.type) + g);
             v4 = reinterpret_cast<float4*>(a.V)[g];
@@ -836,10 +906,11 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         }
 #pragma unroll
         for (int k = 0; k < kMaxWindow; ++k) {
-            e4[k] = i4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            e4[k].zero();
+            i4[k].zero();
             if (have && k < wl) {
-                e4[k] = reinterpret_cast<float4*>(acc_buf(a, a.acc_e, w0 + k))[g];
-                i4[k] = reinterpret_cast<float4*>(acc_buf(a, a.acc_i, w0 + k))[g];
+                e4[k].load(acc_buf<FX>(a, a.acc_e, w0 + k), g);
+                i4[k].load(acc_buf<FX>(a, a.acc_i, w0 + k), g);
             }
         }
         const int32_t i0 = (int32_t)(g << 2);
@@ -852,13 +923,14 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
             if (have) {
                 float u[4] = {0.f, 0.f, 0.f, 0.f};
                 if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
-                fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e4[k].x, i4[k].x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
-                fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e4[k].y, i4[k].y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
-                fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e4[k].z, i4[k].z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
-                fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e4[k].w, i4[k].w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                const float4 e = e4[k].get(a), ii = i4[k].get(a);
+                fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
+                fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
+                fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
+                fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
                 // the step's input was used: its slot is cleared for step s+4
-                reinterpret_cast<float4*>(acc_buf(a, a.acc_e, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
-                reinterpret_cast<float4*>(acc_buf(a, a.acc_i, s))[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+                In4<FX>::clear(acc_buf<FX>(a, a.acc_e, s), g);
+                In4<FX>::clear(acc_buf<FX>(a, a.acc_i, s), g);
             }
             // the step's spikes into its history slot, in neuron order within
             // the warp (no scan when no lane spiked)
@@ -901,19 +973,20 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
 // before sa0: the prefixes of the n steps by the first n warps, then every
 // warp through the n steps' tasks without a barrier between them.  s, hslot:
 // a step and its history slot, for the slot arithmetic.
+template <bool FX>
 __device__ __forceinline__ void deliver_window(const StepArgs& a, int64_t sa0, int n, int64_t s, int32_t hslot,
                                                int64_t* pre, int64_t warp, int64_t nwarps, unsigned long long* blk_ev)
 {
     const int wib = threadIdx.x >> 5;
     for (int k = wib; k < n; k += blockDim.x >> 5) deliver_prefix(a, sa0 + k, s, hslot, pre + (size_t)k * (a.D + 1));
     __syncthreads();
-    deliver_tasks<kMaxWindow>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
+    deliver_tasks<FX, kMaxWindow>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
 }
 
 __device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0,
                                             int64_t& rbase);
 
-template <bool CUR, int MINB>
+template <bool CUR, int MINB, bool FX>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t nsteps, int32_t W)
 {
     extern __shared__ int64_t wpre[];   // [kMaxWindow][D + 1]
@@ -940,12 +1013,12 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         if (lead)
             for (int k = 1; k <= n; ++k) a.hist_cnt[hs_of(s0 + k)] = 0;
         __syncthreads();
-        if (n > 0) deliver_window(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
+        if (n > 0) deliver_window<FX>(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
         if (!grid_barrier(a, &abort_flag)) return;
     }
     for (int64_t w0 = s0; w0 < s_end;) {
         const int wl = (int)(s_end - w0 < W ? s_end - w0 : W);
-        neuron_window<CUR>(a, w0, wl, hs_of(w0), warp, nwarps);
+        neuron_window<CUR, FX>(a, w0, wl, hs_of(w0), warp, nwarps);
         if (!grid_barrier(a, &abort_flag)) return;
         // the window's spikes are complete: its raster, then the next
         // window's arrivals (only those of s_end after the last window)
@@ -955,7 +1028,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         const int nn = (int)(next < s_end ? (s_end - next < W ? s_end - next : W) : 1);
         if (lead)
             for (int k = 0; k < nn; ++k) a.hist_cnt[hs_of(next + k)] = 0;
-        deliver_window(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
+        deliver_window<FX>(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
         if (next >= s_end) {  // the block's events, before the last barrier
             __syncthreads();
             if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);
@@ -982,7 +1055,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
 // small network takes few blocks and cheap barriers.  Waits are bounded
 // (kStatusBarrier).
 // ---------------------------------------------------------------------------
-template <bool CUR>
+template <bool CUR, bool FX>
 __global__ void __launch_bounds__(kPushBlock, 2) k_steps1(StepArgs a, int32_t nsteps)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
@@ -1000,11 +1073,11 @@ __global__ void __launch_bounds__(kPushBlock, 2) k_steps1(StepArgs a, int32_t ns
         // the arrivals of step s: spikes of steps <= s-1, complete at the last barrier
         if (threadIdx.x < 32) deliver_prefix(a, s, s, hslot, pre);
         __syncthreads();
-        deliver_tasks(a, s, s, hslot, pre, warp, nwarps);
+        deliver_tasks<FX>(a, s, s, hslot, pre, warp, nwarps);
         if (!grid_barrier(a, &abort_flag)) return;
         // step s+1's slot held step s+1-H, which no delivery reads any more
         if (lead) a.hist_cnt[next_h] = 0;
-        neuron_groups<2, CUR>(a, s, hslot, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps,
+        neuron_groups<2, CUR, FX>(a, s, hslot, acc_buf<FX>(a, a.acc_e, s), acc_buf<FX>(a, a.acc_i, s), warp, nwarps,
                               a.record ? rbase : 0);
         if (!grid_barrier(a, &abort_flag)) return;
         // step s is complete on every block
@@ -1124,7 +1197,7 @@ __device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32
     rbase += cnt;
 }
 
-template <bool CUR, int MINB>
+template <bool CUR, int MINB, bool FX>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t nsteps)
 {
     __shared__ int64_t pre[kMaxBuckets + 1];
@@ -1156,7 +1229,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
     if (nsteps > 0) {
         if (threadIdx.x < 32) deliver_prefix(a, s0 + 1, s0, h0, pre);
         __syncthreads();
-        deliver_tasks(a, s0 + 1, s0, h0, pre, warp, nwarps);
+        deliver_tasks<FX>(a, s0 + 1, s0, h0, pre, warp, nwarps);
     }
     arrive(a, 0, 0, nullptr, nullptr, false);
     for (int32_t i = 0; i < nsteps; ++i) {
@@ -1174,10 +1247,10 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_pipe(StepArgs a, int32_t n
         const int b = i & 1;
         unsigned long long* evb = a.trace ? &blk_ev[b] : &blk_ev[0];  // per step, or for the group
         if (deliver && threadIdx.x < 32) deliver_prefix(a, s + 2, s, hs, pre);
-        neuron_groups<2, CUR>(a, s, hs, acc_buf(a, a.acc_e, s), acc_buf(a, a.acc_i, s), warp, nwarps, 0,
+        neuron_groups<2, CUR, FX>(a, s, hs, acc_buf<FX>(a, a.acc_e, s), acc_buf<FX>(a, a.acc_i, s), warp, nwarps, 0,
                               a.trace ? pop_cnt[b] : nullptr, false);
         __syncthreads();
-        if (deliver) deliver_tasks(a, s + 2, s, hs, pre, warp, nwarps, evb);
+        if (deliver) deliver_tasks<FX>(a, s + 2, s, hs, pre, warp, nwarps, evb);
         arrive(a, i + 1, s, pop_cnt[b], evb, i == nsteps - 1);
     }
     // the group's last steps: all blocks done (phases n-1 and n), remaining raster, the clock
@@ -1239,7 +1312,11 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
             if (!MGC_OK_INDEX(tgt < (uint32_t)a.ns && slot >= 0 && slot < a.M)) continue;
             const float wt = as_f(w[u].y);
             float* ring = wt > 0.0f ? a.ring_e : a.ring_i;
-            red_add(ring + (size_t)slot * (size_t)a.ns + tgt, wt);
+            const size_t at = (size_t)slot * (size_t)a.ns + tgt;
+            if (FX)
+                red_add_fx(reinterpret_cast<unsigned long long*>(ring) + at, to_fx(wt, a.fx_scale));
+            else
+                red_add(ring + at, wt);
         }
     }
     if (lane == 0 && ev) atomicAdd(a.events, ev);

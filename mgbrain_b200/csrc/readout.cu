@@ -335,6 +335,8 @@ mgc_status mgc_get_info(mgc_sim* s, mgc_info* info)
     info->first_neuron = s->a.src_base;
     info->total_neurons = s->n_src;
     info->window = s->fused ? s->window : 0;
+    info->accumulation = s->a.fx ? MGC_ACC_FIXED : MGC_ACC_FLOAT;
+    info->fx_shift = s->fx_shift;
     return MGC_OK;
 }
 

@@ -101,6 +101,7 @@ struct mgc_sim {
     int64_t* in_syn64 = nullptr;  // synapse-list index of each incoming-row position (pull)
     bool ahead = true;   // arrivals of the current device step are already delivered
     std::vector<void*> allocs;
+    std::vector<size_t> alloc_bytes;  // size of each of allocs
     size_t bytes = 0;
     int64_t* csr_syn64 = nullptr;  // synapse-list index of each CSR position (explicit nets)
     int64_t launches = 0;
@@ -123,6 +124,7 @@ struct mgc_sim {
     int window_grid_v[2] = {1, 1};    // its co-resident grids by variant
     size_t window_smem = 0;           // its dynamic shared memory: the window's delivery prefixes
     int group_grid1 = 1;              // minimum delay 1: the step group's grid
+    int32_t fx_shift = 0;             // fixed-point shift the builder picked for this network's weights
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
 
@@ -145,10 +147,24 @@ struct mgc_sim {
         size_t b = std::max<size_t>(count, 1) * sizeof(T);
         CK(mgc::dev_malloc(&v, b));
         allocs.push_back(v);
+        alloc_bytes.push_back(b);
         bytes += b;
         if (zero) CK(cudaMemsetAsync(v, 0, b, stream));
         *p = static_cast<T*>(v);
         return MGC_OK;
+    }
+
+    // Frees one of the handle's buffers (after the stream is idle).
+    void release(void* p)
+    {
+        for (size_t i = 0; i < allocs.size(); ++i)
+            if (allocs[i] == p) {
+                cudaFree(p);
+                bytes -= alloc_bytes[i];
+                allocs.erase(allocs.begin() + i);
+                alloc_bytes.erase(alloc_bytes.begin() + i);
+                return;
+            }
     }
 
     template <class T>
@@ -203,6 +219,8 @@ const void* sched_decide_kernel();
 
 // ---- network construction (build.cu) ----------------------------------------
 mgc_status pick_device(int device);
+// Grids of the kernels the handle launches (after the kernel selection changed).
+mgc_status launch_shapes(mgc_sim* s);
 // Segments of up to `gap` synapses cut into chunks of about `target`.
 void set_chunking(StepArgs& a, int64_t gap, int64_t target);
 

@@ -133,9 +133,9 @@ __global__ void __launch_bounds__(kPushBlock) k_stdp(StepArgs a)
     if (last_block(a.done)) step_epilogue(a);
 }
 
-StepKernel neuron_kernel(const mgc_sim*) { return k_neuron<false>; }
-StepKernel deliver_kernel(const mgc_sim*) { return k_deliver<false>; }
-StepKernel push_kernel(const mgc_sim*) { return k_push<false>; }
+StepKernel neuron_kernel(const mgc_sim* s) { return s->a.fx ? k_neuron<true> : k_neuron<false>; }
+StepKernel deliver_kernel(const mgc_sim* s) { return s->a.fx ? k_deliver<true> : k_deliver<false>; }
+StepKernel push_kernel(const mgc_sim* s) { return s->a.fx ? k_push<true> : k_push<false>; }
 StepKernel pull_kernel(const mgc_sim*) { return k_pull; }
 StepKernel stdp_kernel(const mgc_sim*) { return k_stdp; }
 

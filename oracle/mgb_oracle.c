@@ -39,6 +39,11 @@ struct mgbo_sim {
     int32_t id_offset;
     int64_t step, events;
     int32_t* spk;
+    /* fixed-point accumulation (mgbo_set_fx): integer rings, weights added
+     * as rint(w * fx_scale), sums read as float(sum) * fx_unscale */
+    int fx;
+    float fx_scale, fx_unscale;
+    int64_t *ring_fx_e, *ring_fx_i;
 };
 
 /* ------------------------------------------------------------------ */
@@ -277,6 +282,22 @@ int64_t mgbo_effective_steps(int64_t steps, int32_t min_delay)
 /* ------------------------------------------------------------------ */
 static inline float mgbo_exp_f32(float x) { return expf(x); }
 static inline double mgbo_exp_f64(double x) { return exp(x); }
+
+/* A neuron's input of the step from ring entry loc, and the clearing of the
+ * entry: the REAL rings, or with fixed-point accumulation the integer sum
+ * converted to float once (round to nearest) and scaled by 2^-shift. */
+#define IN_E(loc) (s->fx ? (REAL)((float)s->ring_fx_e[loc] * s->fx_unscale) : re[loc])
+#define IN_I(loc) (s->fx ? (REAL)((float)s->ring_fx_i[loc] * s->fx_unscale) : ri[loc])
+#define CLEAR_IN(loc)                                         \
+    do {                                                      \
+        if (s->fx) {                                          \
+            s->ring_fx_e[loc] = 0;                            \
+            s->ring_fx_i[loc] = 0;                            \
+        } else {                                              \
+            re[loc] = 0;                                      \
+            ri[loc] = 0;                                      \
+        }                                                     \
+    } while (0)
 
 #define REAL float
 #define SUFFIX(x) x##_f32
@@ -599,10 +620,23 @@ void mgbo_destroy(mgbo_sim* s)
     free(s->refrac); free(s->V); free(s->Iexc); free(s->Iinh); free(s->ring_e); free(s->ring_i);
     free(s->w); free(s->axon_off); free(s->csr_tar); free(s->csr_src); free(s->csr_delay);
     free(s->csr_syn); free(s->csr_plastic); free(s->dend_off); free(s->dend_pos); free(s->spk);
+    free(s->ring_fx_e); free(s->ring_fx_i);
     free(s);
 }
 
 void mgbo_set_id_offset(mgbo_sim* s, int32_t id_offset) { s->id_offset = id_offset; }
+
+int mgbo_set_fx(mgbo_sim* s, int32_t shift)
+{
+    if (s->precision != MGBO_F32 || s->step != 0 || s->fx) return -1;
+    s->ring_fx_e = xcalloc((size_t)s->n * s->M, sizeof(int64_t));
+    s->ring_fx_i = xcalloc((size_t)s->n * s->M, sizeof(int64_t));
+    if (!s->ring_fx_e || !s->ring_fx_i) return -1;
+    s->fx = 1;
+    s->fx_scale = ldexpf(1.0f, shift);
+    s->fx_unscale = ldexpf(1.0f, -shift);
+    return 0;
+}
 
 void mgbo_set_threads(mgbo_sim* s, int32_t nthreads)
 {

@@ -122,6 +122,13 @@ void mgbo_set_threads(mgbo_sim* s, int32_t nthreads);  /* threads of later runs 
 /* Neuron ids in the POISSON draws are offset by id_offset (a block of a
  * larger network draws as it does there). */
 void mgbo_set_id_offset(mgbo_sim* s, int32_t id_offset);
+/* Fixed-point accumulation, as the CUDA core's (include/mgc.h,
+ * MGC_ACC_FIXED): every weight is added as llrintf(w * 2^shift) into a
+ * 64-bit sum, which the neuron update reads as (float)sum * 2^-shift.  F32
+ * sims, before the first step; returns 0 or -1.  Not a restatement of the
+ * reference (whose fp32 atomics leave the order of unequal additions open):
+ * it pins the CUDA core's order-independent arithmetic bit for bit. */
+int mgbo_set_fx(mgbo_sim* s, int32_t shift);
 int64_t mgbo_events(const mgbo_sim* s);      /* synaptic events delivered so far */
 int64_t mgbo_step(const mgbo_sim* s);        /* steps simulated so far */
 int32_t mgbo_ring_len(const mgbo_sim* s);    /* M = max_delay + 1 */

@@ -31,9 +31,13 @@ def ref_outputs(name):
     return counts, ids, st
 
 
-def run_oracle(name, precision=T.F32):
+def run_oracle(name, precision=T.F32, fx=None):
+    """The oracle on a golden case; fx: fixed-point accumulation with this
+    shift (the CUDA core's MGC_ACC_FIXED arithmetic)."""
     c, net, v0 = load(name)
     sim = T.OracleSim(net, c["seed"], v0=v0, stdp=c["stdp"], precision=precision)
+    if fx is not None:
+        sim.set_fx(fx)
     off = c.get("rates_off")
     if off:
         c1, i1 = sim.run(off)

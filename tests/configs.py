@@ -13,6 +13,12 @@ C1  Vogels-Abbott-style network: 3,200 exc + 800 inh LIF with V shifted by
     p = 0.02, +0.27 mV / -4.5 mV, delay 0.1 ms (one step); 5 % of the neurons
     (200 exc) each get a POISSON input at 100 Hz (0.01 per step, 20 mV, one
     to one) for the first 50 ms; V0 ~ U[0, 10 mV); dt 0.1 ms, 10 s.
+C0R a C0-shaped network (2,000 LIFB + 200 POISSON, p = 0.1) whose weights
+    and delays are drawn from ranges by NetGen's rand_weight / rand_delay
+    (exc ranges 0.4-0.6 mV, inh -3 to -2 mV, in steps of DW = 0.05 mV;
+    delays 1.0-2.0 ms): unequal weights of one sign, the case whose fp32 sums
+    depend on the order of arrival.  (rand_weight draws downwards from a
+    positive floor, netgen.cpp:19-31, so the exc weights are 0.2-0.4 mV.)
 C3  lives in stdp_net.py (explicit synapse lists: all-to-all, one-to-one and
     all-but-self, per-projection plasticity).
 """
@@ -60,8 +66,19 @@ def c1_spec():
     return "\n".join(lines) + "\n"
 
 
+def c0r_spec():
+    lines = ["timestep 0.0001", "dw 0.00005", lif_line(*C0_LIF),
+             "pop 1600 LIFB 0", "pop 400 LIFB 0", "pop 200 POISSON 1"]
+    for src, (lo, hi) in ((2, (0.0004, 0.0006)), (0, (0.0004, 0.0006)), (1, (-0.003, -0.002))):
+        for t in (0, 1):
+            lines.append(f"conn {src} {t} {lo!r} {hi!r} 0.001 0.002 0.1 STATIC")
+    lines.append("rate 2 0.02")
+    return "\n".join(lines) + "\n"
+
+
 C0 = dict(spec=c0_spec(), mt=1, rnd=1, seed=1, v0=(0.0, 0.02, 11), lif=C0_LIF, seconds=1.0)
 C0_DRIVEN = dict(spec=c0_spec(rate=0.01), mt=2, rnd=2, seed=2, v0=(0.0, 0.02, 12), lif=C0_LIF, seconds=0.3)
+C0R = dict(spec=c0r_spec(), mt=4, rnd=4, seed=4, v0=(0.0, 0.02, 14), lif=C0_LIF, seconds=0.2)
 C1 = dict(spec=c1_spec(), mt=3, rnd=3, seed=3, v0=(0.0, 0.01, 13), lif=C1_LIF, seconds=10.0, rates_off=500)
 
 

@@ -74,6 +74,8 @@ def oracle():
     L.mgbo_create_fixed_indegree.argtypes = [vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp,
                                              vp, u64, u64, i32, i32, i32]
     L.mgbo_set_id_offset.argtypes = [vp, i32]
+    L.mgbo_set_fx.argtypes = [vp, i32]
+    L.mgbo_set_fx.restype = C.c_int
     L.mgbo_run.restype = C.c_int
     L.mgbo_run.argtypes = [vp, i64, vp, vp, i64, C.POINTER(i64)]
     L.mgbo_set_rates.argtypes = [vp, vp]
@@ -296,6 +298,11 @@ class OracleSim:
         r = np.ascontiguousarray(rate, np.float32)
         self.L.mgbo_set_rates(self.h, _p(r))
 
+    def set_fx(self, shift):
+        """Fixed-point accumulation with the CUDA core's shift (before the
+        first step): the core's order-independent sums, bit for bit."""
+        assert self.L.mgbo_set_fx(self.h, int(shift)) == 0
+
     def state(self):
         n, S = self.n, self.S
         out = {k: np.zeros(n, np.float64) for k in ("V", "Iexc", "Iinh")}
@@ -379,3 +386,47 @@ def rate_and_cv(counts, ids, n, steps, dt):
             isi = np.diff(sst[a:b]).astype(np.float64)
             cvs.append(isi.std() / isi.mean())
     return len(ids) / (n * steps * dt), (float(np.mean(cvs)) if cvs else 0.0), len(cvs)
+
+
+def fx_shift_for(bound, min_exp, exact):
+    """The fixed-point shift rule of the CUDA core's builder (build.cu,
+    fx_shift_for): the sums must fit 61 bits, and no finer than needed to make
+    every weight an exact multiple of 2^-shift."""
+    k = 0
+    if bound > 0.0:
+        e = int(np.frexp(np.float64(bound))[1])
+        k = 61 - e
+        if exact:
+            k = min(k, 24 - int(min_exp))
+    return max(-100, min(120, k))
+
+
+def fx_plan(net, stdp=False, plastic=None, wlim=0.0):
+    """(hetero, shift) of a synapse list as the core's builder computes them:
+    hetero when some target receives unequal weights of one sign (or weights
+    are plastic)."""
+    n = int(net["n"])
+    tar = np.asarray(net["tar"], np.int64)
+    w = np.asarray(net["weight"], np.float32)
+    pl = np.zeros(len(w), bool)
+    if stdp:
+        pl = np.ones(len(w), bool) if plastic is None else np.asarray(plastic) != 0
+    mag = np.abs(w.astype(np.float64))
+    mag = np.where(pl, np.maximum(mag, float(wlim)), mag)
+    bound = float(np.bincount(tar, weights=mag, minlength=n).max()) if len(w) else 0.0
+    nz = w[w != 0]
+    min_exp = int(np.frexp(nz)[1].min()) if len(nz) else 1 << 20
+    hetero = False
+    for sel in (w > 0, w <= 0):
+        if sel.any():
+            lo = np.full(n, np.inf)
+            hi = np.full(n, -np.inf)
+            np.minimum.at(lo, tar[sel], w[sel].astype(np.float64))
+            np.maximum.at(hi, tar[sel], w[sel].astype(np.float64))
+            hetero |= bool(np.any(hi > lo))
+    return hetero or bool(pl.any()), fx_shift_for(bound, min_exp, not pl.any())
+
+
+def equal_per_sign(w):
+    w = np.asarray(w)
+    return len(np.unique(w[w > 0])) <= 1 and len(np.unique(w[w <= 0])) <= 1

@@ -61,7 +61,7 @@ def test_rand_weight_subtracts_for_nonnegative_floor():
     assert net["weight"].max() <= np.float32(0.2) and net["weight"].min() < 0.0
 
 
-@pytest.mark.parametrize("cfg", ["C0", "C1"])
+@pytest.mark.parametrize("cfg", ["C0", "C1", "C0R"])
 def test_netgen_matches_reference_at_config_size(cfg, tmp_path):
     """The benchmark configurations at their stated sizes (C0: 1.1e7
     synapses; C1: 3.2e5): the oracle's gen_net against the reference's own

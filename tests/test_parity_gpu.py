@@ -2,7 +2,9 @@
 on the golden networks, through the C ABI.
 
 Bar: rasters (step and neuron id of every spike) and every fp32 state array
-bit-exact against the oracle's fp32 path; STDP weights within 1e-5
+bit-exact against the oracle's fp32 path, or against the oracle's
+fixed-point path where the core sums inputs in fixed point (networks in which
+some neuron receives unequal weights of one sign); STDP weights within 1e-5
 relative (CUDA expf vs the host libm expf)."""
 import numpy as np
 import pytest
@@ -44,8 +46,17 @@ MODES = {"push": mgb.MODE_PUSH, "auto": mgb.MODE_AUTO, "pull": mgb.MODE_PULL}
 @pytest.mark.parametrize("name", NAMES)
 def test_cuda_matches_oracle(name, mode):
     c, net, _ = load(name)
-    oc, oi, ost, osim = run_oracle(name)
     gc, gi, gst, gsim = run_cuda(name, MODES[mode])
+    info = gsim.info()
+    fixed = info["accumulation"] == mgb.ACC_FIXED
+    hetero, shift = T.fx_plan(net, stdp=bool(c["stdp"]), wlim=max(abs(T.default_stdpconst(net)[4]),
+                                                                   abs(T.default_stdpconst(net)[5])))
+    # fixed point exactly where some neuron gets unequal weights of one sign
+    # (or weights are plastic), except for the pull method
+    assert fixed == (hetero and info["mode"] != mgb.MODE_PULL)
+    if fixed:
+        assert info["fx_shift"] == shift
+    oc, oi, ost, osim = run_oracle(name, fx=info["fx_shift"] if fixed else None)
     if mode == "auto":
         expect_mode = mgb.MODE_PULL if c["stdp"] else mgb.MODE_DEFERRED
     else:
@@ -61,14 +72,10 @@ def test_cuda_matches_oracle(name, mode):
         np.testing.assert_allclose(w, ost["weight32"], rtol=W_RTOL, atol=1e-9)
         np.testing.assert_allclose(gst["V"], ost["V32"], rtol=W_RTOL, atol=1e-8)
     else:
-        wt = net["weight"]
-        if len(np.unique(wt[wt > 0])) <= 1 and len(np.unique(wt[wt <= 0])) <= 1:
-            # one weight per sign: every order of the fp32 input sums gives the same bits
-            assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
-        else:
-            # unequal weights of one sign: fp32 sums depend on the arrival order,
-            # which atomics (here and in the reference) leave open
-            np.testing.assert_allclose(gst["V"], ost["V32"], rtol=W_RTOL, atol=1e-8)
+        # one weight per sign: every order of the fp32 input sums gives the
+        # same bits; unequal weights: the order-independent fixed-point sums
+        # of the oracle's fixed-point path, bit for bit
+        assert np.array_equal(gst["V"].view(np.int32), ost["V32"].view(np.int32)), "V not bit-exact"
         assert np.array_equal(w, net["weight"])
     if gsim.info()["mode"] in (mgb.MODE_PUSH, mgb.MODE_PULL):
         assert gsim.info()["events"] == osim.events  # counted at emission
@@ -90,8 +97,13 @@ def test_cuda_matches_reference_kernels(name):
     if c["stdp"]:
         np.testing.assert_allclose(gst["V"], rst["V"], rtol=1e-5, atol=1e-9)
         np.testing.assert_allclose(gsim.weights(), rst["weight"], rtol=W_RTOL, atol=1e-9)
-    else:
+    elif T.equal_per_sign(net["weight"]):
         assert np.array_equal(gst["V"].view(np.int32), rst["V"].view(np.int32))
+    else:
+        # unequal weights of one sign: the reference's fp32 atomics add them in
+        # an order its scheduling decides, the core in fixed point exactly
+        assert gsim.info()["accumulation"] == mgb.ACC_FIXED
+        np.testing.assert_allclose(gst["V"], rst["V"], rtol=W_RTOL, atol=1e-8)
     for k in ("fire_cnt", "last_fired", "refrac"):
         assert np.array_equal(gst[k], rst[k]), k
 
@@ -102,9 +114,9 @@ def test_windowed_group_matches_reference_kernels(name):
     """The windowed step group (mgc_set_persistent mode 3, windows of up to 4
     steps) against the reference kernels' outputs: rasters and integer state
     bit-exact; V bit-exact with one weight per sign, else within 1e-5
-    relative (it adds a neuron's inputs of one step in another order than the
-    pipelined group, and with unequal weights of one sign fp32 sums depend on
-    that order)."""
+    relative of the reference (whose fp32 atomics leave the order of unequal
+    additions open) and bit-exact against the pipelined group (both sum
+    such inputs in fixed point)."""
     ref = ref_outputs(name)
     if ref is None:
         pytest.skip("no golden reference outputs for " + name)
@@ -121,11 +133,15 @@ def test_windowed_group_matches_reference_kernels(name):
     assert np.array_equal(gi, ri)
     for k in ("fire_cnt", "last_fired", "refrac"):
         assert np.array_equal(gst[k], rst[k]), k
-    wt = net["weight"]
-    if len(np.unique(wt[wt > 0])) <= 1 and len(np.unique(wt[wt <= 0])) <= 1:
+    if T.equal_per_sign(net["weight"]):
         assert np.array_equal(gst["V"].view(np.int32), rst["V"].view(np.int32))
     else:
         np.testing.assert_allclose(gst["V"], rst["V"], rtol=W_RTOL, atol=1e-8)
+        # the pipelined group gives the same bits (fixed-point sums do not
+        # depend on which warp adds which input)
+        pc, pi, pst, _ = run_cuda(name)
+        assert np.array_equal(pc, gc) and np.array_equal(pi, gi)
+        assert np.array_equal(pst["V"].view(np.int32), gst["V"].view(np.int32))
 
 
 @pytest.mark.gpu

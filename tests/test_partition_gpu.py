@@ -67,11 +67,17 @@ def test_explicit_partitions_equal_whole(name, parts, cap):
         assert s.first == first and s.n == count and s.n_src == net["n"]
         assert s.info()["mode"] == mgb.MODE_DEFERRED
     assert sum(s.S for s in sims) == len(net["src"])
+    # unequal weights of one sign: every partition sums in fixed point with
+    # the whole network's shift, so the merged state is the same bits
+    wi = whole.info()
+    for s in sims:
+        assert (s.info()["accumulation"], s.info()["fx_shift"]) == (wi["accumulation"], wi["fx_shift"])
+    assert wi["accumulation"] == (mgb.ACC_FLOAT if equal_weights(net["weight"]) else mgb.ACC_FIXED)
     g = PartitionGroup(sims, cap_per_step=cap)   # exact exchange, or the device one with 64 ids per step
     g.run(700)
     g.run(1300)
     g.sync()
-    compare(whole, g, equal_weights(net["weight"]))
+    compare(whole, g, True)
 
 
 def fixed(w, **kw):
