@@ -17,8 +17,10 @@ POISSON rates copied from pinned host memory and the raster read back every
 bench step.  The CSR (8.8 GB) is larger than L2, so no flush is needed.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-With N > 1 every rank advances its own independent instance (replicas);
-value is the sum over ranks divided by the slowest rank's time.
+With N > 1 the network is split into one contiguous neuron range per rank
+(strong scaling; spike ids all-gathered through NCCL every min_delay - 1
+steps); --workload replicas runs N independent instances instead (weak
+scaling).  value is the total over ranks divided by the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -465,6 +467,19 @@ def run_ours(a, ws, rank, local):
                   "neuron_update_avg_us": 1e3 * kmd[0] / 500,
                   "whole_step_frac_of_reduction_ceiling": dev / (dms / 1e3) / ws / red_ceiling}
         simd.close()
+        # the same driven network with its inputs summed in 64-bit fixed
+        # point (what a network with unequal weights of one sign runs):
+        # the cost of order-independent sums
+        simf = make_sim(wd, local, seed=1 + rank, record=False)
+        simf.set_accumulation(mgb.ACC_FIXED)
+        simf.autotune(steps_per_trial=640)
+        simf.run(CHUNK // 2)
+        simf.sync()
+        fms, fev, _ = timed_device(simf, CHUNK, 1, ws)
+        fms, fev = allmax(ws, fms), allsum(ws, fev)
+        driven["fixed_point"] = {"events_per_s": fev / (fms / 1e3), "sim_s_per_wall_s": CHUNK * DT / (fms / 1e3),
+                                 "step_group": simf.info()["persistent"], "fx_shift": simf.info()["fx_shift"]}
+        simf.close()
 
     cpu = parity = None
     if rank == 0 and not a.no_cpu:
@@ -548,18 +563,56 @@ def run_partition(a, ws, rank, local):
     sim.sync()   # raises if an exchange window was refused (the run would miss spikes)
     ms = allmax(ws, e0.elapsed_time(e1))
     events = allsum(ws, sim.info()["events"] - ev0)
-    line = {"workload": "partition", "metric": METRIC, "value": events / (ms / 1e3), "unit": "events/s",
+    launches = sim.kernel_launches
+    hbm, peak_kind = peaks()
+    # the dominant kernel's algorithmic bytes over the timed region: 24 B per
+    # LIFB neuron-step of this partition plus 8 B per delivered event
+    lif_here = max(0, min(first + count, w["n_lif"]) - first)
+    steps_timed = a.steps * CHUNK
+    dbytes = 24.0 * lif_here * steps_timed + 8.0 * (events / ws)
+    achieved = allmax(ws, dbytes / (ms / 1e3) / 1e9) if ms > 0 else 0.0
+    # end to end through the C ABI: each bench step the rates from pinned
+    # host memory, the steps with their exchanges, the fire counts read back
+    pinned = torch.empty(count, dtype=torch.float32, pin_memory=True)
+    pinned.numpy()[:] = w["rate"][first:first + count]
+    import ctypes as C
+    L = mgb.lib()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ev_e = sim.info()["events"]
+    t0 = time.perf_counter()
+    for _ in range(a.e2e_steps):
+        mgb.capi.check(L.mgc_set_rates(sim._h, C.c_void_p(pinned.data_ptr()), count))
+        part.run(CHUNK)
+        fc = sim.state()["fire_cnt"]
+    sim.sync()
+    e2e_s = allmax(ws, time.perf_counter() - t0)
+    e2e_ev = allsum(ws, sim.info()["events"] - ev_e)
+    line = {"metric": METRIC, "value": events / (ms / 1e3), "unit": "events/s",
             "n_gpus": ws, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
-            "scaling": "strong", "window_steps": part.window,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded, generated on the device)",
+            "config": {"workload": "large Brunel: 1M LIFB (800k/200k) + 100k POISSON @20 Hz, fixed in-degree "
+                                   "800/200/100, J 0.1 mV, g 5, delays U{10..50} steps, dt 0.1 ms, split into "
+                                   "one contiguous neuron range per GPU",
+                       "scale": a.scale, "bench_step": "1 s simulated (10,000 timesteps)",
+                       "l2": "inputs larger than L2 (8.8 GB CSR)",
+                       "parallelism": f"partitions x{ws} (spike ids all-gathered every {part.window} steps)"},
             "sim_s_per_wall_s": a.steps * CHUNK * DT / (ms / 1e3), "build_s": build_s,
+            "window_steps": part.window,
             "partition": {"first": first, "neurons": count, "synapses": sim.S},
             "exchange": ("none (one partition)" if ws == 1 else
                          "NCCL all-gather of counts, then of ids (host waits)" if cap is None else
                          f"NCCL all-gather of fixed buffers on the stream, {cap} ids per step"),
-            "clocks": clk.summary()}
+            "roofline": {"bound": "hbm", "kernel": "step groups of the partition", "achieved": achieved,
+                         "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None},
+            "e2e": {"value": e2e_ev / e2e_s, "unit": "events/s", "h2d_bytes_per_step": 4 * count,
+                    "d2h_bytes_per_step": 4 * count},
+            "gpu_launches": int(launches), "cpu_baseline": None, "clocks": clk.summary()}
     if ws == 1:
         whole = make_sim(w, local, seed=1, record=False)
-        whole.run(CHUNK * (a.warmup + a.steps))
+        whole.run(CHUNK * (a.warmup + a.steps + a.e2e_steps))
         ws_ = whole.state()
         st = sim.state()
         line["identical_to_whole"] = bool(np.array_equal(st["V"].view(np.int32), ws_["V"].view(np.int32)) and
@@ -885,7 +938,8 @@ def main():
                     help="skip the reference's own kernels on this GPU (reference_gpu key)")
     ap.add_argument("--ref-syn", type=float, default=1e8)
     ap.add_argument("--ref-seconds", type=float, default=1.0)
-    ap.add_argument("--workload", default="brunel1m", choices=["brunel1m", "sweep", "sched", "refgpu", "partition"],
+    ap.add_argument("--workload", default="brunel1m",
+                    choices=["brunel1m", "replicas", "sweep", "sched", "refgpu", "partition"],
                     help="brunel1m: the 1M-neuron network (default); sweep: batched vs plain "
                          "parameter sweep; sched: the step scheduler's modes on a periodic drive; refgpu: "
                          "the reference's own simulator and this core on the reference's benchmark network; "
@@ -905,9 +959,13 @@ def main():
                     help="only build the network at --scale, run --warmup bench steps, 300 "
                          "steps as timed, and 300 profiled steps (separate kernels); for ncu captures")
     a = ap.parse_args()
-    ws, rank, local = dist_init("nccl" if a.workload == "partition" and a.impl == "ours" else "gloo")
+    multi = int(os.environ.get("WORLD_SIZE", "1")) > 1
+    split = a.impl == "ours" and (a.workload == "partition" or (a.workload == "brunel1m" and multi))
+    ws, rank, local = dist_init("nccl" if split else "gloo")
     try:
-        if a.workload == "partition" and a.impl == "ours":
+        if split:
+            # several GPUs: the one network split over them (strong scaling);
+            # independent replicas with --workload replicas
             run_partition(a, ws, rank, local)
         elif a.workload == "sweep":
             run_sweep(a, ws, rank, local)
@@ -927,7 +985,7 @@ def main():
         elif a.impl == "reference":
             run_reference(a, ws, rank)
         else:
-            run_ours(a, ws, rank, local)
+            run_ours(a, ws, rank, local)   # one GPU, or --workload replicas
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -64,6 +64,11 @@ public:
     // at least NETGEN_PARALLEL_PAIRS pairs; the network is the same
     static int NETGEN_THREADS;
     static long long NETGEN_PARALLEL_PAIRS;
+    // addition: NetGen::gen_net records the projections instead of listing
+    // the synapses on the host, and MGSimulator generates them on the device
+    // (mgc_create_generated): the same network, without the host synapse
+    // list (Network::recipe)
+    static bool DEVICE_NETGEN;
 
     static void set_timestep(real time_step)
     {
@@ -95,6 +100,7 @@ public:
         NETGEN_PARALLEL_PAIRS = min_pairs;
     }
     static void throw_on_error(bool on) { THROW_ON_ERROR = on; }
+    static void enable_device_netgen(bool on = true) { DEVICE_NETGEN = on; }
     // With STDP on, the reference updates every synapse (mgcore.cu:365-412)
     // whatever its projection's SynapseType; this restricts it to STDP ones.
     static void enable_stdp_by_type()

@@ -22,6 +22,10 @@
 // needs the partition's neurons to be consecutive ids (SIMPLE and BSIM
 // partitions are), static weights and a minimum delay >= 2; otherwise the
 // network runs as one handle and a line on stderr says why.
+//
+// A Network that NetGen::gen_net recorded under Config::DEVICE_NETGEN (no
+// host synapse list, Network::recipe) is generated on the device
+// (mgc_create_generated) and runs as one handle.
 #pragma once
 #include <cstdint>
 #include <stdexcept>
@@ -63,6 +67,7 @@ class MGSimulator {
     std::vector<int> raster_ids;
     bool raster_complete = true;
     void check(int status, const char* what);
+    void build_generated(Network& net);
     void drain_raster();
     void exchange(int steps);
     real get_firing_rate(real time);

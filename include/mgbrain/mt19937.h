@@ -47,6 +47,12 @@ public:
     // this ^= o, word by word in logical order (linear combination of states)
     void add(const Mt19937& o);
     void clear();
+    // The state in logical order: out[k] = the word the (k+1)-th next step
+    // replaces, so that the next 624 outputs are those of one block twist of
+    // out[0..623] (624 words).
+    void state_words(uint32_t* out) const;
+    // The state from words in that order (ring position 0).
+    void set_state_words(const uint32_t* in);
 
 private:
     static uint32_t temper(uint32_t y)
@@ -68,9 +74,12 @@ public:
     uint64_t steps() const { return steps_; }
     // g advanced by steps() outputs
     void apply(Mt19937& g) const;
+    // the jump by 2 * steps() outputs (x^(2J) = (x^J)^2 mod phi)
+    MtJump doubled() const;
 
 private:
-    uint64_t steps_;
+    MtJump() = default;
+    uint64_t steps_ = 0;
     std::vector<uint64_t> poly_;
 };
 

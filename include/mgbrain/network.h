@@ -57,6 +57,30 @@ public:
     // projections should gate plasticity; empty means Config::STDP decides
     // for every synapse, as the reference does.
     std::vector<unsigned char> plastic;
+    // addition: with Config::DEVICE_NETGEN, gen_net leaves `synapses` and the
+    // neurons' nxt/pre/syns lists empty and records here what MGSimulator
+    // generates on the device: the projections in gen_net's order, NetGen's
+    // mt19937 before the first (its 624 words in logical order), and the
+    // weights and delays (in steps) gen_net draws with rand() for ranged
+    // projections, in synapse order.
+    struct GenProjection {
+        int src = 0, tar = 0;     // population indices
+        int rule = 0;             // mgc_gen_proj rule (MGC_RULE_*)
+        float prob = 0.0f;
+        int k = 0;
+        unsigned long long seed = 1;
+        real weight = 0;
+        int delay = 1, delay_max = 1;  // steps
+        std::vector<real> weights;     // empty: every synapse has `weight`
+        std::vector<int> delays;       // empty: every synapse has `delay`
+        bool plastic = false;
+    };
+    struct GenRecipe {
+        bool active = false;
+        std::vector<GenProjection> projs;
+        std::array<uint32_t, 624> mt{};
+        long long synapses = 0;
+    } recipe;
 };
 
 }  // namespace MGBrain

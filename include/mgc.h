@@ -162,6 +162,79 @@ mgc_status mgc_create(const mgc_net_desc* desc, mgc_sim** out);
  * cannot express a fixed in-degree). */
 mgc_status mgc_create_fixed_indegree(const mgc_fixed_indegree_desc* desc, mgc_sim** out);
 
+/* ---- Network generation on the device by NetGen's rules ------------------
+ * The synapses NetGen::gen_net (src/model/netgen.cpp:39-229) would make,
+ * generated on the device and turned into the CSR there: no host synapse
+ * list (the reference's gen_net is an O(sn*tn) host loop that also keeps
+ * about 90 bytes per synapse in host memory).  Populations occupy
+ * consecutive ids in population order, as gen_net assigns them; projections
+ * are generated in order, each synapse in the rule's order, so the synapse
+ * list (mgc_read_weights order) is gen_net's.  Rules:
+ *   MGC_RULE_PROB  the fixed-probability rule (netgen.cpp:169-186): pair k of
+ *                  the row-major sn x tn pairs is taken, while fewer than
+ *                  gen_num = round(float(sn*tn) * prob) are taken, when the
+ *                  k-th output of NetGen's mt19937 modulo sn*tn is below
+ *                  gen_num * 1.1; list slots left over are pair (0, 0).  The
+ *                  candidate pairs are cut into stretches generated at once,
+ *                  each from the generator jumped ahead to its start.
+ *   MGC_RULE_ALL   every pair (m, n), row-major (ctype 1).
+ *   MGC_RULE_ONE   pairs (k, k), k < sn (ctype 0).
+ *   MGC_RULE_ALL_BUT_SELF  every pair with m != n, row-major (no reference
+ *                  counterpart; Model::connect_all_but_self).
+ *   MGC_RULE_FIXED_INDEGREE  k sources per target drawn as by
+ *                  mgc_create_fixed_indegree with counter (target, draw,
+ *                  projection index) (Model::connect_fixed_indegree).
+ * Weights and delays: one value per projection, or (ranges, which NetGen
+ * draws with glibc rand() in synapse order, netgen.cpp:19-38) host arrays
+ * of the projection's synapses in order, drawn by the caller.  The shuffle
+ * placement (Config::SHUFFLE_GEN) stays on the host. */
+enum { MGC_RULE_PROB = 0, MGC_RULE_ALL = 1, MGC_RULE_ONE = 2, MGC_RULE_ALL_BUT_SELF = 3,
+       MGC_RULE_FIXED_INDEGREE = 4 };
+
+typedef struct mgc_gen_proj {
+    int32_t src, tar;          /* population indices */
+    int32_t rule;              /* MGC_RULE_* */
+    float prob;                /* MGC_RULE_PROB: Projection::ctype */
+    int32_t k;                 /* MGC_RULE_FIXED_INDEGREE: sources per target */
+    uint64_t conn_seed;        /* MGC_RULE_FIXED_INDEGREE: key of its draws */
+    float weight;              /* every synapse's weight when weights is NULL */
+    int32_t delay;             /* delay in steps when delays is NULL (FIXED_INDEGREE: the least) */
+    int32_t delay_max;         /* MGC_RULE_FIXED_INDEGREE: delays uniform in [delay, delay_max] */
+    const float* weights;      /* host [mgc_gen_count] weights in synapse order, or NULL */
+    const int32_t* delays;     /* host [mgc_gen_count] delays in steps, or NULL */
+    int32_t plastic;           /* the projection's synapses learn (with stdp) */
+} mgc_gen_proj;
+
+typedef struct mgc_gen_desc {
+    int32_t n_pops;
+    const int32_t* pop_num;    /* [n_pops] neurons */
+    const int8_t* pop_type;    /* [n_pops] NeuronType */
+    int32_t n_proj;
+    const mgc_gen_proj* proj;  /* [n_proj], in gen_net's order */
+    uint32_t mt_state[624];    /* NetGen's mt19937 before the first projection, in logical
+                                  order: the next 624 outputs are one twist of these words
+                                  (a freshly seeded generator: its seeding words as they are) */
+    uint32_t* mt_state_out;    /* [624] or NULL: the generator after the network, same order */
+    const float* rate;         /* [n] or NULL */
+    const float* v_init;       /* [n] or NULL */
+    float lifconst[30];
+    float stdpconst[6];
+    int32_t stdp;
+    int32_t mode;
+    uint64_t seed;
+    int32_t device;
+    int64_t raster_steps;
+    int64_t raster_ids;
+} mgc_gen_desc;
+
+/* Builds the network of `desc` on the device (see above); everything else
+ * as mgc_create.  Fails with MGC_ERR_INVALID for more than 2^31-1 synapses. */
+mgc_status mgc_create_generated(const mgc_gen_desc* desc, mgc_sim** out);
+
+/* Synapses projection r of desc generates (the length of its weights and
+ * delays arrays), or -1 for a bad projection. */
+int64_t mgc_gen_count(const mgc_gen_desc* desc, int32_t r);
+
 /* Many independent fixed in-degree networks advanced together in one
  * handle (a parameter sweep).  Block b's neurons occupy ids
  * [start_b, start_b + n_b), start_b = sizes of the blocks before it; its
@@ -315,7 +388,8 @@ mgc_status mgc_get_info(mgc_sim* sim, mgc_info* info);
 /* Runs `steps` steps with each kernel class bracketed by CUDA events (the
  * steps and their event records are captured in batches of 64 as CUDA
  * graphs, so the kernels run back to back as in mgc_run): ms[0] neuron
- * update, ms[1] event delivery, ms[2] STDP, summed over the steps.  No reference counterpart (the
+ * update, ms[1] event delivery (with STDP, which runs inside the push or
+ * the pull), ms[2] 0 (kept for the layout), summed over the steps.  No reference counterpart (the
  * reference was profiled externally with nvprof, shell/single.sh:15). */
 mgc_status mgc_profile_steps(mgc_sim* sim, int64_t steps, float* ms);
 

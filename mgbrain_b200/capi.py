@@ -23,6 +23,7 @@ RAW, LIF0, POISSON, LIF, LIFE, LIFB = range(6)
 MODE_AUTO, MODE_PUSH, MODE_DEFERRED, MODE_PULL = 0, 1, 2, 3
 SCHED_STATIC, SCHED_THRESHOLD, SCHED_LEARNED = 0, 1, 2
 ACC_FLOAT, ACC_FIXED = 0, 1
+RULE_PROB, RULE_ALL, RULE_ONE, RULE_ALL_BUT_SELF, RULE_FIXED_INDEGREE = range(5)
 MLP_IN, MLP_HIDDEN, MLP_OUT, MLP_PARAMS = 20, 32, 5, 837
 
 EXPORTED = (
@@ -36,6 +37,7 @@ EXPORTED = (
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
     "mgc_fault_inject_alloc", "mgc_selftest_wait_timeout", "mgc_partition_stats", "mgc_part_export_dev",
     "mgc_part_import_dev", "mgc_raster_stage", "mgc_raster_collect", "mgc_set_accumulation",
+    "mgc_create_generated", "mgc_gen_count",
 )
 
 
@@ -67,6 +69,34 @@ class FixedInDegreeDesc(C.Structure):
         ("raster_steps", C.c_int64), ("raster_ids", C.c_int64), ("id_offset", C.c_int32),
         ("proj_offset", C.c_int32),
     ]
+
+
+class GenProj(C.Structure):
+    _fields_ = [
+        ("src", C.c_int32), ("tar", C.c_int32), ("rule", C.c_int32), ("prob", C.c_float), ("k", C.c_int32),
+        ("conn_seed", C.c_uint64), ("weight", C.c_float), ("delay", C.c_int32), ("delay_max", C.c_int32),
+        ("weights", C.c_void_p), ("delays", C.c_void_p), ("plastic", C.c_int32),
+    ]
+
+
+class GenDesc(C.Structure):
+    _fields_ = [
+        ("n_pops", C.c_int32), ("pop_num", C.c_void_p), ("pop_type", C.c_void_p), ("n_proj", C.c_int32),
+        ("proj", C.c_void_p), ("mt_state", C.c_uint32 * 624), ("mt_state_out", C.c_void_p),
+        ("rate", C.c_void_p), ("v_init", C.c_void_p), ("lifconst", C.c_float * 30), ("stdpconst", C.c_float * 6),
+        ("stdp", C.c_int32), ("mode", C.c_int32), ("seed", C.c_uint64), ("device", C.c_int32),
+        ("raster_steps", C.c_int64), ("raster_ids", C.c_int64),
+    ]
+
+
+def mt19937_seed_words(seed):
+    """The 624 words of MT19937 seeded with `seed` (Matsumoto and Nishimura's
+    initialisation, as std::mt19937(seed) does), in the order mgc_gen_desc
+    takes them."""
+    x = [int(seed) & 0xFFFFFFFF]
+    for k in range(1, 624):
+        x.append((1812433253 * (x[-1] ^ (x[-1] >> 30)) + k) & 0xFFFFFFFF)
+    return x
 
 
 class TuneReport(C.Structure):
@@ -160,6 +190,10 @@ def lib():
     L.mgc_set_persistent.restype = C.c_int
     L.mgc_set_window.argtypes = [vp, i32]
     L.mgc_set_window.restype = C.c_int
+    L.mgc_create_generated.argtypes = [C.POINTER(GenDesc), C.POINTER(vp)]
+    L.mgc_create_generated.restype = C.c_int
+    L.mgc_gen_count.argtypes = [C.POINTER(GenDesc), i32]
+    L.mgc_gen_count.restype = i64
     L.mgc_set_accumulation.argtypes = [vp, i32]
     L.mgc_set_accumulation.restype = C.c_int
     L.mgc_checkpoint_size.argtypes = [vp, C.POINTER(i64)]
@@ -330,6 +364,61 @@ class Simulator:
             return cls._partition(h.value)
         check(lib().mgc_create_fixed_indegree(C.byref(d), C.byref(h)))
         return cls(h.value, n, S)
+
+    @classmethod
+    def generated(cls, pops, projs, lifconst, mt_seed=None, mt_state=None, stdpconst=None, rate=None,
+                  v_init=None, stdp=False, seed=1, device=0, mode=MODE_AUTO, raster_steps=0, raster_ids=0,
+                  state_out=None):
+        """The network NetGen's rules make, generated on the device
+        (mgc_create_generated).  pops: list of (num, type); projs: dicts with
+        src, tar, rule and prob / k, conn_seed, weight or weights (array in
+        synapse order), delay (steps) or delays (array), delay_max, plastic.
+        mt_seed seeds NetGen's mt19937 (or mt_state gives its 624 words);
+        state_out: a list that receives the generator's words afterwards."""
+        keep = []
+        P = list(pops)
+        pn = np.array([p[0] for p in P], np.int32)
+        pt = np.array([p[1] for p in P], np.int8)
+        arr = (GenProj * max(1, len(projs)))()
+        for i, r in enumerate(projs):
+            g = arr[i]
+            g.src, g.tar, g.rule = int(r["src"]), int(r["tar"]), int(r["rule"])
+            g.prob, g.k, g.conn_seed = float(r.get("prob", 0.0)), int(r.get("k", 0)), int(r.get("conn_seed", 1))
+            g.weight, g.delay = float(r.get("weight", 0.0)), int(r.get("delay", 1))
+            g.delay_max, g.plastic = int(r.get("delay_max", r.get("delay", 1))), int(bool(r.get("plastic", 0)))
+            if r.get("weights") is not None:
+                w = np.ascontiguousarray(r["weights"], np.float32)
+                keep.append(w)
+                g.weights = _ptr(w)
+            if r.get("delays") is not None:
+                dl = np.ascontiguousarray(r["delays"], np.int32)
+                keep.append(dl)
+                g.delays = _ptr(dl)
+        d = GenDesc()
+        d.n_pops, d.pop_num, d.pop_type = len(P), _ptr(pn), _ptr(pt)
+        d.n_proj, d.proj = len(projs), C.cast(arr, C.c_void_p)
+        words = mt_state if mt_state is not None else mt19937_seed_words(5489 if mt_seed is None else mt_seed)
+        d.mt_state[:] = [int(x) & 0xFFFFFFFF for x in words]
+        out_words = (C.c_uint32 * 624)()
+        d.mt_state_out = C.cast(out_words, C.c_void_p)
+        rate_a = None if rate is None else np.ascontiguousarray(rate, np.float32)
+        v0_a = None if v_init is None else np.ascontiguousarray(v_init, np.float32)
+        d.rate, d.v_init = _ptr(rate_a), _ptr(v0_a)
+        d.lifconst[:] = [float(x) for x in np.asarray(lifconst, np.float32)]
+        sc = np.asarray(stdpconst if stdpconst is not None else [0.1, -0.01, 17, 34, 40, 0], np.float32)
+        d.stdpconst[:] = [float(x) for x in sc]
+        d.stdp, d.mode, d.seed, d.device = int(bool(stdp)), int(mode), int(seed), int(device)
+        d.raster_steps, d.raster_ids = int(raster_steps), int(raster_ids)
+        counts = [int(lib().mgc_gen_count(C.byref(d), i)) for i in range(len(projs))]
+        for i, r in enumerate(projs):
+            for key in ("weights", "delays"):
+                if r.get(key) is not None and len(r[key]) != counts[i]:
+                    raise ValueError(f"projection {i}: {key} holds {len(r[key])}, the rule makes {counts[i]}")
+        h = C.c_void_p()
+        check(lib().mgc_create_generated(C.byref(d), C.byref(h)))
+        if state_out is not None:
+            state_out[:] = list(out_words)
+        return cls(h.value, int(pn.sum()), int(sum(counts)))
 
     @classmethod
     def batch(cls, blocks, lifconst, seed=1, device=0, mode=MODE_AUTO, raster_steps=0, raster_ids=0):

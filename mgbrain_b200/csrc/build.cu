@@ -433,7 +433,7 @@ mgc_status finish_build(mgc_sim* s)
         CKS(s->alloc(&a.ring_e, (size_t)s->M * a.ns * words));
         CKS(s->alloc(&a.ring_i, (size_t)s->M * a.ns * words));
         CKS(s->alloc(&a.spk, s->n));
-        if (a.pull) {
+        if (a.pull || s->stdp) {  // this step's spikes as a bitmap (the pull, the ring STDP's incoming side)
             const int64_t groups = a.ns / 4;
             CKS(s->alloc(&a.fired_bits, (size_t)((groups + 31) / 32) * 4));
         }
@@ -630,8 +630,6 @@ mgc_status launch_shapes(mgc_sim* s)
     } else {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, push_kernel(s), kPushBlock, 0));
         s->push_grid = sms * std::max(1, occ);
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, stdp_kernel(s), kPushBlock, 0));
-        s->stdp_grid = sms * std::max(1, occ);
         if (a.pull) {
             CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pull_kernel(s), kPushBlock, 0));
             s->pull_grid = sms * std::max(1, occ);
@@ -653,6 +651,141 @@ void set_chunking(StepArgs& a, int64_t gap, int64_t target)
     len = (len + 31) / 32 * 32;
     a.bucket_chunks = (int32_t)ch;
     a.chunk_len = (int32_t)len;
+}
+
+// Construction steps for the other builders (netgen.cu): the neuron arrays,
+// the method (with the fixed-point plan), and the shared tail.
+mgc_status build_neurons(mgc_sim* s, int32_t n, const int8_t* type, const float* rate, const float* v_init,
+                         const float* lifc, const float* stdpc, uint64_t seed, int64_t raster_steps,
+                         int64_t raster_ids)
+{
+    return init_common(s, n, type, rate, v_init, lifc, stdpc, seed, raster_steps, raster_ids);
+}
+
+mgc_status build_method(mgc_sim* s, int requested, bool hetero, int32_t fx_shift)
+{
+    CKS(check_tbits(s));
+    CKS(choose_mode(s, requested));
+    apply_fx(s, FxPlan{hetero, fx_shift});
+    return MGC_OK;
+}
+
+int32_t fx_shift_rule(double bound, int min_exp, bool exact) { return fx_shift_for(bound, min_exp, exact); }
+
+mgc_status build_set_fx(mgc_sim* s, bool hetero, int32_t fx_shift)
+{
+    apply_fx(s, FxPlan{hetero, fx_shift});
+    return MGC_OK;
+}
+
+mgc_status build_finish(mgc_sim* s) { return finish_build(s); }
+
+// The CSR (and the method's extra layouts) of a network handed over as a
+// device-resident synapse list in synapse-list order: sources, targets,
+// weights, delays in steps and (STDP) plasticity flags (or null).  The
+// builders call begin_list_layout once the method is chosen, then this.
+mgc_status begin_list_layout(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    CKS(begin_layout(s));
+    uint2* syn;
+    CKS(s->alloc(&syn, s->S, false));
+    a.syn = syn;
+    a.n_syn = s->S;
+    CKS(s->alloc(&s->csr_syn64, s->S, false));
+    return MGC_OK;
+}
+
+mgc_status csr_from_list(mgc_sim* s, int32_t* src, int32_t* tar, float* w, int32_t* dl, uint8_t* pl)
+{
+    StepArgs& a = s->a;
+    const int64_t S = s->S;
+    const int dbits = sort_dbits(s);
+    uint2* syn = a.syn;
+    DevTmp t_keys2;
+    uint32_t* keys2 = nullptr;
+    {
+        DevTmp t_keys, t_vals, t_order, t_bad;
+        int32_t* bad;
+        uint32_t *keys, *vals, *order;
+        CKS(tmp_alloc(t_bad, &bad, 1));
+        CK(cudaMemsetAsync(bad, 0, 4, s->stream));
+        k_validate<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, s->n_src, s->n, 1 << (32 - a.tbits), bad);
+        int32_t hbad = 0;
+        CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        if (hbad) return fail(MGC_ERR_INVALID, "synapse with out-of-range source, target or delay");
+        if (a.pull) {
+            const int db = s->dmax > s->dmin ? bits_for(s->dmax - s->dmin + 1) : 0;
+            DevTmp t_k64a, t_k64b, t_v, t_o;
+            uint64_t *k64a, *k64b;
+            uint32_t *pv, *po;
+            CKS(tmp_alloc(t_k64a, &k64a, S));
+            CKS(tmp_alloc(t_k64b, &k64b, S));
+            CKS(tmp_alloc(t_v, &pv, S));
+            CKS(tmp_alloc(t_o, &po, S));
+            k_pull_keys<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, a.tbits, db, s->dmin, k64a, pv);
+            CKS(sort_pairs(k64a, k64b, pv, po, S, 2 * a.tbits + db, s->stream));
+            int64_t* in_ptr;
+            uint2* in_ent;
+            uint8_t* in_pl = nullptr;
+            CKS(s->alloc(&in_ptr, (size_t)s->n + 1));
+            CKS(s->alloc(&in_ent, S, false));
+            CKS(s->alloc(&s->in_syn64, S, false));
+            if (s->stdp && pl) CKS(s->alloc(&in_pl, S, false));
+            k_gather_pull<<<grid_for(S), 256, 0, s->stream>>>(po, src, w, dl, pl, S, a.tbits, in_ent, s->in_syn64,
+                                                               in_pl);
+            uint32_t* tkeys = reinterpret_cast<uint32_t*>(pv);
+            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, tkeys);
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(tkeys, S, 0, in_ptr);
+            CKS(exclusive_scan(in_ptr, s->n, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+            a.in_ptr = in_ptr;
+            a.in_ent = in_ent;
+            a.in_plastic = in_pl;
+        }
+        // CSR by source (and delay bucket), synapse-list order inside (stable)
+        CKS(tmp_alloc(t_keys, &keys, S));
+        CKS(tmp_alloc(t_vals, &vals, S));
+        CKS(tmp_alloc(t_order, &order, S));
+        CKS(tmp_alloc(t_keys2, &keys2, S));
+        k_explicit_keys<<<grid_for(S), 256, 0, s->stream>>>(src, dl, S, dbits, s->dmin, keys, vals);
+        CKS(sort_pairs(keys, keys2, vals, order, S, s->sbits + dbits, s->stream));
+        int32_t* csr_src = nullptr;
+        uint8_t* plastic = nullptr;
+        if (s->stdp && !a.pull) {
+            CKS(s->alloc(&csr_src, S, false));
+            if (pl) CKS(s->alloc(&plastic, S, false));
+        }
+        k_gather_explicit<<<grid_for(S), 256, 0, s->stream>>>(order, keys2, dbits, tar, w, dl, pl, S, a.tbits, syn,
+                                                               s->csr_syn64, csr_src, plastic);
+        a.csr_src = csr_src;
+        a.plastic = plastic;
+        if (s->stdp && !a.pull) {
+            // incoming lists: CSR positions sorted by target, synapse-list order
+            int64_t* dend_off;
+            int64_t* dend_pos;
+            CKS(s->alloc(&dend_off, (size_t)s->n + 1));
+            CKS(s->alloc(&dend_pos, S, false));
+            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, keys);
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(keys, S, 0, dend_off);
+            CKS(exclusive_scan(dend_off, s->n, s->stream));
+            k_inverse<<<grid_for(S), 256, 0, s->stream>>>(s->csr_syn64, S, vals);  // vals := pos_of
+            uint32_t* keys_out = reinterpret_cast<uint32_t*>(src);  // src is no longer needed
+            CKS(sort_pairs(keys, keys_out, vals, order, S, a.tbits, s->stream));
+            k_widen<<<grid_for(S), 256, 0, s->stream>>>(order, S, dend_pos);
+            a.dend_off = dend_off;
+            a.dend_pos = dend_pos;
+            int64_t max_in = 0;
+            CK(cudaStreamSynchronize(s->stream));
+            CKS(max_row(dend_off, s->n, &max_in));
+            a.chunks_in_per_spike = (int32_t)std::max<int64_t>(1, (max_in + kChunk - 1) / kChunk);
+        }
+        count_keys(s, keys2, S);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    return MGC_OK;
 }
 
 
@@ -764,26 +897,16 @@ mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim*
                           ? part->fx
                           : fx_plan_list(s->n, S, d->syn_tar, d->syn_weight, d->syn_plastic, s->stdp,
                                          std::max(std::fabs(d->stdpconst[4]), std::fabs(d->stdpconst[5]))));
-    const int dbits = sort_dbits(s.get());
-    CKS(begin_layout(s.get()));
-    uint2* syn;
-    CKS(s->alloc(&syn, S, false));
-    a.syn = syn;
-    a.n_syn = S;
-    CKS(s->alloc(&s->csr_syn64, S, false));
-    DevTmp t_keys2;
-    uint32_t* keys2 = nullptr;
+    CKS(begin_list_layout(s.get()));
     if (S > 0) {
-        DevTmp t_src, t_tar, t_w, t_d, t_pl, t_keys, t_vals, t_order, t_bad;
-        int32_t *src, *tar, *dl, *bad;
+        DevTmp t_src, t_tar, t_w, t_d, t_pl;
+        int32_t *src, *tar, *dl;
         float* w;
         uint8_t* pl = nullptr;
-        uint32_t *keys, *vals, *order;
         CKS(tmp_alloc(t_src, &src, S));
         CKS(tmp_alloc(t_tar, &tar, S));
         CKS(tmp_alloc(t_w, &w, S));
         CKS(tmp_alloc(t_d, &dl, S));
-        CKS(tmp_alloc(t_bad, &bad, 1));
         CK(cudaMemcpyAsync(src, d->syn_src, 4 * S, cudaMemcpyHostToDevice, s->stream));
         CK(cudaMemcpyAsync(tar, d->syn_tar, 4 * S, cudaMemcpyHostToDevice, s->stream));
         CK(cudaMemcpyAsync(w, d->syn_weight, 4 * S, cudaMemcpyHostToDevice, s->stream));
@@ -792,77 +915,7 @@ mgc_status create_explicit(const mgc_net_desc* d, const PartSpec* part, mgc_sim*
             CKS(tmp_alloc(t_pl, &pl, S));
             CK(cudaMemcpyAsync(pl, d->syn_plastic, S, cudaMemcpyHostToDevice, s->stream));
         }
-        CK(cudaMemsetAsync(bad, 0, 4, s->stream));
-        k_validate<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, s->n_src, s->n, 1 << (32 - a.tbits), bad);
-        int32_t hbad = 0;
-        CK(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaStreamSynchronize(s->stream));
-        if (hbad) return fail(MGC_ERR_INVALID, "synapse with out-of-range source, target or delay");
-        if (a.pull) {
-            const int db = s->dmax > s->dmin ? bits_for(s->dmax - s->dmin + 1) : 0;
-            DevTmp t_k64a, t_k64b, t_v, t_o;
-            uint64_t *k64a, *k64b;
-            uint32_t *pv, *po;
-            CKS(tmp_alloc(t_k64a, &k64a, S));
-            CKS(tmp_alloc(t_k64b, &k64b, S));
-            CKS(tmp_alloc(t_v, &pv, S));
-            CKS(tmp_alloc(t_o, &po, S));
-            k_pull_keys<<<grid_for(S), 256, 0, s->stream>>>(src, tar, dl, S, a.tbits, db, s->dmin, k64a, pv);
-            CKS(sort_pairs(k64a, k64b, pv, po, S, 2 * a.tbits + db, s->stream));
-            int64_t* in_ptr;
-            uint2* in_ent;
-            uint8_t* in_pl = nullptr;
-            CKS(s->alloc(&in_ptr, (size_t)s->n + 1));
-            CKS(s->alloc(&in_ent, S, false));
-            CKS(s->alloc(&s->in_syn64, S, false));
-            if (s->stdp && d->syn_plastic) CKS(s->alloc(&in_pl, S, false));
-            k_gather_pull<<<grid_for(S), 256, 0, s->stream>>>(po, src, w, dl, pl, S, a.tbits, in_ent, s->in_syn64,
-                                                               in_pl);
-            uint32_t* tkeys = reinterpret_cast<uint32_t*>(pv);
-            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, tkeys);
-            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(tkeys, S, 0, in_ptr);
-            CKS(exclusive_scan(in_ptr, s->n, s->stream));
-            CK(cudaStreamSynchronize(s->stream));
-            a.in_ptr = in_ptr;
-            a.in_ent = in_ent;
-            a.in_plastic = in_pl;
-        }
-        // CSR by source (and delay bucket), synapse-list order inside (stable)
-        CKS(tmp_alloc(t_keys, &keys, S));
-        CKS(tmp_alloc(t_vals, &vals, S));
-        CKS(tmp_alloc(t_order, &order, S));
-        CKS(tmp_alloc(t_keys2, &keys2, S));
-        k_explicit_keys<<<grid_for(S), 256, 0, s->stream>>>(src, dl, S, dbits, s->dmin, keys, vals);
-        CKS(sort_pairs(keys, keys2, vals, order, S, s->sbits + dbits, s->stream));
-        int32_t* csr_src = nullptr;
-        uint8_t* plastic = nullptr;
-        if (s->stdp && !a.pull) {
-            CKS(s->alloc(&csr_src, S, false));
-            if (d->syn_plastic) CKS(s->alloc(&plastic, S, false));
-        }
-        k_gather_explicit<<<grid_for(S), 256, 0, s->stream>>>(order, keys2, dbits, tar, w, dl, pl, S, a.tbits, syn,
-                                                               s->csr_syn64, csr_src, plastic);
-        a.csr_src = csr_src;
-        a.plastic = plastic;
-        if (s->stdp && !a.pull) {
-            // incoming lists: CSR positions sorted by target, synapse-list order
-            int64_t* dend_off;
-            int64_t* dend_pos;
-            CKS(s->alloc(&dend_off, (size_t)s->n + 1));
-            CKS(s->alloc(&dend_pos, S, false));
-            k_cast_keys<<<grid_for(S), 256, 0, s->stream>>>(tar, S, keys);
-            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(keys, S, 0, dend_off);
-            CKS(exclusive_scan(dend_off, s->n, s->stream));
-            k_inverse<<<grid_for(S), 256, 0, s->stream>>>(s->csr_syn64, S, vals);  // vals := pos_of
-            uint32_t* keys_out = reinterpret_cast<uint32_t*>(src);  // src is no longer needed
-            CKS(sort_pairs(keys, keys_out, vals, order, S, a.tbits, s->stream));
-            k_widen<<<grid_for(S), 256, 0, s->stream>>>(order, S, dend_pos);
-            a.dend_off = dend_off;
-            a.dend_pos = dend_pos;
-        }
-        count_keys(s.get(), keys2, S);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(s->stream));
+        CKS(csr_from_list(s.get(), src, tar, w, dl, pl));
     }
     CKS(finish_build(s.get()));
     *out = s.release();

@@ -60,9 +60,91 @@ void MGSimulator::check(int status, const char* what)
     exit(1);
 }
 
+// The network of a Config::DEVICE_NETGEN recipe, generated on the device
+// (mgc_create_generated) as one handle.
+void MGSimulator::build_generated(Network& net)
+{
+    const size_t n = net.neurons.size();
+    n_neurons = (int)n;
+    std::vector<float> rate(n), v0(n);
+    for (size_t i = 0; i < n; ++i) {
+        rate[i] = net.neurons[i].rate;
+        v0[i] = net.v_init.size() == n ? net.v_init[i] : net.lifconst[1];
+    }
+    std::vector<int32_t> pop_num(net.pops.size());
+    std::vector<int8_t> pop_type(net.pops.size());
+    for (size_t p = 0; p < net.pops.size(); ++p) {
+        pop_num[p] = net.pops[p].num;
+        pop_type[p] = (int8_t)net.pops[p].type;
+    }
+    const Network::GenRecipe& rc = net.recipe;
+    std::vector<mgc_gen_proj> pr(rc.projs.size());
+    for (size_t r = 0; r < rc.projs.size(); ++r) {
+        const Network::GenProjection& g = rc.projs[r];
+        mgc_gen_proj& q = pr[r];
+        q.src = g.src;
+        q.tar = g.tar;
+        q.rule = g.rule;
+        q.prob = g.prob;
+        q.k = g.k;
+        q.conn_seed = g.seed;
+        q.weight = g.weight;
+        q.delay = g.delay;
+        q.delay_max = g.delay_max;
+        q.weights = g.weights.empty() ? nullptr : g.weights.data();
+        q.delays = g.delays.empty() ? nullptr : g.delays.data();
+        // Config::STDP makes every synapse plastic unless STDP_BY_TYPE gates it by projection
+        q.plastic = Config::STDP_BY_TYPE ? (g.plastic ? 1 : 0) : 1;
+    }
+    mgc_gen_desc d{};
+    d.n_pops = (int32_t)pop_num.size();
+    d.pop_num = pop_num.data();
+    d.pop_type = pop_type.data();
+    d.n_proj = (int32_t)pr.size();
+    d.proj = pr.data();
+    for (int k = 0; k < 624; ++k) d.mt_state[k] = rc.mt[k];
+    d.rate = rate.data();
+    d.v_init = v0.data();
+    const std::array<float, 30> lc = net.nlifconst ? net.lifconst : default_lifconst(net.nstdpconst, Config::DT);
+    for (int i = 0; i < 30; ++i) d.lifconst[i] = lc[i];
+    const std::array<float, 6> sc =
+        net.nstdpconst ? net.stdpconst : std::array<float, 6>{0.1f, -0.01f, 17, 34, 40, 0};
+    for (int i = 0; i < 6; ++i) d.stdpconst[i] = sc[i];
+    d.stdp = Config::STDP ? 1 : 0;
+    d.mode = MGC_MODE_AUTO;
+    if (Config::SEED >= 0) {
+        d.seed = (uint64_t)Config::SEED;
+    } else {
+        srand((unsigned)time(0));  // as init_state does (mgcore.cu:665-669)
+        d.seed = (uint64_t)rand();
+    }
+    d.device = Config::DEVICE;
+    d.raster_steps = 65536;
+    d.raster_ids = 0;
+    if (npart > 1)
+        std::cerr << "mgbrain_b200: a network generated on the device runs as one handle; the " << npart
+                  << " partitions run together" << std::endl;
+    std::cout << (npart == 1 ? "run single-net on single-GPU" : "run multi-net on single-GPU") << std::endl;
+    Piece pc;
+    pc.count = (int)n;
+    pc.device = Config::DEVICE;
+    check(mgc_create_generated(&d, &pc.sim), "mgc_create_generated");
+    pieces.push_back(pc);
+    sim = pc.sim;
+    mgc_info info;
+    check(mgc_get_info(sim, &info), "mgc_get_info");
+    min_delay = info.min_delay;
+    max_delay = info.max_delay;
+}
+
 MGSimulator::MGSimulator(Network& net, std::vector<int>& part, int nparts)
 {
     npart = nparts < 1 ? 1 : nparts;
+    this->part = part;
+    if (net.recipe.active) {
+        build_generated(net);
+        return;
+    }
     const size_t n = net.neurons.size();
     const size_t S = net.synapses.size();
     n_neurons = (int)n;

@@ -6,6 +6,7 @@
 
 #include "mgbrain/constgen.h"
 #include "mgbrain/mt19937.h"
+#include "mgc.h"
 #include "mgbrain/netgen.h"
 
 #ifndef __CUDACC__  // the core's Philox header, here compiled for the host only
@@ -37,6 +38,7 @@ bool Config::THROW_ON_ERROR = false;
 bool Config::STDP_BY_TYPE = false;
 int Config::NETGEN_THREADS = 0;
 long long Config::NETGEN_PARALLEL_PAIRS = 1LL << 24;
+bool Config::DEVICE_NETGEN = false;
 
 Model::Model() { indexer = 0; }
 
@@ -309,6 +311,68 @@ void add_pairs(Network& net, const Pop& sp, const Pop& tp, const std::vector<siz
     for (auto& th : pool) th.join();
 }
 
+// Config::DEVICE_NETGEN: the projections as the device generator takes
+// them (mgc_gen_proj), with the weights and delays gen_net draws with rand()
+// for ranged projections drawn here, in the same order (one rand_weight and
+// one rand_delay per synapse, projection after projection), so the rand()
+// stream advances as gen_net's does; the mt19937 draws of the
+// fixed-probability rule happen on the device, from the state recorded here.
+void record_recipe(Network& net, const Model& model, const Mt19937& rng)
+{
+    Network::GenRecipe& rc = net.recipe;
+    rc = Network::GenRecipe{};
+    rc.active = true;
+    rng.state_words(rc.mt.data());
+    for (size_t pi = 0; pi < model.pros.size(); ++pi) {
+        const Projection& pr = model.pros[pi];
+        const size_t sn = (size_t)net.pops[pr.src].num, tn = (size_t)net.pops[pr.tar].num;
+        const real w0 = pr.wrange[0], w1 = pr.wrange[1], d0 = pr.drange[0], d1 = pr.drange[1];
+        Network::GenProjection g;
+        g.src = pr.src;
+        g.tar = pr.tar;
+        g.plastic = pr.stype == SynapseType::STDP;
+        g.weight = w0;
+        g.delay = (int)std::round(d0 / Config::STEP);  // build_multinet's rounding (mgsim.cpp:49)
+        size_t count = 0;
+        if (pr.rule == 1) {
+            g.rule = MGC_RULE_FIXED_INDEGREE;
+            g.k = pr.k;
+            g.seed = pr.seed;
+            g.delay_max = (int)std::round(d1 / Config::STEP);
+            count = tn * (size_t)pr.k;
+        } else if (pr.rule == 2) {
+            g.rule = MGC_RULE_ALL_BUT_SELF;
+            count = sn * tn - std::min(sn, tn);
+        } else if (pr.ctype == 1.0) {
+            g.rule = MGC_RULE_ALL;
+            count = sn * tn;
+        } else if (pr.ctype == 0.0) {
+            g.rule = MGC_RULE_ONE;
+            count = sn;
+        } else if (pr.ctype > 0.0 && pr.ctype < 1.0) {
+            g.rule = MGC_RULE_PROB;
+            g.prob = pr.ctype;
+            const size_t max_num = sn * tn;
+            count = static_cast<size_t>(std::round(max_num * pr.ctype));
+        } else {
+            continue;  // gen_net makes no synapses for it
+        }
+        g.delay_max = std::max(g.delay_max, g.delay);
+        if (g.rule != MGC_RULE_FIXED_INDEGREE && (w1 != w0 || d1 != d0)) {
+            if (w1 != w0) g.weights.reserve(count);
+            if (d1 != d0) g.delays.reserve(count);
+            for (size_t t = 0; t < count; ++t) {
+                const real w = NetGen::rand_weight(w0, w1);
+                const real d = NetGen::rand_delay(d0, d1);
+                if (w1 != w0) g.weights.push_back(w);
+                if (d1 != d0) g.delays.push_back((int)std::round(d / Config::STEP));
+            }
+        }
+        rc.synapses += (long long)count;
+        rc.projs.push_back(std::move(g));
+    }
+}
+
 }  // namespace
 
 void NetGen::gen_net(Network& net, Model& model)
@@ -334,6 +398,15 @@ void NetGen::gen_net(Network& net, Model& model)
         }
     }
     model.indexer = next_id;
+    net.recipe = Network::GenRecipe{};
+    if (Config::DEVICE_NETGEN) {
+        if (!Config::SHUFFLE_GEN) {
+            record_recipe(net, model, rng);
+            return;
+        }
+        std::cerr << "mgbrain_b200: the shuffle placement is drawn on the host; NetGen lists the synapses"
+                  << std::endl;
+    }
 
     for (size_t pi = 0; pi < model.pros.size(); ++pi) {
         const Projection& pr = model.pros[pi];

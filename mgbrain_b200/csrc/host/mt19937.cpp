@@ -207,6 +207,17 @@ void Mt19937::clear()
     for (int k = 0; k < N; ++k) x_[k] = 0;
 }
 
+void Mt19937::state_words(uint32_t* out) const
+{
+    for (int k = 0; k < N; ++k) out[k] = x_[(i_ + k) % N];
+}
+
+void Mt19937::set_state_words(const uint32_t* in)
+{
+    for (int k = 0; k < N; ++k) x_[k] = in[k];
+    i_ = 0;
+}
+
 MtJump::MtJump(uint64_t steps) : steps_(steps)
 {
     // x^steps mod phi by squaring and multiplying by x, from the top bit
@@ -232,6 +243,16 @@ MtJump::MtJump(uint64_t steps) : steps_(steps)
             }
         }
     }
+}
+
+MtJump MtJump::doubled() const
+{
+    MtJump j;
+    j.steps_ = 2 * steps_;
+    Poly sq = square(poly_);
+    reduce(sq);
+    j.poly_ = sq;
+    return j;
 }
 
 void MtJump::apply(Mt19937& g) const

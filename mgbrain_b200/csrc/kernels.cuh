@@ -4,7 +4,7 @@
 //  ring (immediate push; needed when weights are plastic):
 //   k_neuron  neuron update reading ring slot s % M, spike compaction
 //   k_push    event push from the spiking rows into ring slots (s+d) % M
-//   k_stdp    (Config::STDP) weight update over the spikers' rows
+//             (k_push_stdp with Config::STDP: push and both STDP sides)
 //  deferred (static weights):
 //   k_deliver events whose arrival step is s: for every delay d, the
 //             spikes of step s-d push their delay-d row segment (rows are
@@ -62,6 +62,7 @@ struct StepArgs {
     float C[30];          // LIFECONSTS
     float P[6];           // STDPCONSTS
     int32_t chunks_per_spike;
+    int32_t chunks_in_per_spike;  // ring method with STDP: 128-entry chunks of the longest incoming list
     int32_t has_cur;      // some neuron is LIF or LIFE: the update loads Iexc/Iinh with the group
                           // (k_fused is instantiated for each case)
     int32_t stdp;
@@ -81,7 +82,7 @@ struct StepArgs {
     float fx_scale;       //   2^fx_shift: a weight w is added as the integer rint(w * fx_scale)
     float fx_unscale;     //   2^-fx_shift: an input sum is float(sum) * fx_unscale
     int32_t pull;         // pull method (per-target pass at emission, STDP fused)
-    uint32_t* fired_bits; //   [ns/32] spikes of the current step
+    uint32_t* fired_bits; //   [ns/32] spikes of the current step (also the ring method with STDP)
     const int64_t* in_ptr;//   [n+1] incoming rows (by target)
     uint2* in_ent;        //   [S] {source | delay << tbits, weight bits}, rows sorted by
                           //   (delay, source, synapse-list order)
@@ -433,8 +434,9 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                     reinterpret_cast<float4*>(a.Iinh)[g] = ci4[h];
                 }
             }
-            if (a.pull) {
-                // bitmap of this step's spikes: 8 lanes (32 neurons) per word
+            if (a.fired_bits) {
+                // bitmap of this step's spikes (pull method, ring method with
+                // STDP): 8 lanes (32 neurons) per word
                 unsigned wv = fmask[h] << (4 * (lane & 7));
                 wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
                 wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
@@ -1320,9 +1322,7 @@ __global__ void __launch_bounds__(kPushBlock) k_push(StepArgs a)
         }
     }
     if (lane == 0 && ev) atomicAdd(a.events, ev);
-    if (!a.stdp) {
-        if (last_block(a.done)) step_epilogue(a);
-    }
+    if (last_block(a.done)) step_epilogue(a);
 }
 
 

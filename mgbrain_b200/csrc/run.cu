@@ -32,8 +32,7 @@ int graph_group_mode(const mgc_sim* s, int p) { return p == 3 ? (s->dmin >= 4 ? 
 int kernels_per_step(const mgc_sim* s)
 {
     if (s->a.deferred) return s->fused ? 1 : 2;
-    if (s->a.pull) return 2;
-    return s->stdp ? 3 : 2;
+    return 2;  // neuron update, then the push (with STDP fused) or the pull
 }
 
 mgc_status enqueue_step(mgc_sim* s)
@@ -58,7 +57,6 @@ mgc_status enqueue_step(mgc_sim* s)
             pull_kernel(s)<<<s->pull_grid, kPushBlock, 0, s->stream>>>(s->a);
         } else {
             push_kernel(s)<<<s->push_grid, kPushBlock, 0, s->stream>>>(s->a);
-            if (s->stdp) stdp_kernel(s)<<<s->stdp_grid, kPushBlock, 0, s->stream>>>(s->a);
         }
         s->launches += kernels_per_step(s);
     }

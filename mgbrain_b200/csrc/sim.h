@@ -94,7 +94,7 @@ struct mgc_sim {
     int64_t S = 0;
     int mode = MGC_MODE_PUSH;
     bool stdp = false;
-    int neuron_grid = 1, push_grid = 1, stdp_grid = 1, deliver_grid = 1, fused_grid = 1;
+    int neuron_grid = 1, push_grid = 1, deliver_grid = 1, fused_grid = 1;
     bool fused = false;  // one launch per step (deferred, min delay >= 2)
     bool explicit_net = false;  // built from a synapse list (mgc_create)
     int pull_grid = 1;
@@ -204,7 +204,6 @@ StepKernel neuron_kernel(const mgc_sim* s);
 StepKernel deliver_kernel(const mgc_sim* s);
 StepKernel push_kernel(const mgc_sim* s);
 StepKernel pull_kernel(const mgc_sim* s);
-StepKernel stdp_kernel(const mgc_sim* s);
 // The fused step kernel for this network (with or without LIF/LIFE
 // currents), variant 0 compiled for 2 resident blocks per SM, 1 for 3.
 StepKernel fused_kernel(const mgc_sim* s, int v);
@@ -221,6 +220,24 @@ const void* sched_decide_kernel();
 mgc_status pick_device(int device);
 // Grids of the kernels the handle launches (after the kernel selection changed).
 mgc_status launch_shapes(mgc_sim* s);
+// The builders' steps, in order: neuron arrays and constants; the method
+// (CSR word layout, delivery method, fixed-point plan: hetero = some neuron
+// receives unequal weights of one sign); the CSR layout; the CSR from a
+// device-resident synapse list (src, tar, weight, delay in steps, plastic
+// flags or null; src is overwritten); the method's buffers and launch shapes.
+mgc_status build_neurons(mgc_sim* s, int32_t n, const int8_t* type, const float* rate, const float* v_init,
+                         const float* lifc, const float* stdpc, uint64_t seed, int64_t raster_steps,
+                         int64_t raster_ids);
+mgc_status build_method(mgc_sim* s, int requested, bool hetero, int32_t fx_shift);
+// The fixed-point plan alone (a builder that learns it after the method).
+mgc_status build_set_fx(mgc_sim* s, bool hetero, int32_t fx_shift);
+mgc_status begin_list_layout(mgc_sim* s);
+mgc_status csr_from_list(mgc_sim* s, int32_t* src, int32_t* tar, float* w, int32_t* dl, uint8_t* pl);
+mgc_status build_finish(mgc_sim* s);
+// The fixed-point shift rule (kernels.cuh): sums of up to `bound` fit 61
+// bits; with `exact`, no finer than the smallest weight's last mantissa bit
+// (min_exp: its frexp exponent).
+int32_t fx_shift_rule(double bound, int min_exp, bool exact);
 // Segments of up to `gap` synapses cut into chunks of about `target`.
 void set_chunking(StepArgs& a, int64_t gap, int64_t target);
 

@@ -6,6 +6,8 @@
 //   api_driver simulate <spec> <out_prefix> <seconds> <v0.f32|-> <stdp 0|1> [npart [single|multi]]
 //                                                env MGB_MT_SEED, MGB_RAND_SEED, MGB_SEED
 //   (npart > 1: SIMPLE partitions; "single" calls config::enable_single_gpu())
+//   env MGB_DEVICE_NETGEN=1: config::enable_device_netgen() (the network is
+//   generated on the device when the simulator is built)
 // simulate writes <out_prefix>.state (V, fire_cnt, weights) and .raster.
 #include <cstdio>
 #include <cstdlib>
@@ -34,6 +36,7 @@ static long long env(const char* k, long long d)
 static void build(const char* spec, network& net)
 {
     config::set_netgen_seed(env("MGB_MT_SEED", 5489));
+    config::enable_device_netgen(env("MGB_DEVICE_NETGEN", 0) != 0);
     srand((unsigned)env("MGB_RAND_SEED", 1));
     model m;
     mgb_spec::Applied app = mgb_spec::apply(slurp(spec), m);

@@ -430,3 +430,34 @@ def fx_plan(net, stdp=False, plastic=None, wlim=0.0):
 def equal_per_sign(w):
     w = np.asarray(w)
     return len(np.unique(w[w > 0])) <= 1 and len(np.unique(w[w <= 0])) <= 1
+
+
+def gen_projs(spec, net):
+    """The projections of a model description as mgc_create_generated takes
+    them; ranged weights and delays (which NetGen draws with glibc rand())
+    come from `net`, the list gen_net made for the same description (its
+    per-synapse projection index says whose they are)."""
+    import mgbrain_b200 as mgb
+    out = []
+    proj = np.asarray(net["proj"])
+    dsteps, _, _ = quantize_delays(net["delay"], net["step"])
+    for r, p in enumerate(spec.pros):
+        if p.ctype == 1.0:
+            rule = mgb.RULE_ALL
+        elif p.ctype == 0.0:
+            rule = mgb.RULE_ONE
+        else:
+            rule = mgb.RULE_PROB
+        # plastic: every synapse takes part when STDP is on (Config::STDP), as in gen_net
+        d = dict(src=p.src, tar=p.tar, rule=rule, prob=float(p.ctype), plastic=1)
+        sel = proj == r
+        if p.wmin == p.wmax:
+            d["weight"] = float(p.wmin)
+        else:
+            d["weights"] = np.asarray(net["weight"])[sel]
+        if p.dmin == p.dmax:
+            d["delay"] = int(quantize_delays(np.array([p.dmin], np.float32), spec.dt)[0][0])
+        else:
+            d["delays"] = dsteps[sel]
+        out.append(d)
+    return out

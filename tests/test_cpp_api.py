@@ -96,3 +96,24 @@ def test_cpp_partitions_run_as_separate_handles(driver, tmp_path, name):
     for tag in ("multi", "single"):
         assert outs[tag][0] == outs["one"][0], tag
         assert outs[tag][1] == outs["one"][1], tag
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_cpp_device_netgen_equals_host_netgen(driver, tmp_path, name):
+    """config::enable_device_netgen(): gen_net records the projections and the
+    simulator generates the synapses on the device; the run ends in exactly
+    the state (V, fire counts, weights in synapse order) and raster of the
+    host-generated network, and the rand() stream advances as gen_net's."""
+    c, _, _ = load(name)
+    v0p = os.path.join(T.GOLDEN, name + ".v0")
+    outs = {}
+    for dev in ("0", "1"):
+        pre = str(tmp_path / ("dev" + dev))
+        r = subprocess.run([driver, "simulate", os.path.join(T.GOLDEN, name + ".spec"), pre, "0.1",
+                            v0p if os.path.exists(v0p) else "-", str(c["stdp"])],
+                           check=True, env=dict(_env(c), MGB_DEVICE_NETGEN=dev), capture_output=True, text=True)
+        outs[dev] = (open(pre + ".state", "rb").read(), open(pre + ".raster", "rb").read(), r.stdout)
+    assert outs["1"][0] == outs["0"][0]
+    assert outs["1"][1] == outs["0"][1]
+    assert len(outs["0"][1]) > 16
