@@ -845,6 +845,25 @@ def run_refgpu(a, ws, rank, local):
     print(json.dumps(refgpu_compare(a, local)), flush=True)
 
 
+def brunel_maker(nsyn, step):
+    """ModelMaker::make_brunel (src/model/maker.h:10-25) as populations and
+    projections for the device generator: 50 % POISSON inputs, 40 % exc, 10 %
+    inh LIFB, every projection fixed-probability 0.1, the maker's weights and
+    1.6 ms delay, computed in the same float / double mix."""
+    import math
+    import mgbrain_b200 as mgb
+    prob = np.float32(0.1)
+    size = int(math.sqrt(float(np.float32(nsyn)) / (float(prob) * 0.5)))
+    pops = [(size * 5 // 10, mgb.POISSON), (size * 4 // 10, mgb.LIFB), (size * 1 // 10, mgb.LIFB)]
+    w1 = float(np.float32(0.0001 * 20000 / size))
+    w2 = float(np.float32(-0.0005 * 20000 / size))
+    delay = int(np.floor(np.float32(0.0016) / np.float32(step) + np.float32(0.5)))
+    P, E, I = 0, 1, 2
+    projs = [dict(src=s_, tar=t_, rule=mgb.RULE_PROB, prob=float(prob), weight=w, delay=delay)
+             for s_, t_, w in ((P, E, w1), (P, I, w1), (E, E, w1), (E, I, w1), (I, I, w2), (I, E, w2))]
+    return pops, projs
+
+
 def refgpu_compare(a, local):
     """The reference's own benchmark network (ModelMaker::make_brunel with
     --ref-syn synapses, Poisson inputs at 20 Hz, generated by the reference's
@@ -904,9 +923,26 @@ def refgpu_compare(a, local):
         ours_dev = e0.elapsed_time(e1) / 1e3
         st = sim.state()
         events = sim.info()["events"]
+        # the same network generated on the device from the same mt19937 seed
+        # (mgc_create_generated): synapse for synapse the reference's list
+        pops, projs = brunel_maker(a.ref_syn, net["step"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gen = mgb.Simulator.generated(pops, projs, netfile.default_lifconst(net), mt_seed=1, rate=net["rate"],
+                                      seed=7, device=local, raster_ids=-1)
+        gen.sync()
+        gen_dev_s = time.perf_counter() - t0
+        ra, ta, wa, da = sim.export_csr()
+        rb, tb, wb, db = gen.export_csr()
+        netgen_identical = bool(np.array_equal(ra, rb) and np.array_equal(ta, tb) and np.array_equal(da, db) and
+                                np.array_equal(wa.view(np.int32), wb.view(np.int32)))
+        gen.close()
         sim.close()
         return {
             "workload": "refgpu",
+            "netgen": {"reference_gen_net_s": gen_s, "ours_device_s": gen_dev_s, "identical": netgen_identical,
+                       "how": "mgc_create_generated from the same mt19937 seed, CSR and weights compared with the "
+                              "handle built from the reference gen_net's list"},
             "config": {"network": f"the reference's make_brunel, {S} synapses, {n} neurons, inputs 20 Hz, "
                                   f"dt 0.1 ms, generated by the reference's gen_net",
                        "seconds": a.ref_seconds, "steps": steps},
