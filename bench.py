@@ -306,7 +306,7 @@ def make_sim(w, device, seed, record=True):
     import mgbrain_b200 as mgb
     return mgb.Simulator.fixed_indegree(
         w["pops"], w["projs"], w["lif"], rate=w["rate"], v_init=w["v0"], conn_seed=1,
-        seed=seed, device=device, raster_steps=CHUNK * 2, raster_ids=-1 if not record else 0)
+        seed=seed, device=device, raster_steps=CHUNK * 4, raster_ids=-1 if not record else 0)
 
 
 def timed_device(sim, steps_per, k, ws):
@@ -417,7 +417,7 @@ def run_ours(a, ws, rank, local):
     L = mgb.lib()
     for _ in range(1):
         sim.run(CHUNK)
-        sim.read_raster(max_steps=CHUNK * 2, max_ids=w["n"] * 16)  # also drops the autotuner's steps
+        sim.read_raster(max_steps=CHUNK * 4, max_ids=w["n"] * 16)  # also drops the autotuner's steps
     torch.cuda.synchronize()
     barrier(ws)
     h2d = d2h = 0
@@ -988,7 +988,7 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=10000)
     ap.add_argument("--group-mode", type=int, default=0, choices=[0, 1, 2, 3],
                     help="with --kernel-profile or --no-autotune: 0 graphs of k_fused, 1 k_steps groups, "
-                         "2 k_pipe groups, 3 k_window groups (window of 4 steps)")
+                         "2 k_pipe groups, 3 k_window groups (window of min(8, minimum delay) steps)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner and run --group-mode (for launch lists)")
     ap.add_argument("--kernel-profile", choices=["quiet", "driven"],

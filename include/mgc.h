@@ -442,9 +442,12 @@ mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
 mgc_status mgc_set_accumulation(mgc_sim* sim, int32_t mode);
 
 /* Steps per window of the windowed step group (mode 3 of
- * mgc_set_persistent): 1 <= steps <= min(4, minimum delay); default the
- * largest.  Results are the same for every window.  No reference
- * counterpart. */
+ * mgc_set_persistent): 1 <= steps <= min(8, minimum delay); default the
+ * largest.  Windows of more than 4 steps hold their steps' inputs in eight
+ * accumulator buffers (allocated for a minimum delay >= 5) instead of four;
+ * the next mgc_run moves the current step's buffer between the two cycles,
+ * one small kernel on the handle's stream.  Results are the same for every
+ * window.  No reference counterpart. */
 mgc_status mgc_set_window(mgc_sim* sim, int32_t steps);
 
 /* ---- Step scheduler (fused deferred method: minimum delay >= 2) ----------

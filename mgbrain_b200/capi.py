@@ -608,7 +608,7 @@ class Simulator:
         check(lib().mgc_set_accumulation(self._h, int(mode)))
 
     def set_window(self, steps):
-        """Steps per window of the windowed step group (1..min(4, min delay))."""
+        """Steps per window of the windowed step group (1..min(8, min delay))."""
         check(lib().mgc_set_window(self._h, int(steps)))
 
     def profile(self, steps):

@@ -317,7 +317,9 @@ mgc_status choose_mode(mgc_sim* s, int requested)
         a.deferred = 1;
         a.D = D;
         a.dmin = s->dmin;
-        a.H = s->dmax + 4;  // + 3: the windowed step group clears the next window's slots
+        // the step groups clear the history slots of the steps up to a
+        // window (the pipelined group: 3 steps) ahead
+        a.H = s->dmax + std::max(4, std::min(kMaxWindow, s->dmin));
     }
     return MGC_OK;
 }
@@ -411,8 +413,11 @@ mgc_status finish_build(mgc_sim* s)
         s->max_gap = (int64_t)gap;
         CKS(s->alloc(&a.hist_ids, (size_t)a.H * s->n_src, false));
         CKS(s->alloc(&a.hist_cnt, a.H));
-        CKS(s->alloc(&a.acc_e, kAccBuffers * (size_t)a.ns * words));  // step buffers, s % kAccBuffers
-        CKS(s->alloc(&a.acc_i, kAccBuffers * (size_t)a.ns * words));
+        // step buffers, s & acc_mask; eight when windows of 5 steps or more fit
+        s->acc_buffers = s->dmin > kAccBuffers ? kAccBuffersWide : kAccBuffers;
+        a.acc_mask = kAccBuffers - 1;
+        CKS(s->alloc(&a.acc_e, s->acc_buffers * (size_t)a.ns * words));
+        CKS(s->alloc(&a.acc_i, s->acc_buffers * (size_t)a.ns * words));
         // fused step kernel: one resident wave, every warp updates then delivers
         s->fused = s->dmin >= 2;
         s->fused_variant = 1;
@@ -423,9 +428,13 @@ mgc_status finish_build(mgc_sim* s)
         s->persistent = s->fused ? (s->dmin >= 4 ? 2 : 1) : 1;
         if (!s->fused) CKS(s->alloc(&a.bar, 4));  // the grid barrier's arrivals and generation
         if (s->fused) {
-            // windowed group: prefixes of up to kMaxWindow steps in dynamic shared memory
+            // windowed group: the delivery prefixes of a window's steps in
+            // dynamic shared memory (up to 4, or 8 for the wide instantiation)
             s->window = std::min(kMaxWindow, s->dmin);
-            s->window_smem = (size_t)kMaxWindow * (size_t)(a.D + 1) * sizeof(int64_t);
+            for (int wide = 0; wide < 2; ++wide) {
+                const size_t steps = wide ? kMaxWindow : kAccBuffers;
+                s->window_smem[wide] = steps * (size_t)(a.D + 1) * sizeof(int64_t);
+            }
             CKS(init_sched(s));
         }
     } else {
@@ -612,13 +621,14 @@ mgc_status launch_shapes(mgc_sim* s)
                     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, steps_kernel(s, p, v), kPushBlock, 0));
                     s->group_grid_v[p - 1][v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
                 }
-            for (int v = 0; v < 2; ++v) {
-                CK(cudaFuncSetAttribute((const void*)window_kernel(s, v), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)s->window_smem));
-                CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, window_kernel(s, v), kPushBlock,
-                                                                 s->window_smem));
-                s->window_grid_v[v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
-            }
+            for (int wide = 0; wide < 2; ++wide)
+                for (int v = 0; v < 2; ++v) {
+                    const WindowKernel k = window_kernel(s, v, wide);
+                    CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)s->window_smem[wide]));
+                    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kPushBlock, s->window_smem[wide]));
+                    s->window_grid_v[wide][v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
+                }
         } else {
             // minimum delay 1: a barrier-per-phase step group sized to the
             // neurons (8 warps x 64 neuron groups a block per pass)
@@ -1122,7 +1132,7 @@ extern "C" mgc_status mgc_set_accumulation(mgc_sim* s, int32_t mode)
     if (step != 0 || s->graph) return fail(MGC_ERR_INVALID, "the accumulation is chosen before the first step");
     StepArgs& a = s->a;
     float** bufs[2] = {a.deferred ? &a.acc_e : &a.ring_e, a.deferred ? &a.acc_i : &a.ring_i};
-    const size_t entries = (a.deferred ? (size_t)kAccBuffers : (size_t)s->M) * (size_t)a.ns;
+    const size_t entries = (a.deferred ? (size_t)s->acc_buffers : (size_t)s->M) * (size_t)a.ns;
     for (float** b : bufs) {
         float* nb = nullptr;
         CKS(s->alloc(&nb, entries * (fx ? 2 : 1)));  // zeroed: nothing has arrived before the first step

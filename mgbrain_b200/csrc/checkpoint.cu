@@ -9,13 +9,14 @@ extern "C" {
 
 namespace {
 
-constexpr uint64_t kCheckpointMagic = 0x3130545043474d4dull;  // "MMGCPT01"
+constexpr uint64_t kCheckpointMagic = 0x3230545043474d4dull;  // "MMGCPT02"
 
 struct CheckpointHeader {
     uint64_t magic;
     int64_t n, ns, S;
     int32_t mode, M, H, D, stdp, ahead, fx, fx_shift;
-    int64_t bytes;  // whole checkpoint
+    int32_t acc_mask, reserved;  // the accumulator cycle the buffers are laid out in
+    int64_t bytes;               // whole checkpoint
 };
 
 struct Segment {
@@ -34,8 +35,8 @@ std::vector<Segment> state_segments(mgc_sim* s)
         {a.fire_cnt, 4 * ns}, {const_cast<float*>(a.rate), 4 * ns}, {a.step, 16}, {a.events, 8},
         {a.spk_count, 4}};
     if (a.deferred) {
-        v.push_back({a.acc_e, acc * kAccBuffers * ns});
-        v.push_back({a.acc_i, acc * kAccBuffers * ns});
+        v.push_back({a.acc_e, acc * (size_t)s->acc_buffers * ns});
+        v.push_back({a.acc_i, acc * (size_t)s->acc_buffers * ns});
         v.push_back({a.hist_ids, 4 * (size_t)a.H * (size_t)s->n_src});
         v.push_back({a.hist_cnt, 4 * (size_t)a.H});
     } else {
@@ -62,6 +63,7 @@ CheckpointHeader checkpoint_header(mgc_sim* s)
     h.ahead = s->ahead;
     h.fx = s->a.fx;
     h.fx_shift = s->fx_shift;
+    h.acc_mask = s->a.acc_mask;
     h.bytes = sizeof(CheckpointHeader);
     for (const Segment& g : state_segments(s)) h.bytes += (int64_t)g.bytes;
     return h;
@@ -107,7 +109,7 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
     if (h.magic != kCheckpointMagic) return fail(MGC_ERR_INVALID, "not a checkpoint");
     if (h.n != mine.n || h.S != mine.S || h.mode != mine.mode || h.M != mine.M || h.H != mine.H || h.D != mine.D ||
         h.stdp != mine.stdp || h.fx != mine.fx || h.fx_shift != mine.fx_shift || h.bytes != mine.bytes ||
-        bytes < h.bytes)
+        bytes < h.bytes || (s->a.deferred && h.acc_mask != kAccBuffers - 1 && h.acc_mask + 1 != s->acc_buffers))
         return fail(MGC_ERR_INVALID, "the checkpoint is of another network or method");
     CK(cudaStreamSynchronize(s->stream));
     const char* p = static_cast<const char*>(buf) + sizeof(h);
@@ -130,6 +132,7 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
     }
     s->ahead = h.ahead != 0;
     s->pending = 0;  // a partition's checkpoint is taken between exchanges
+    CKS(set_acc_mask(s, h.acc_mask, false));  // the restored buffers' cycle
     return MGC_OK;
 }
 

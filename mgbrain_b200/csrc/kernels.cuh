@@ -70,14 +70,16 @@ struct StepArgs {
     int32_t deferred;     // deferred delivery (else ring)
     int32_t dmin;         // deferred: delay of bucket 0
     int32_t D;            //   number of delay buckets per row
-    int32_t H;            //   history slots: dmax + 4 (step groups clear slots up to four steps ahead)
+    int32_t H;            //   history slots: dmax + max(4, longest window) (step groups clear the
+                          //   slots of the next steps up to a window ahead)
     int32_t bucket_chunks;//   delivery tasks per (spike, delay) segment
     int32_t chunk_len;    //   synapses per task: segment positions [c*len, (c+1)*len)
     int32_t* hist_ids;    //   [H][n_src] spike ids per step
     int32_t* hist_cnt;    //   [H]
     const int64_t* bucket;   // [n_src*D + 1] CSR position of (source, bucket)
-    float* acc_e;         //   [4][ns] input arriving at step s in buffer s % 4 (fixed-point
-    float* acc_i;         //   accumulation: 64-bit integers, 8 bytes an entry)
+    float* acc_e;         //   [4 or 8][ns] input arriving at step s in buffer s & acc_mask
+    float* acc_i;         //   (fixed-point accumulation: 64-bit integers, 8 bytes an entry)
+    int32_t acc_mask;     //   3, or 7 while windows of more than 4 steps run (8 buffers allocated)
     int32_t fx;           // fixed-point accumulation (deferred and ring methods)
     float fx_scale;       //   2^fx_shift: a weight w is added as the integer rint(w * fx_scale)
     float fx_unscale;     //   2^-fx_shift: an input sum is float(sum) * fx_unscale
@@ -491,15 +493,23 @@ __device__ __forceinline__ int64_t raster_base(const StepArgs& a)
     return (a.deferred || a.pull) && a.record ? *a.raster_pos : 0;
 }
 
-// Accumulator buffer of the input arriving at step s: four buffers, so the
-// pipelined step group can deliver two steps ahead while the oldest buffer
-// is still being read.
+// Accumulator buffer of the input arriving at step s: four buffers in use
+// (s & 3), so the pipelined step group can deliver two steps ahead while the
+// oldest buffer is still being read, and a window of up to 4 steps holds its
+// steps' inputs at once; eight (s & 7) while windows of 5 to 8 steps run.
+// The eight are allocated only for a minimum delay >= 5; the smaller cycle is
+// kept otherwise because it touches half the memory each 4 steps.
 constexpr int kAccBuffers = 4;
+constexpr int kAccBuffersWide = 8;
 
-template <bool FX = false>
+// MASK: the cycle when the kernel fixes it at compile time (the windowed
+// groups: 3 up to 4 steps, 7 above; the host launches them only in that
+// cycle), 0 for the handle's current one.
+template <bool FX = false, int MASK = 0>
 __device__ __forceinline__ typename AccT<FX>::type* acc_buf(const StepArgs& a, float* base, int64_t s)
 {
-    return reinterpret_cast<typename AccT<FX>::type*>(base) + (size_t)(s & (kAccBuffers - 1)) * (size_t)a.ns;
+    const int64_t m = MASK ? MASK : a.acc_mask;
+    return reinterpret_cast<typename AccT<FX>::type*>(base) + (size_t)(s & m) * (size_t)a.ns;
 }
 
 template <bool FX>
@@ -593,8 +603,8 @@ __device__ __forceinline__ void deliver_prefix(const StepArgs& a, int64_t sa, in
 // counter (shared memory) instead of the global one.  NMAX > 1: the tasks of
 // the n <= NMAX consecutive arrival steps sa, sa+1, ... as one task space
 // (step k's prefixes at pre + k*(D+1)), so that a warp's lanes fetch the
-// segments of several steps in one batch.
-template <bool FX, int NMAX = 1>
+// segments of several steps in one batch.  MASK: as for acc_buf.
+template <bool FX, int NMAX = 1, int MASK = 0>
 __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int64_t s, int32_t hslot,
                                               const int64_t* pre, int64_t warp, int64_t nwarps,
                                               unsigned long long* blk_ev = nullptr, int n = 1)
@@ -690,10 +700,10 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
                 const float wt = as_f(w[u].y);
                 const int64_t sx = sa + (NMAX > 1 ? st_of[u] : 0);
                 if (FX)
-                    red_add_fx(acc_buf<true>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask),
+                    red_add_fx(acc_buf<true, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask),
                                to_fx(wt, a.fx_scale));
                 else
-                    red_add(acc_buf(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
+                    red_add(acc_buf<false, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
             }
         }
     }
@@ -865,7 +875,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
 }
 
 // ---------------------------------------------------------------------------
-// Windowed step group (window W <= minimum delay, W <= 4).  The inputs of
+// Windowed step group (window W <= minimum delay, W <= 8).  The inputs of
 // the W steps of a window arrive from spikes of steps before the window, so
 // all of them are delivered before it, and then every neuron advances W
 // steps in registers: its state is loaded and stored once per window, its W
@@ -873,18 +883,22 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_steps(StepArgs a, int32_t 
 // the update, after the next window's deliveries) instead of at every step.
 // The arithmetic of each step is that of the single-step update, step by
 // step, so the results are the same bits.  Accumulator buffers: step x in
-// x & 3, as for the other kernels (W <= 4 keeps a window's buffers distinct);
-// history: H >= max delay + 4, so the slots cleared for the next window hold
-// steps no delivery of this window reads.  The group starts and ends in the
+// x & acc_mask (the 8-buffer cycle for W > 4 keeps a window's buffers
+// distinct); history: H >= max delay + W, so the slots cleared for the next
+// window hold steps no delivery of this window reads.  WMAX (4 or 8) is the
+// longest window an instantiation runs: the 4-step one keeps the smaller
+// per-task step table of the delivery.  The group starts and ends in the
 // state of the single-step kernels (arrivals of its first step delivered,
 // nothing later).  Waits are bounded (kStatusBarrier).
 // ---------------------------------------------------------------------------
-constexpr int kMaxWindow = 4;
+constexpr int kMaxWindow = 8;
+constexpr int kWinLoad = 4;  // input slots a lane holds at once
 
 // Neurons [first group, ...) advanced through the window's wl steps.  One
-// group of four neurons per lane per pass: its state and its wl input slots
-// are loaded at once, the steps run in registers, the state is stored once.
-template <bool CUR, bool FX>
+// group of four neurons per lane per pass: its state is loaded once, its
+// input slots four steps at a time, the steps run in registers, the state is
+// stored once.
+template <bool CUR, bool FX, int WMAX>
 __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int wl, int32_t hs0, int64_t warp,
                                               int64_t nwarps)
 {
@@ -896,7 +910,6 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         char4 t4 = make_char4(0, 0, 0, 0);
         float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), ce4 = v4, ci4 = v4;
         int4 r4 = make_int4(0, 0, 0, 0);
-        In4<FX> e4[kMaxWindow], i4[kMaxWindow];
         if (have) {
             t4 = __ldg(reinterpret_cast<const char4*>(a.type) + g);
             v4 = reinterpret_cast<float4*>(a.V)[g];
@@ -906,58 +919,66 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                 ci4 = reinterpret_cast<float4*>(a.Iinh)[g];
             }
         }
-#pragma unroll
-        for (int k = 0; k < kMaxWindow; ++k) {
-            e4[k].zero();
-            i4[k].zero();
-            if (have && k < wl) {
-                e4[k].load(acc_buf<FX>(a, a.acc_e, w0 + k), g);
-                i4[k].load(acc_buf<FX>(a, a.acc_i, w0 + k), g);
-            }
-        }
         const int32_t i0 = (int32_t)(g << 2);
         const bool pois = t4.x == kPOISSON || t4.y == kPOISSON || t4.z == kPOISSON || t4.w == kPOISSON;
+        // the window's steps four at a time: their input slots loaded at once
+        // (one copy of the update in the code; the loop forms keep the
+        // 3-blocks-per-SM instantiations within their 80 registers)
+#pragma unroll 1
+        for (int h = 0; h < (WMAX > kWinLoad ? wl : WMAX); h += kWinLoad) {
+            if (h >= wl) break;
+            In4<FX> e4[kWinLoad], i4[kWinLoad];
 #pragma unroll
-        for (int k = 0; k < kMaxWindow; ++k) {
-            if (k >= wl) break;
-            const int64_t s = w0 + k;
-            unsigned fm = 0;
-            if (have) {
-                float u[4] = {0.f, 0.f, 0.f, 0.f};
-                if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
-                const float4 e = e4[k].get(a), ii = i4[k].get(a);
-                fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
-                fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
-                fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
-                fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
-                // the step's input was used: its slot is cleared for step s+4
-                In4<FX>::clear(acc_buf<FX>(a, a.acc_e, s), g);
-                In4<FX>::clear(acc_buf<FX>(a, a.acc_i, s), g);
+            for (int k = 0; k < kWinLoad; ++k) {
+                e4[k].zero();
+                i4[k].zero();
+                if (have && h + k < wl) {
+                    e4[k].load(acc_buf<FX, WMAX - 1>(a, a.acc_e, w0 + h + k), g);
+                    i4[k].load(acc_buf<FX, WMAX - 1>(a, a.acc_i, w0 + h + k), g);
+                }
             }
-            // the step's spikes into its history slot, in neuron order within
-            // the warp (no scan when no lane spiked)
-            if (!__any_sync(0xffffffffu, fm != 0)) continue;
-            const int c = __popc(fm);
-            int incl = c;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            if (total) {
-                int32_t hs = hs0 + k;
-                if (hs >= a.H) hs -= a.H;
-                int32_t base = 0;
-                if (lane == 31) base = atomicAdd(a.hist_cnt + hs, total);
-                base = __shfl_sync(0xffffffffu, base, 31);
-                int32_t pos = base + incl - c;
-                int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
-                for (int q = 0; q < 4; ++q)
-                    if (fm & (1u << q)) {
-                        if (!MGC_OK_INDEX(pos < a.n_src)) break;
-                        ids[pos++] = a.src_base + i0 + q;
-                    }
+            for (int k = 0; k < kWinLoad; ++k) {
+                if (h + k >= wl) break;
+                const int64_t s = w0 + h + k;
+                unsigned fm = 0;
+                if (have) {
+                    float u[4] = {0.f, 0.f, 0.f, 0.f};
+                    if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
+                    const float4 e = e4[k].get(a), ii = i4[k].get(a);
+                    fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
+                    fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
+                    fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
+                    fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                    // the step's input was used: its slot is cleared for step s + acc_mask + 1
+                    In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
+                    In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_i, s), g);
+                }
+                // the step's spikes into its history slot, in neuron order within
+                // the warp (no scan when no lane spiked)
+                if (!__any_sync(0xffffffffu, fm != 0)) continue;
+                const int c = __popc(fm);
+                int incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                if (total) {
+                    int32_t hs = hs0 + h + k;
+                    if (hs >= a.H) hs -= a.H;
+                    int32_t base = 0;
+                    if (lane == 31) base = atomicAdd(a.hist_cnt + hs, total);
+                    base = __shfl_sync(0xffffffffu, base, 31);
+                    int32_t pos = base + incl - c;
+                    int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
+                    for (int q = 0; q < 4; ++q)
+                        if (fm & (1u << q)) {
+                            if (!MGC_OK_INDEX(pos < a.n_src)) break;
+                            ids[pos++] = a.src_base + i0 + q;
+                        }
+                }
             }
         }
         if (have) {
@@ -971,27 +992,27 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
     }
 }
 
-// The arrivals of steps [sa0, sa0 + n) (n <= kMaxWindow), from spikes of steps
+// The arrivals of steps [sa0, sa0 + n) (n <= WMAX), from spikes of steps
 // before sa0: the prefixes of the n steps by the first n warps, then every
 // warp through the n steps' tasks without a barrier between them.  s, hslot:
 // a step and its history slot, for the slot arithmetic.
-template <bool FX>
+template <bool FX, int WMAX>
 __device__ __forceinline__ void deliver_window(const StepArgs& a, int64_t sa0, int n, int64_t s, int32_t hslot,
                                                int64_t* pre, int64_t warp, int64_t nwarps, unsigned long long* blk_ev)
 {
     const int wib = threadIdx.x >> 5;
     for (int k = wib; k < n; k += blockDim.x >> 5) deliver_prefix(a, sa0 + k, s, hslot, pre + (size_t)k * (a.D + 1));
     __syncthreads();
-    deliver_tasks<FX, kMaxWindow>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
+    deliver_tasks<FX, WMAX, WMAX - 1>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
 }
 
 __device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0,
                                             int64_t& rbase);
 
-template <bool CUR, int MINB, bool FX>
+template <bool CUR, int MINB, bool FX, int WMAX>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t nsteps, int32_t W)
 {
-    extern __shared__ int64_t wpre[];   // [kMaxWindow][D + 1]
+    extern __shared__ int64_t wpre[];   // [WMAX][D + 1]
     __shared__ int abort_flag;
     __shared__ unsigned long long blk_ev;  // the block's delivered events, added once at the end
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1015,12 +1036,12 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         if (lead)
             for (int k = 1; k <= n; ++k) a.hist_cnt[hs_of(s0 + k)] = 0;
         __syncthreads();
-        if (n > 0) deliver_window<FX>(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
+        if (n > 0) deliver_window<FX, WMAX>(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
         if (!grid_barrier(a, &abort_flag)) return;
     }
     for (int64_t w0 = s0; w0 < s_end;) {
         const int wl = (int)(s_end - w0 < W ? s_end - w0 : W);
-        neuron_window<CUR, FX>(a, w0, wl, hs_of(w0), warp, nwarps);
+        neuron_window<CUR, FX, WMAX>(a, w0, wl, hs_of(w0), warp, nwarps);
         if (!grid_barrier(a, &abort_flag)) return;
         // the window's spikes are complete: its raster, then the next
         // window's arrivals (only those of s_end after the last window)
@@ -1030,7 +1051,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         const int nn = (int)(next < s_end ? (s_end - next < W ? s_end - next : W) : 1);
         if (lead)
             for (int k = 0; k < nn; ++k) a.hist_cnt[hs_of(next + k)] = 0;
-        deliver_window<FX>(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
+        deliver_window<FX, WMAX>(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
         if (next >= s_end) {  // the block's events, before the last barrier
             __syncthreads();
             if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);

@@ -18,6 +18,30 @@ __global__ void k_rate_to_v(const int8_t* type, const float* rate, float* V, int
     }
 }
 
+// The current step's arrivals from buffer s & from_mask to s & to_mask (both
+// accumulators; `words`: 32-bit words per entry).  Between runs only that
+// buffer holds anything (the step kernels clear a buffer when its step's
+// update reads it, and every step form ends with nothing delivered past the
+// current step), so the target is zero and the source is left zero.
+__global__ void k_acc_move(float* acc_e, float* acc_i, const int64_t* step, int32_t from_mask, int32_t to_mask,
+                           int64_t ns, int32_t words)
+{
+    const int64_t s = *step;
+    const int64_t from = s & from_mask, to = s & to_mask;
+    if (from == to) return;
+    const int64_t n = ns * words;
+    uint32_t* bufs[2] = {reinterpret_cast<uint32_t*>(acc_e), reinterpret_cast<uint32_t*>(acc_i)};
+    for (uint32_t* b : bufs) {
+        uint32_t* src = b + from * n;
+        uint32_t* dst = b + to * n;
+        GRID_STRIDE(i, n)
+        {
+            dst[i] = src[i];
+            src[i] = 0u;
+        }
+    }
+}
+
 
 }  // namespace
 
@@ -27,6 +51,34 @@ namespace mgc {
 // group keeps no schedule trace, so the graph takes the pipelined group (or
 // the barrier per step, for a minimum delay below 4) in its place.
 int graph_group_mode(const mgc_sim* s, int p) { return p == 3 ? (s->dmin >= 4 ? 2 : 1) : p; }
+
+int32_t wanted_acc_mask(const mgc_sim* s)
+{
+    const bool wide = s->acc_buffers == kAccBuffersWide && s->persistent == 3 && s->window > kAccBuffers;
+    return wide && !sched_wanted(s) ? kAccBuffersWide - 1 : kAccBuffers - 1;
+}
+
+mgc_status set_acc_mask(mgc_sim* s, int32_t mask, bool move)
+{
+    StepArgs& a = s->a;
+    if (!a.deferred || mask == a.acc_mask) return MGC_OK;
+    if (mask + 1 > s->acc_buffers) return fail(MGC_ERR_INVALID, "%d accumulator buffers, not %d", s->acc_buffers,
+                                               mask + 1);
+    if (s->graph) {  // its launches hold the old cycle
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        s->sched_graph = false;
+    }
+    if (move) {
+        k_acc_move<<<grid_for(a.ns), 256, 0, s->stream>>>(a.acc_e, a.acc_i, a.step, a.acc_mask, mask, a.ns,
+                                                          a.fx ? 2 : 1);
+        CK(cudaGetLastError());
+        s->launches += 1;
+    }
+    a.acc_mask = mask;
+    return MGC_OK;
+}
 
 
 int kernels_per_step(const mgc_sim* s)
@@ -205,6 +257,7 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
     }
     CK(cudaSetDevice(s->device));
     int64_t left = steps;
+    if (left > 0) CKS(set_acc_mask(s, wanted_acc_mask(s), true));
     if (s->a.deferred && s->fused && !s->ahead && left > 0) {
         CKS(enqueue_step(s));  // catches up the delivery, leaves ahead = true
         --left;
@@ -223,9 +276,14 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
             cudaError_t e;
             if (p == 3) {
                 int32_t w = s->window;
+                // a window of w steps holds w buffers; each instantiation
+                // is compiled for one cycle (3, or 7 above 4 steps)
+                const int wide = w > kAccBuffers;
+                if (s->a.acc_mask != (wide ? kAccBuffersWide : kAccBuffers) - 1)
+                    return fail(MGC_ERR_INVALID, "a window of %d steps in the %d-buffer cycle", w, s->a.acc_mask + 1);
                 void* wargs[] = {&ga, &n, &w};
-                e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v), dim3(s->window_grid_v[v]),
-                                                dim3(kPushBlock), wargs, s->window_smem, s->stream);
+                e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v, wide), dim3(s->window_grid_v[wide][v]),
+                                                dim3(kPushBlock), wargs, s->window_smem[wide], s->stream);
             } else {
                 const int grid = s->fused ? s->group_grid_v[p - 1][v] : s->group_grid1;
                 e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(grid), dim3(kPushBlock),

@@ -120,9 +120,10 @@ struct mgc_sim {
     int persistent = 0;               // fused method as cooperative step groups: 1 barrier per
                                       // step, 2 pipelined (min delay >= 4), 3 windowed
     int group_grid_v[2][2] = {{1, 1}, {1, 1}};  // [persistent-1][variant] co-resident grids
-    int window = 1;                   // steps per window of the windowed group (<= min delay, <= 4)
-    int window_grid_v[2] = {1, 1};    // its co-resident grids by variant
-    size_t window_smem = 0;           // its dynamic shared memory: the window's delivery prefixes
+    int window = 1;                   // steps per window of the windowed group (<= min delay, <= 8)
+    int window_grid_v[2][2] = {{1, 1}, {1, 1}};  // its co-resident grids [window > 4][variant]
+    size_t window_smem[2] = {0, 0};   // its dynamic shared memory [window > 4]: the delivery prefixes
+    int acc_buffers = 4;              // accumulator buffers allocated (8 for a minimum delay >= 5)
     int group_grid1 = 1;              // minimum delay 1: the step group's grid
     int32_t fx_shift = 0;             // fixed-point shift the builder picked for this network's weights
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
@@ -211,8 +212,9 @@ StepKernel fused_kernel(const mgc_sim* s, int v);
 // p = 2 pipelined; a minimum delay of 1 has its own group (k_steps1).
 GroupKernel steps_kernel(const mgc_sim* s, int p, int v);
 GroupKernel pipe_kernel(const mgc_sim* s, int v);
-// The windowed step group of variant v.
-WindowKernel window_kernel(const mgc_sim* s, int v);
+// The windowed step group of variant v: for windows of up to 4 steps, or
+// (wide) of up to 8.
+WindowKernel window_kernel(const mgc_sim* s, int v, bool wide);
 // The scheduler's decision kernel (sched.cu).
 const void* sched_decide_kernel();
 
@@ -250,6 +252,13 @@ bool sched_wanted(const mgc_sim* s);
 mgc_status refresh_graph(mgc_sim* s);
 // The step-group mode the scheduler's graph runs for mode p.
 int graph_group_mode(const mgc_sim* s, int p);
+// The accumulator cycle the next steps run with: 7 (eight buffers) while
+// windowed groups of more than 4 steps run, else 3.
+int32_t wanted_acc_mask(const mgc_sim* s);
+// Switch the accumulator cycle to `mask`: with `move`, the buffer holding the
+// current step's arrivals moves to its place in the new cycle (on the
+// stream); graphs holding the old cycle are dropped.
+mgc_status set_acc_mask(mgc_sim* s, int32_t mask, bool move);
 
 // Stream-ordered write of one field of the device scheduler state.
 template <class T>

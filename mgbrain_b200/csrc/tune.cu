@@ -238,12 +238,17 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     const int window0 = s->window;
     int best_window = window0;
     // step-group trials: p = 1, 2 of both instantiations, then the windows
-    // 2..min(4, min delay) of the windowed group (p = 3) of both
+    // 2..min(4, min delay) of the windowed group (p = 3) of both, and the
+    // longest, min(8, min delay), when above 4 (windows of 5 to 7 steps load
+    // their inputs in a second, partial batch and measured slower than both
+    // 4 and 8 on the benchmark networks)
     std::vector<std::pair<int, int>> groups;  // (mode, window)
     if (s->fused) {
         for (int p = 1; p <= 2; ++p)
             if (p == 1 || s->dmin >= 4) groups.push_back({p, window0}), groups.push_back({p, window0});
-        for (int w = 2; w <= std::min(kMaxWindow, s->dmin); ++w) groups.push_back({3, w}), groups.push_back({3, w});
+        for (int w = 2; w <= std::min(kAccBuffers, s->dmin); ++w) groups.push_back({3, w}), groups.push_back({3, w});
+        const int widest = std::min(kMaxWindow, s->dmin);
+        if (widest > kAccBuffers) groups.push_back({3, widest}), groups.push_back({3, widest});
     } else {
         groups.push_back({1, window0});
     }

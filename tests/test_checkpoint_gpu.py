@@ -27,6 +27,34 @@ def stdp(mode):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("wide_first", [True, False])
+def test_resume_across_accumulator_cycles(wide_first):
+    """A checkpoint taken while windows of 8 steps run (8-buffer cycle) loads
+    into a fresh handle (4-buffer cycle) and continues under the pipelined
+    group, and the other way round, exactly as the uninterrupted run."""
+    def form(sim, wide):
+        sim.set_persistent(3 if wide else 2)
+        if wide:
+            sim.set_window(8)
+    a = brunel(mgb.MODE_AUTO)
+    form(a, wide_first)
+    a.run(1203)
+    a.read_raster()
+    blob = a.checkpoint()
+    b = brunel(mgb.MODE_AUTO)
+    b.restore(blob)
+    form(a, not wide_first)
+    form(b, not wide_first)
+    a.run(1501)
+    b.run(1501)
+    fa, ca, ia = a.read_raster()
+    fb, cb, ib = b.read_raster()
+    assert fa == fb == 1203 and ca.sum() > 0
+    assert np.array_equal(ca, cb) and np.array_equal(ia, ib)
+    assert np.array_equal(a.state()["V"], b.state()["V"])
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("make,mode", [(brunel, mgb.MODE_AUTO), (brunel, mgb.MODE_PUSH),
                                        (stdp, mgb.MODE_PUSH), (stdp, mgb.MODE_PULL)])
 def test_resume_equals_uninterrupted(make, mode):

@@ -63,7 +63,7 @@ def forms(dmin):
     out = [("push", mgb.MODE_PUSH, None, None), ("graphs", mgb.MODE_AUTO, 0, None)]
     if dmin >= 2:
         out.append(("barrier-per-step", mgb.MODE_AUTO, 1, None))
-        out += [(f"windowed-{w}", mgb.MODE_AUTO, 3, w) for w in range(1, min(4, dmin) + 1)]
+        out += [(f"windowed-{w}", mgb.MODE_AUTO, 3, w) for w in range(1, min(8, dmin) + 1)]
     else:
         out.append(("step-group-delay-1", mgb.MODE_AUTO, 1, None))
     if dmin >= 4:

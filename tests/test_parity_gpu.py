@@ -111,7 +111,7 @@ def test_cuda_matches_reference_kernels(name):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", NAMES)
 def test_windowed_group_matches_reference_kernels(name):
-    """The windowed step group (mgc_set_persistent mode 3, windows of up to 4
+    """The windowed step group (mgc_set_persistent mode 3, windows of up to 8
     steps) against the reference kernels' outputs: rasters and integer state
     bit-exact; V bit-exact with one weight per sign, else within 1e-5
     relative of the reference (whose fp32 atomics leave the order of unequal
@@ -128,7 +128,7 @@ def test_windowed_group_matches_reference_kernels(name):
         pytest.skip("a minimum delay of one step has one step-group form")
     rc, ri, rst = ref
     gc, gi, gst, gsim = run_cuda(name, persistent=3)
-    assert gsim.info()["persistent"] == 3 and gsim.info()["window"] == min(4, dmin)
+    assert gsim.info()["persistent"] == 3 and gsim.info()["window"] == min(8, dmin)
     assert np.array_equal(gc, rc)
     assert np.array_equal(gi, ri)
     for k in ("fire_cnt", "last_fired", "refrac"):

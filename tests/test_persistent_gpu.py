@@ -102,7 +102,7 @@ def test_one_step_delay_group_equals_graphs(nu):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("nu", [0.002, 0.02])
-@pytest.mark.parametrize("window", [1, 2, 3, 4])
+@pytest.mark.parametrize("window", [1, 2, 3, 4, 5, 8])
 def test_windowed_group_equals_graphs(nu, window):
     """The windowed step group (arrivals of W steps delivered before the
     window, then W updates with the state in registers) gives the rasters,
@@ -147,10 +147,11 @@ def test_windowed_group_equals_graphs(nu, window):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dmin", [2, 5])
+@pytest.mark.parametrize("dmin", [2, 5, 9])
 def test_windowed_group_short_min_delay(dmin):
-    """Minimum delays 2 and 5: every window up to min(4, dmin) steps gives
-    the rasters and state of the graph path; a longer window is refused."""
+    """Minimum delays 2, 5 and 9: every window up to min(8, dmin) steps
+    (those of 5 or more in the 8-buffer cycle) gives the rasters and state of
+    the graph path; a longer window is refused."""
     w = bench.workload(scale=0.03, nu=0.02)
     projs = [(s, t, k, wt, dmin, dmin + 5) for (s, t, k, wt, _, _) in w["projs"]]
 
@@ -163,7 +164,7 @@ def test_windowed_group_short_min_delay(dmin):
     _, cr, ir = ref.read_raster()
     vr = ref.state()["V"]
     ref.close()
-    for window in range(1, min(4, dmin) + 1):
+    for window in range(1, min(8, dmin) + 1):
         sim = mk()
         sim.set_persistent(3)
         sim.set_window(window)
@@ -175,10 +176,45 @@ def test_windowed_group_short_min_delay(dmin):
         assert np.array_equal(sim.state()["V"], vr)
         assert c.sum() > 0
         with pytest.raises(mgb.MgcError):
-            sim.set_window(min(4, dmin) + 1)
+            sim.set_window(min(8, dmin) + 1)
         with pytest.raises(mgb.MgcError):
             sim.set_window(0)
         sim.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nu", [0.002, 0.02])
+def test_accumulator_cycle_switches(nu):
+    """Runs that alternate between windows of more than 4 steps (8-buffer
+    cycle) and every other form (4-buffer cycle), at odd step counts, give
+    the rasters, state and event count of the graph path."""
+    ref = make(nu)
+    ref.set_persistent(0)
+    ref.run(2400)
+    _, cr, ir = ref.read_raster()
+    vr, ev = ref.state()["V"], ref.info()["events"]
+    ref.close()
+    sim = make(nu)
+    assert sim.info()["min_delay"] >= 8
+    plan = [(3, 8, 301), (2, None, 211), (3, 5, 157), (0, None, 130), (3, 4, 99), (3, 7, 64), (1, None, 3),
+            (3, 6, 1), (3, 8, 2), (2, None, 5)]
+    done = 0
+    for mode, window, steps in plan:
+        sim.set_persistent(mode)
+        if window:
+            sim.set_window(window)
+        sim.run(steps)
+        done += steps
+    sim.set_persistent(3)
+    sim.set_window(8)
+    sim.run(2400 - done)
+    sim.sync()
+    _, c, i = sim.read_raster()
+    assert c.sum() > 0
+    assert np.array_equal(c, cr) and np.array_equal(i, ir)
+    assert np.array_equal(sim.state()["V"], vr)
+    assert sim.info()["events"] == ev
+    sim.close()
 
 
 @pytest.mark.gpu

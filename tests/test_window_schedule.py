@@ -6,9 +6,12 @@ launches (k_fused) between groups:
 - every arrival step is delivered exactly once, in a phase after every phase
   that updated one of its source steps (sa - d, min delay <= d <= max delay)
   and before the phase that updates it;
-- an accumulator buffer (step % 4) is written only after the step that used it
-  before was updated (its input consumed and cleared);
-- a history slot (step % H, H = max delay + 4) is cleared in a phase that reads
+- an accumulator buffer (step & 3, or step & 7 while windows of more than 4
+  steps run) is written only after the step that used it before was updated
+  (its input consumed and cleared), and between groups only the buffer of the
+  current step holds input, so switching the cycle moves that one buffer;
+- a history slot (step % H, H = max delay + max(4, min(8, min delay))) is
+  cleared in a phase that reads
   no step sharing that slot, after every read of its old step, and before its
   new step's update writes it; the raster copy of a step reads its slot after
   the update and before the slot is cleared again.
@@ -21,12 +24,16 @@ import random
 import pytest
 
 ACC_BUFFERS = 4
-MAX_WINDOW = 4
+ACC_BUFFERS_WIDE = 8
+MAX_WINDOW = 8
 
 
 class Schedule:
     def __init__(self, dmin, dmax):
-        self.dmin, self.dmax, self.H = dmin, dmax, dmax + 4
+        self.dmin, self.dmax = dmin, dmax
+        self.H = dmax + max(4, min(MAX_WINDOW, dmin))
+        self.mask = ACC_BUFFERS - 1
+        self.buf = {}          # buffer -> [step it holds, phase of the update that consumed it]
         self.phase = 0
         self.updated = {}      # step -> phase of its update
         self.delivered = {}    # step -> phase of its delivery
@@ -35,6 +42,7 @@ class Schedule:
         self.step = 0
         # start state: arrivals of step 0 delivered (nothing to deliver), slot 0 clear
         self.delivered[0] = -1
+        self.buf[0] = [0, None]
         self.cleared.setdefault(0, []).append((-1, 0))
 
     # ---- actions inside a phase ------------------------------------------
@@ -45,9 +53,10 @@ class Schedule:
             if x >= 0:
                 assert self.updated.get(x, 1 << 30) < self.phase, f"step {sa} reads unfinished step {x}"
                 self.reads.append((self.phase, x))
-        prev = sa - ACC_BUFFERS  # the buffer's previous step: input consumed before the write
-        if prev >= 0:
-            assert self.updated.get(prev, 1 << 30) < self.phase, f"buffer of {sa} still holds {prev}"
+        held = self.buf.get(sa & self.mask)  # the buffer's previous step: input consumed before the write
+        if held is not None:
+            assert held[1] is not None and held[1] < self.phase, f"buffer of {sa} still holds {held[0]}"
+        self.buf[sa & self.mask] = [sa, None]
         self.delivered[sa] = self.phase
 
     def update(self, x):
@@ -55,6 +64,9 @@ class Schedule:
         assert x not in self.updated
         slot_clears = [p for p, y in self.cleared.get(x % self.H, []) if y == x]
         assert slot_clears and slot_clears[-1] < self.phase, f"slot of step {x} not cleared before its update"
+        held = self.buf.get(x & self.mask)
+        assert held is not None and held[0] == x and held[1] is None, f"step {x} reads another step's buffer"
+        held[1] = self.phase
         self.updated[x] = self.phase
 
     def clear(self, y):
@@ -68,6 +80,19 @@ class Schedule:
         self.phase += 1
 
     # ---- the kernels ------------------------------------------------------
+    def set_cycle(self, mask):
+        """The host's switch between runs (k_acc_move): only the current
+        step's buffer holds input; it moves to its place in the new cycle and
+        its old buffer is left zero."""
+        for x, used in self.buf.values():
+            assert x == self.step or used is not None, f"buffer of step {x} in use at a switch"
+        old, cur = self.step & self.mask, self.buf.get(self.step & self.mask)
+        if cur is not None and cur[0] == self.step and (self.step & mask) != old:
+            self.buf[old] = [None, -1]
+            self.buf[self.step & mask] = cur
+        self.mask = mask
+        self.barrier()
+
     def fused_step(self):
         """k_fused: update step s, deliver step s+1, the epilogue clears slot s+1."""
         s = self.step
@@ -79,6 +104,7 @@ class Schedule:
         self.step = s + 1
 
     def window_group(self, nsteps, W):
+        assert W <= self.mask + 1, "a window's steps need distinct buffers"
         s0, s_end = self.step, self.step + nsteps
         n = nsteps - 1 if nsteps < W else W - 1
         for k in range(1, n + 1):
@@ -134,10 +160,13 @@ def test_window_schedule_orderings(seed):
     # the single-step kernels need arrivals of the current step delivered: true at start
     for _ in range(30):
         if rng.random() < 0.25:
+            sch.set_cycle(ACC_BUFFERS - 1)
             for _ in range(rng.randint(1, 5)):
                 sch.fused_step()
         else:
             W = rng.randint(1, min(MAX_WINDOW, dmin))
+            # the host's choice of cycle (wanted_acc_mask): 8 buffers for W > 4
+            sch.set_cycle(ACC_BUFFERS_WIDE - 1 if W > ACC_BUFFERS else ACC_BUFFERS - 1)
             sch.window_group(rng.randint(1, 40), W)
     # every step up to the clock was updated once; arrivals of the clock's step are in
     assert sorted(sch.updated) == list(range(sch.step))
@@ -145,15 +174,33 @@ def test_window_schedule_orderings(seed):
     sch.check_slots()
 
 
-def test_window_schedule_catches_a_short_history():
-    """The check has teeth, and H = max delay + 4 is the least history a window
-    of 4 needs: with max delay + 3 slots it clears the next window's last slot
-    while a delivery of the same phase still reads the step it held."""
-    sch = Schedule(4, 6)
-    sch.H = 6 + 3
-    sch.window_group(16, 4)
+@pytest.mark.parametrize("W", [4, 8])
+def test_window_schedule_catches_a_short_history(W):
+    """The check has teeth, and H = max delay + W is the least history a window
+    of W needs: with max delay + W - 1 slots it clears the next window's last
+    slot while a delivery of the same phase still reads the step it held."""
+    sch = Schedule(W, W + 2)
+    sch.H = W + 2 + W - 1
+    if W > ACC_BUFFERS:
+        sch.set_cycle(ACC_BUFFERS_WIDE - 1)
+    sch.window_group(4 * W, W)
     with pytest.raises(AssertionError, match="cleared"):
         sch.check_slots()
+
+
+def test_window_schedule_catches_a_wide_window_in_four_buffers():
+    """A window of 5 steps or more in the 4-buffer cycle: window_group
+    refuses it, and without that guard the buffer check catches the fifth
+    step's delivery into the buffer of a step the window has not updated."""
+    sch = Schedule(8, 20)
+    with pytest.raises(AssertionError, match="distinct buffers"):
+        sch.window_group(16, 8)
+    sch = Schedule(8, 20)
+    for k in range(1, 8):
+        sch.clear(k)
+    with pytest.raises(AssertionError, match="still holds"):
+        for k in range(1, 8):
+            sch.deliver(k)
 
 
 def test_window_schedule_catches_a_long_window():
