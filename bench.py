@@ -481,6 +481,13 @@ def run_ours(a, ws, rank, local):
                                  "step_group": simf.info()["persistent"], "fx_shift": simf.info()["fx_shift"]}
         simf.close()
 
+    pull = None
+    if rank == 0 and not a.no_pull:
+        try:
+            pull = pull_variant(local)
+        except Exception as e:  # a side leg: its failure does not void the line
+            pull = {"unavailable": f"{type(e).__name__}: {e}"}
+
     cpu = parity = None
     if rank == 0 and not a.no_cpu:
         try:
@@ -514,13 +521,57 @@ def run_ours(a, ws, rank, local):
             "roofline": roofline, "kernels": kern, "e2e": e2e, "cpu_baseline": cpu,
             "clocks": clk.summary(), "gpu_launches": int(launches), "parity": parity,
             "reference_gpu": reference_gpu,
-            "build_s": build_s, "autotune": tune, "driven_variant": driven,
+            "build_s": build_s, "autotune": tune, "driven_variant": driven, "pull_variant": pull,
             "delivery_ceiling": {"reductions_per_s": red_ceiling, "stream_read_gbs": read_ceiling / 1e9,
                                  "how": "mgc_measure_scatter: 1e8 random fp32 red.add into 2^20 "
                                         "accumulators fed by streamed 8-byte records; plain stream "
                                         "of the same records"},
         }
         print(json.dumps(line), flush=True)
+
+
+def pull_variant(local, steps=3000, warm=1000):
+    """Pull steps on the load they are for: the bursting network of
+    mgbrain_b200.brunel.burst_network (10k LIFB, 1.1e7 synapses, volleys of
+    more than half the neurons).  Device time of `steps` steps after `warm`,
+    with the autotuner's push-only form, the windowed group pushing, and the
+    windowed group with pull steps at three thresholds ((spike, delay) pairs
+    per step); every end state compared with the push-only one."""
+    from mgbrain_b200 import brunel
+    net = brunel.burst_network()
+    S = len(net["src"])
+    out = {"network": "burst: 8k exc + 2k inh LIFB, 1k POISSON @100 Hz, in-degree 800/200/100, J 0.1 mV, g 2, "
+                      "one 1.5 ms delay (tests/burst_net.py); fires in volleys",
+           "synapses": S, "steps": steps, "forms": {}}
+    ref = None
+    for label, pull, tune in (("push_autotuned", 0, True), ("push_window8", 0, False),
+                              ("pull_500", 500, False), ("pull_1500", 1500, False), ("pull_3000", 3000, False)):
+        sim = brunel.burst_simulator(net, device=local, raster_ids=-1)
+        if tune:
+            t = sim.autotune(steps_per_trial=640)
+            form = {"persistent": t["persistent"], "window": t["window"], "chunk_len": t["chunk_len"]}
+        else:
+            sim.set_persistent(3)
+            sim.set_window(8)
+            sim.set_pull(pull)
+            form = {"persistent": 3, "window": 8, "pull_min_pairs": pull}
+        left = warm + steps - sim.info()["step"]
+        sim.run(max(0, left - steps))
+        sim.sync()
+        ms, ev, _ = timed_device(sim, steps, 1, 1)
+        st = sim.state()
+        end = (sim.info()["step"], st["V"].tobytes(), st["fire_cnt"].tobytes())
+        if label == "push_window8":
+            ref = end
+        out["forms"][label] = {"us_per_step": 1e3 * ms / steps, "events_per_s": ev / (ms / 1e3),
+                               "events_per_step": ev / steps, "form": form,
+                               "end_state_equal_push": None if ref is None or tune else end == ref}
+        sim.close()
+    best = min((v["us_per_step"], k) for k, v in out["forms"].items() if k.startswith("pull"))
+    push = min(out["forms"]["push_autotuned"]["us_per_step"], out["forms"]["push_window8"]["us_per_step"])
+    out["best_pull"] = best[1]
+    out["speedup_over_best_push"] = push / best[0]
+    return out
 
 
 def run_partition(a, ws, rank, local):
@@ -970,6 +1021,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=200)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-driven", action="store_true")
+    ap.add_argument("--no-pull", action="store_true", help="skip the bursting network's pull-step leg")
     ap.add_argument("--no-refgpu", action="store_true",
                     help="skip the reference's own kernels on this GPU (reference_gpu key)")
     ap.add_argument("--ref-syn", type=float, default=1e8)

@@ -436,6 +436,25 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * counterpart. */
 mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
 
+/* Pull steps (deferred method, minimum delay >= 2, not for partition
+ * handles): in the windowed step group (mgc_set_persistent mode 3), a step
+ * whose arrivals come from at least `min_pairs` (spike, delay) pairs is
+ * delivered by pull instead of push: one warp per target walks the target's
+ * incoming row and adds the weights of the synapses whose source spiked at
+ * the step minus the delay (the spike history kept as a bitmap per step),
+ * with no atomics.  A pull reads every incoming synapse, so it pays off only
+ * on steps where a large part of the network's sources send (synchronous
+ * bursts: one burst of a dense network can put hundreds of events on every
+ * target in one step).  The choice is made on the device per step from the
+ * spike counts the delivery already holds; results are those of the push
+ * bit for bit (fixed-point sums exact; fp32 sums need one weight per sign,
+ * else the call returns MGC_ERR_INVALID).  The first call builds the
+ * incoming rows (8 bytes per synapse) and the bitmaps, which every step form
+ * then writes; steps whose sources ran before it are pushed.  0 turns pull
+ * steps off.  No reference counterpart (the reference always pushes,
+ * mgcore.cu:271-305). */
+mgc_status mgc_set_pull(mgc_sim* sim, int32_t min_pairs);
+
 /* Chooses how inputs are summed (MGC_ACC_FLOAT or MGC_ACC_FIXED, see
  * above), before the handle's first step (MGC_ERR_INVALID after it, or for
  * FIXED with the pull method).  No reference counterpart. */

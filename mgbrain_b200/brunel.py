@@ -91,3 +91,37 @@ def sweep_alone(instances, i, seed=1, **kw):
     return Simulator.fixed_indegree(b["pops"], b["projs"], brunel_lifconst(), rate=b["rate"],
                                     v_init=b["v_init"], conn_seed=b["conn_seed"], seed=seed,
                                     id_offset=start, proj_offset=proj_off, **kw)
+
+
+def burst_network(ne=8000, ni=2000, nx=1000, ke=800, ki=200, kx=100, J=1e-4, g=2.0, d=15, rate=0.01, seed=0):
+    """A Brunel network in the synchronous regime, the load pull steps
+    (Simulator.set_pull) are for: ne exc + ni inh LIFB with the large
+    network's neuron constants, nx POISSON inputs at `rate` per step, fixed
+    in-degree ke exc / ki inh / kx inputs per neuron (sources drawn with
+    numpy's default_rng(seed)), J, g = 2 (excitation dominates), one delay of
+    d steps.  It fires in volleys: in some steps more than half of the
+    neurons spike, and their events (about ke + ki per spike) arrive
+    together d steps later.  Returns the synapse list and the arrays
+    Simulator.from_arrays takes (delays in steps)."""
+    rng = np.random.default_rng(seed)
+    n = ne + ni + nx
+    types = np.array([LIFB] * (ne + ni) + [POISSON] * nx, np.int8)
+    k = ke + ki + kx
+    src = np.empty((ne + ni, k), np.int32)
+    src[:, :ke] = rng.integers(0, ne, (ne + ni, ke))
+    src[:, ke:ke + ki] = ne + rng.integers(0, ni, (ne + ni, ki))
+    src[:, ke + ki:] = ne + ni + rng.integers(0, nx, (ne + ni, kx))
+    src = src.reshape(-1)
+    tar = np.repeat(np.arange(ne + ni, dtype=np.int32), k)
+    w = np.where(src < ne, J, np.where(src < ne + ni, -g * J, J)).astype(np.float32)
+    r = np.zeros(n, np.float32)
+    r[ne + ni:] = rate
+    v0 = np.random.default_rng(seed + 1).uniform(0.0, 0.02, n).astype(np.float32)
+    return dict(n=n, type=types, rate=r, src=src, tar=tar, weight=w, dsteps=np.full(len(src), d, np.int32),
+                lifconst=brunel_lifconst(), v0=v0, d=d)
+
+
+def burst_simulator(net, seed=3, **kw):
+    """The handle of a burst_network (Simulator.from_arrays)."""
+    return Simulator.from_arrays(net["n"], net["type"], net["src"], net["tar"], net["weight"], net["dsteps"],
+                                 net["lifconst"], rate=net["rate"], v_init=net["v0"], seed=seed, **kw)

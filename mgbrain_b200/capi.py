@@ -31,7 +31,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_set_window", "mgc_checkpoint_size",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_set_window", "mgc_set_pull", "mgc_checkpoint_size",
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
@@ -188,6 +188,8 @@ def lib():
     L.mgc_autotune.restype = C.c_int
     L.mgc_set_persistent.argtypes = [vp, i32]
     L.mgc_set_persistent.restype = C.c_int
+    L.mgc_set_pull.argtypes = [vp, i32]
+    L.mgc_set_pull.restype = C.c_int
     L.mgc_set_window.argtypes = [vp, i32]
     L.mgc_set_window.restype = C.c_int
     L.mgc_create_generated.argtypes = [C.POINTER(GenDesc), C.POINTER(vp)]
@@ -606,6 +608,12 @@ class Simulator:
         """ACC_FLOAT (fp32 additions) or ACC_FIXED (order-independent 64-bit
         fixed point), before the first step (mgc_set_accumulation)."""
         check(lib().mgc_set_accumulation(self._h, int(mode)))
+
+    def set_pull(self, min_pairs):
+        """Pull steps of the windowed group: a step whose arrivals come from at
+        least min_pairs (spike, delay) pairs is delivered by pull (mgc_set_pull);
+        0 turns them off.  Results are unchanged."""
+        check(lib().mgc_set_pull(self._h, int(min_pairs)))
 
     def set_window(self, steps):
         """Steps per window of the windowed step group (1..min(8, min delay))."""

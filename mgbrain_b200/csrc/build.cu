@@ -99,6 +99,35 @@ __global__ void k_pull_keys(const int32_t* src, const int32_t* tar, const int32_
     }
 }
 
+// Pull steps of the deferred method: for every CSR position its target (the
+// sort key) and its source (one warp per source row of the bucketed CSR).
+__global__ void k_row_sources(const int64_t* bucket, int32_t n_src, int D, const uint2* syn, uint32_t tmask,
+                              uint32_t* tkey, uint32_t* pos, int32_t* src_of)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n_src; r += nw) {
+        const int64_t b = bucket[(size_t)r * D], e = bucket[(size_t)r * D + D];
+        for (int64_t p = b + lane; p < e; p += 32) {
+            tkey[p] = syn[p].x & tmask;
+            pos[p] = (uint32_t)p;
+            src_of[p] = (int32_t)r;
+        }
+    }
+}
+
+// Incoming entries {source | delay << tbits, weight} in target order.
+__global__ void k_gather_in(const uint32_t* order, const uint2* syn, const int32_t* src_of, int64_t S, uint32_t tmask,
+                            uint2* in_ent)
+{
+    GRID_STRIDE(i, S)
+    {
+        const uint32_t p = order[i];
+        const uint2 w = syn[p];
+        in_ent[i] = make_uint2((w.x & ~tmask) | (uint32_t)src_of[p], w.y);
+    }
+}
+
 __global__ void k_gather_pull(const uint32_t* order, const int32_t* src, const float* w, const int32_t* delay,
                               const uint8_t* plastic_in, int64_t S, int tbits, uint2* ent, int64_t* ent_syn,
                               uint8_t* plastic_out)
@@ -573,6 +602,7 @@ FxPlan fx_plan_blocks(const mgc_fixed_indegree_desc* blocks, int32_t n_blocks)
 // except for the pull method, whose per-target pass adds in a fixed order.
 void apply_fx(mgc_sim* s, const FxPlan& p)
 {
+    s->hetero = p.hetero;
     s->fx_shift = p.shift;
     s->a.fx = p.hetero && !s->a.pull ? 1 : 0;
     s->a.fx_scale = std::ldexp(1.0f, p.shift);
@@ -623,9 +653,11 @@ mgc_status launch_shapes(mgc_sim* s)
                 }
             for (int wide = 0; wide < 2; ++wide)
                 for (int v = 0; v < 2; ++v) {
-                    const WindowKernel k = window_kernel(s, v, wide);
-                    CK(cudaFuncSetAttribute((const void*)k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)s->window_smem[wide]));
+                    for (int pl = 0; pl < 2; ++pl)
+                        CK(cudaFuncSetAttribute((const void*)window_kernel(s, v, wide, pl),
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->window_smem[wide]));
+                    // both forms of a variant are compiled for the same blocks per SM
+                    const WindowKernel k = window_kernel(s, v, wide, false);
                     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kPushBlock, s->window_smem[wide]));
                     s->window_grid_v[wide][v] = sms * std::min(std::max(1, occ), v == 0 ? 2 : 3);
                 }
@@ -798,6 +830,55 @@ mgc_status csr_from_list(mgc_sim* s, int32_t* src, int32_t* tar, float* w, int32
     return MGC_OK;
 }
 
+
+// The deferred method's incoming rows and history bitmaps for pull steps
+// (mgc_set_pull), built once from the handle's CSR: rows by target, in CSR
+// order inside (a stable sort), entries {source | delay << tbits, weight}.
+mgc_status build_in_rows(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    if (a.in_ent) return MGC_OK;
+    const int64_t S = s->S;
+    if (S >= (int64_t(1) << 32)) return fail(MGC_ERR_INVALID, "pull steps need fewer than 2^32 synapses");
+    int64_t* in_ptr = nullptr;
+    uint2* in_ent = nullptr;
+    uint32_t* bits = nullptr;
+    const int64_t groups = a.ns / 4;
+    const int32_t words = (int32_t)((groups + 31) / 32 * 4);
+    CKS(s->alloc(&in_ptr, (size_t)s->n + 1));
+    CKS(s->alloc(&in_ent, (size_t)std::max<int64_t>(S, 1), false));
+    CKS(s->alloc(&bits, (size_t)a.H * (size_t)words));
+    int64_t* span = nullptr;
+    CKS(s->alloc(&span, 2));
+    {
+        DevTmp t_k, t_k2, t_p, t_o, t_s;
+        uint32_t *k, *k2, *pos, *order;
+        int32_t* src_of;
+        CKS(tmp_alloc(t_k, &k, S));
+        CKS(tmp_alloc(t_k2, &k2, S));
+        CKS(tmp_alloc(t_p, &pos, S));
+        CKS(tmp_alloc(t_o, &order, S));
+        CKS(tmp_alloc(t_s, &src_of, S));
+        if (S > 0) {
+            k_row_sources<<<grid_for((int64_t)s->n_src * 32), 256, 0, s->stream>>>(a.bucket, s->n_src, a.D, a.syn,
+                                                                                    a.tmask, k, pos, src_of);
+            CKS(sort_pairs(k, k2, pos, order, S, a.tbits, s->stream));
+            k_gather_in<<<grid_for(S), 256, 0, s->stream>>>(order, a.syn, src_of, S, a.tmask, in_ent);
+            k_count_rows<<<grid_for(S), 256, 0, s->stream>>>(k2, S, 0, in_ptr);
+        }
+        CKS(exclusive_scan(in_ptr, s->n, s->stream));
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    a.in_ptr = in_ptr;
+    a.in_ent = in_ent;
+    a.hist_bits = bits;
+    a.bits_words = words;
+    a.bits_span = span;
+    const int64_t none[2] = {0, -1};  // no step has its bitmap yet
+    CK(cudaMemcpy(span, none, sizeof(none), cudaMemcpyHostToDevice));
+    return MGC_OK;
+}
 
 }  // namespace mgc
 

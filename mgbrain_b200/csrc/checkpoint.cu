@@ -124,6 +124,10 @@ mgc_status mgc_checkpoint_load(mgc_sim* s, const void* buf, int64_t bytes)
     CK(cudaMemcpy(&step, s->a.step, 8, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(s->a.raster_step0, &step, 8, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->a.raster_pos, &zero, 8, cudaMemcpyHostToDevice));
+    if (s->a.bits_span) {  // the spike bitmaps of pull steps are not part of it
+        const int64_t none[2] = {0, -1};
+        CK(cudaMemcpy(s->a.bits_span, none, sizeof(none), cudaMemcpyHostToDevice));
+    }
     CK(cudaMemcpy(s->a.status, &zero32, 4, cudaMemcpyHostToDevice));
     if (s->a.ev_mark) {
         unsigned long long ev = 0;

@@ -129,6 +129,15 @@ struct StepArgs {
     unsigned long long* ev_mark;  // events counter at the previous step's end
     unsigned int* bar;        // [4] step-group barriers: arrivals + generation (k_steps, k_steps1),
                               //     phase arrival counters (k_pipe)
+    // deferred method, pull steps of the windowed group (mgc_set_pull): the
+    // incoming rows in_ptr / in_ent (by target, synapse-CSR order inside) and
+    // the spikes of every history slot as a bitmap, which that group writes
+    uint32_t* hist_bits;      // [H][bits_words] bit i of the slot: neuron i spiked at its step
+    int32_t bits_words;       // words per slot (4 per 32 neuron groups)
+    int32_t pull_min;         // a step whose arrivals come from at least this many (spike, delay)
+                              //   pairs is delivered by pull (0: never)
+    int64_t* bits_span;       // [2] the steps [from, end) whose bitmaps the group wrote, one run
+                              //   of groups without other step forms between them
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
@@ -386,6 +395,7 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
     int32_t* ids = step_ids(a, hslot);
     int32_t* cnt = step_count(a, hslot);
     const bool rec = raster && (a.deferred || a.pull) && a.record;  // no push kernel to record
+
     for (int64_t gb = warp * 32 * G; gb < ngroups; gb += nwarps * 32 * G) {
         char4 t4[G];
         float4 v4[G], ce4[G], ci4[G];
@@ -898,7 +908,7 @@ constexpr int kWinLoad = 4;  // input slots a lane holds at once
 // group of four neurons per lane per pass: its state is loaded once, its
 // input slots four steps at a time, the steps run in registers, the state is
 // stored once.
-template <bool CUR, bool FX, int WMAX>
+template <bool CUR, bool FX, int WMAX, bool PULL>
 __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int wl, int32_t hs0, int64_t warp,
                                               int64_t nwarps)
 {
@@ -954,6 +964,16 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                     In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
                     In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_i, s), g);
                 }
+                if (PULL) {  // the step's spikes as a bitmap (pull steps read it)
+                    int32_t hb = hs0 + h + k;
+                    if (hb >= a.H) hb -= a.H;
+                    unsigned wv = fm << (4 * (lane & 7));
+                    wv |= __shfl_xor_sync(0xffffffffu, wv, 1);
+                    wv |= __shfl_xor_sync(0xffffffffu, wv, 2);
+                    wv |= __shfl_xor_sync(0xffffffffu, wv, 4);
+                    if ((lane & 7) == 0 && gb < ngroups)
+                        a.hist_bits[(size_t)hb * (size_t)a.bits_words + (gb >> 3) + (lane >> 3)] = wv;
+                }
                 // the step's spikes into its history slot, in neuron order within
                 // the warp (no scan when no lane spiked)
                 if (!__any_sync(0xffffffffu, fm != 0)) continue;
@@ -996,20 +1016,135 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
 // before sa0: the prefixes of the n steps by the first n warps, then every
 // warp through the n steps' tasks without a barrier between them.  s, hslot:
 // a step and its history slot, for the slot arithmetic.
-template <bool FX, int WMAX>
+// fp32 addition with the rounding and subnormal flushing of red.add.f32
+__device__ __forceinline__ float fadd_ftz(float x, float y)
+{
+    float r;
+    asm("add.rn.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(x), "f"(y));
+    return r;
+}
+
+// Pull delivery of the arrivals of the steps in `mask` (bit k: step sa0 + k):
+// one warp per (step x, target t) walks t's incoming row and adds the
+// weights of the synapses whose source spiked at step x - delay (the history
+// slots' bitmaps), then stores the sums into the accumulators of step x,
+// which nothing else writes for a pulled step.  No atomics, and the sum is
+// the one the push computes: with fixed-point accumulation the exact integer
+// sum; with fp32 sums every neuron receives one weight per sign (the handle
+// refuses pull steps otherwise), and k additions of one weight give the same
+// bits in any order, here a chain of k additions from zero with red.add's
+// rounding (lane 0 the exc sum, lane 1 the inh).  Work starts at the first
+// warp (push tasks start at the last).
+template <bool FX, int MASK>
+__device__ __forceinline__ void pull_steps(const StepArgs& a, int64_t sa0, unsigned mask, int64_t s, int32_t hslot,
+                                           int64_t warp, int64_t nwarps, unsigned long long* blk_ev)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t n = a.n;
+    const int64_t total = (int64_t)__popc(mask) * n;
+    unsigned long long ev = 0;
+    for (int64_t it = warp; it < total; it += nwarps) {
+        const int j = (int)(it / n);  // the j-th pulled step
+        const int32_t t = (int32_t)(it - (int64_t)j * n);
+        unsigned m = mask;
+        for (int q = 0; q < j; ++q) m &= m - 1;
+        const int64_t x = sa0 + (__ffs(m) - 1);
+        const int32_t hx = hist_slot(a, x, s, hslot);
+        const int64_t rb = a.in_ptr[t], re = a.in_ptr[t + 1];
+        int ce = 0, ci = 0;
+        long long fe = 0, fi = 0;
+        float we = 0.f, wi = 0.f;
+        for (int64_t q0 = rb; q0 < re; q0 += 32 * kDeliverUnroll) {
+            uint2 e[kDeliverUnroll];
+#pragma unroll
+            for (int u = 0; u < kDeliverUnroll; ++u) {
+                const int64_t q = q0 + u * 32 + lane;
+                e[u] = q < re ? __ldcs(a.in_ent + q) : make_uint2(0u, 0u);
+            }
+#pragma unroll
+            for (int u = 0; u < kDeliverUnroll; ++u) {
+                if (q0 + u * 32 + lane >= re) continue;
+                const int32_t src = (int32_t)(e[u].x & a.tmask);
+                const int32_t d = (int32_t)(e[u].x >> a.tbits);
+                if (!MGC_OK_INDEX(src < a.n && d >= a.dmin && d < a.dmin + a.D)) continue;
+                int32_t h = hx - d;
+                if (h < 0) h += a.H;
+                if (!((a.hist_bits[(size_t)h * (size_t)a.bits_words + (src >> 5)] >> (src & 31)) & 1u)) continue;
+                const float w = as_f(e[u].y);
+                if (w > 0.0f) {
+                    ++ce;
+                    we = w;
+                    if (FX) fe += to_fx(w, a.fx_scale);
+                } else {
+                    ++ci;
+                    wi = w;
+                    if (FX) fi += to_fx(w, a.fx_scale);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            ce += __shfl_xor_sync(0xffffffffu, ce, o);
+            ci += __shfl_xor_sync(0xffffffffu, ci, o);
+            if (FX) {
+                fe += __shfl_xor_sync(0xffffffffu, fe, o);
+                fi += __shfl_xor_sync(0xffffffffu, fi, o);
+            }
+        }
+        if (!FX) {  // the weight of each sign (the same on every lane that saw one)
+            const unsigned he = __ballot_sync(0xffffffffu, we != 0.0f), hi = __ballot_sync(0xffffffffu, wi != 0.0f);
+            we = he ? __shfl_sync(0xffffffffu, we, __ffs(he) - 1) : 0.0f;
+            wi = hi ? __shfl_sync(0xffffffffu, wi, __ffs(hi) - 1) : 0.0f;
+        }
+        if (lane == 0) ev += (unsigned long long)(ce + ci);
+        if (lane < 2 && (lane == 0 ? ce : ci)) {
+            float* base = lane == 0 ? a.acc_e : a.acc_i;
+            if (FX) {
+                acc_buf<true, MASK>(a, base, x)[t] = (unsigned long long)(lane == 0 ? fe : fi);
+            } else {
+                const float w = lane == 0 ? we : wi;
+                const int c = lane == 0 ? ce : ci;
+                float v = 0.0f;
+                for (int r = 0; r < c; ++r) v = fadd_ftz(v, w);
+                acc_buf<false, MASK>(a, base, x)[t] = v;
+            }
+        }
+    }
+    if (lane == 0 && ev) atomicAdd(blk_ev ? blk_ev : a.events, ev);
+}
+
+template <bool FX, int WMAX, bool PULL>
 __device__ __forceinline__ void deliver_window(const StepArgs& a, int64_t sa0, int n, int64_t s, int32_t hslot,
-                                               int64_t* pre, int64_t warp, int64_t nwarps, unsigned long long* blk_ev)
+                                               int64_t* pre, int64_t warp, int64_t nwarps, unsigned long long* blk_ev,
+                                               int64_t bits_from)
 {
     const int wib = threadIdx.x >> 5;
     for (int k = wib; k < n; k += blockDim.x >> 5) deliver_prefix(a, sa0 + k, s, hslot, pre + (size_t)k * (a.D + 1));
     __syncthreads();
+    unsigned pull = 0;
+    if (PULL && a.pull_min > 0) {
+        // the steps delivered by pull: many arriving (spike, delay) pairs, and
+        // every step they come from has its bitmap (every block takes the
+        // same decision from the same counts)
+        const int64_t dmax = (int64_t)a.dmin + a.D - 1;
+        for (int k = 0; k < n; ++k)
+            if (pre[(size_t)k * (a.D + 1) + a.D] >= a.pull_min && sa0 + k - dmax >= bits_from) pull |= 1u << k;
+        if (pull) {  // their push tasks emptied
+            __syncthreads();
+            for (int k = 0; k < n; ++k)
+                if ((pull >> k) & 1u)
+                    for (int j = threadIdx.x; j <= a.D; j += blockDim.x) pre[(size_t)k * (a.D + 1) + j] = 0;
+            __syncthreads();
+        }
+    }
     deliver_tasks<FX, WMAX, WMAX - 1>(a, sa0, s, hslot, pre, warp, nwarps, blk_ev, n);
+    if (PULL && pull) pull_steps<FX, WMAX - 1>(a, sa0, pull, s, hslot, warp, nwarps, blk_ev);
 }
 
 __device__ __forceinline__ void raster_copy(const StepArgs& a, int64_t sc, int32_t hs, int64_t rstep0,
                                             int64_t& rbase);
 
-template <bool CUR, int MINB, bool FX, int WMAX>
+template <bool CUR, int MINB, bool FX, int WMAX, bool PULL>
 __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t nsteps, int32_t W)
 {
     extern __shared__ int64_t wpre[];   // [WMAX][D + 1]
@@ -1025,6 +1160,10 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
     const int64_t rstep0 = *a.raster_step0;
     const int64_t s_end = s0 + nsteps;
     auto hs_of = [&](int64_t x) { return (int32_t)((h0 + (x - s0)) % a.H); };
+    // pull steps: the bitmaps written since `bits_from`, if the previous
+    // steps were this group's too, else from s0 on
+    int64_t bits_from = s0;
+    if (PULL && *(volatile int64_t*)(a.bits_span + 1) == s0) bits_from = *(volatile int64_t*)a.bits_span;
     if (threadIdx.x == 0) {
         abort_flag = 0;
         blk_ev = 0;
@@ -1036,12 +1175,12 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         if (lead)
             for (int k = 1; k <= n; ++k) a.hist_cnt[hs_of(s0 + k)] = 0;
         __syncthreads();
-        if (n > 0) deliver_window<FX, WMAX>(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev);
+        if (n > 0) deliver_window<FX, WMAX, PULL>(a, s0 + 1, n, s0, h0, wpre, warp, nwarps, &blk_ev, bits_from);
         if (!grid_barrier(a, &abort_flag)) return;
     }
     for (int64_t w0 = s0; w0 < s_end;) {
         const int wl = (int)(s_end - w0 < W ? s_end - w0 : W);
-        neuron_window<CUR, FX, WMAX>(a, w0, wl, hs_of(w0), warp, nwarps);
+        neuron_window<CUR, FX, WMAX, PULL>(a, w0, wl, hs_of(w0), warp, nwarps);
         if (!grid_barrier(a, &abort_flag)) return;
         // the window's spikes are complete: its raster, then the next
         // window's arrivals (only those of s_end after the last window)
@@ -1051,7 +1190,7 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         const int nn = (int)(next < s_end ? (s_end - next < W ? s_end - next : W) : 1);
         if (lead)
             for (int k = 0; k < nn; ++k) a.hist_cnt[hs_of(next + k)] = 0;
-        deliver_window<FX, WMAX>(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev);
+        deliver_window<FX, WMAX, PULL>(a, next, nn, w0, hs_of(w0), wpre, warp, nwarps, &blk_ev, bits_from);
         if (next >= s_end) {  // the block's events, before the last barrier
             __syncthreads();
             if (threadIdx.x == 0 && blk_ev) atomicAdd(a.events, blk_ev);
@@ -1064,6 +1203,10 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_window(StepArgs a, int32_t
         *a.ev_mark = *(volatile unsigned long long*)a.events;
         a.slots[0] = (int32_t)((slot0 + nsteps) % a.M);
         a.slots[1] = hs_of(s_end);
+        if (PULL) {
+            a.bits_span[0] = bits_from;
+            a.bits_span[1] = s_end;
+        }
         __threadfence();
         *a.step = s_end;
     }

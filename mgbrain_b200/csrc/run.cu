@@ -282,8 +282,9 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
                 if (s->a.acc_mask != (wide ? kAccBuffersWide : kAccBuffers) - 1)
                     return fail(MGC_ERR_INVALID, "a window of %d steps in the %d-buffer cycle", w, s->a.acc_mask + 1);
                 void* wargs[] = {&ga, &n, &w};
-                e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v, wide), dim3(s->window_grid_v[wide][v]),
-                                                dim3(kPushBlock), wargs, s->window_smem[wide], s->stream);
+                e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v, wide, s->a.pull_min > 0),
+                                                dim3(s->window_grid_v[wide][v]), dim3(kPushBlock), wargs,
+                                                s->window_smem[wide], s->stream);
             } else {
                 const int grid = s->fused ? s->group_grid_v[p - 1][v] : s->group_grid1;
                 e = cudaLaunchCooperativeKernel((const void*)steps_kernel(s, p, v), dim3(grid), dim3(kPushBlock),

@@ -126,6 +126,7 @@ struct mgc_sim {
     int acc_buffers = 4;              // accumulator buffers allocated (8 for a minimum delay >= 5)
     int group_grid1 = 1;              // minimum delay 1: the step group's grid
     int32_t fx_shift = 0;             // fixed-point shift the builder picked for this network's weights
+    bool hetero = false;              // some neuron receives unequal weights of one sign
     int32_t sched_mode_h = 0;         // host mirrors of what decides the graph's shape
     bool sched_collect_h = false, sched_forced_h = false;
 
@@ -213,8 +214,8 @@ StepKernel fused_kernel(const mgc_sim* s, int v);
 GroupKernel steps_kernel(const mgc_sim* s, int p, int v);
 GroupKernel pipe_kernel(const mgc_sim* s, int v);
 // The windowed step group of variant v: for windows of up to 4 steps, or
-// (wide) of up to 8.
-WindowKernel window_kernel(const mgc_sim* s, int v, bool wide);
+// (wide) of up to 8; with pull steps (mgc_set_pull) or without.
+WindowKernel window_kernel(const mgc_sim* s, int v, bool wide, bool pull);
 // The scheduler's decision kernel (sched.cu).
 const void* sched_decide_kernel();
 
@@ -240,6 +241,9 @@ mgc_status build_finish(mgc_sim* s);
 // bits; with `exact`, no finer than the smallest weight's last mantissa bit
 // (min_exp: its frexp exponent).
 int32_t fx_shift_rule(double bound, int min_exp, bool exact);
+// The incoming rows and history bitmaps of the deferred method's pull steps,
+// built once (mgc_set_pull).
+mgc_status build_in_rows(mgc_sim* s);
 // Segments of up to `gap` synapses cut into chunks of about `target`.
 void set_chunking(StepArgs& a, int64_t gap, int64_t target);
 

@@ -162,6 +162,29 @@ mgc_status mgc_set_persistent(mgc_sim* s, int32_t mode)
     return MGC_OK;
 }
 
+mgc_status mgc_set_pull(mgc_sim* s, int32_t min_pairs)
+{
+    if (!s) return fail(MGC_ERR_INVALID, "null handle");
+    if (min_pairs < 0) return fail(MGC_ERR_INVALID, "pull threshold %d (0 turns pull steps off)", min_pairs);
+    StepArgs& a = s->a;
+    if (min_pairs > 0) {
+        if (!s->fused) return fail(MGC_ERR_INVALID, "pull steps need the deferred method with a minimum delay >= 2");
+        if (s->partition) return fail(MGC_ERR_INVALID, "pull steps are not available for partition handles");
+        if (s->hetero && !a.fx)
+            return fail(MGC_ERR_INVALID, "pull steps with unequal weights of one sign need fixed-point accumulation");
+    }
+    CK(cudaSetDevice(s->device));
+    if (s->graph) {  // its launches hold the old arguments
+        CK(cudaStreamSynchronize(s->stream));
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+        s->sched_graph = false;
+    }
+    if (min_pairs > 0) CKS(build_in_rows(s));
+    a.pull_min = min_pairs;
+    return MGC_OK;
+}
+
 mgc_status mgc_set_window(mgc_sim* s, int32_t steps)
 {
     if (!s) return fail(MGC_ERR_INVALID, "null handle");
