@@ -399,7 +399,7 @@ typedef struct mgc_tune_report {
     int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
     int32_t persistent;           /* chosen step-group mode of the fused method (mgc_set_persistent) */
     int32_t window;               /* chosen window of the windowed step group (mgc_set_window) */
-    int32_t reserved;
+    int32_t pull_min;             /* chosen pull-step threshold (mgc_set_pull), 0: none */
     double ms_per_step;           /* time per step of the chosen configuration */
     double default_ms_per_step;   /* time per step of the builder's configuration */
     int64_t steps;                /* steps simulated by the trials */
@@ -416,7 +416,10 @@ typedef struct mgc_tune_report {
  * additions into a neuron's input: no result changes with one weight per
  * sign; with unequal weights of one sign the last bits of V may (as between
  * two runs of the reference's atomics).  The windowed step group
- * (mgc_set_persistent mode 3) is among the trials.  No reference counterpart
+ * (mgc_set_persistent mode 3) is among the trials, and so are its pull steps
+ * (mgc_set_pull) at thresholds of n/3, n/8 and n/20 arriving (spike, delay)
+ * pairs, on networks of at most 2^27 synapses with a minimum delay >= 2
+ * (their incoming rows are kept only when a threshold wins).  No reference counterpart
  * (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 

@@ -102,7 +102,7 @@ def mt19937_seed_words(seed):
 class TuneReport(C.Structure):
     _fields_ = [
         ("trials", C.c_int32), ("chunk_len", C.c_int32), ("blocks_per_sm", C.c_int32),
-        ("persistent", C.c_int32), ("window", C.c_int32), ("reserved", C.c_int32),
+        ("persistent", C.c_int32), ("window", C.c_int32), ("pull_min", C.c_int32),
         ("ms_per_step", C.c_double), ("default_ms_per_step", C.c_double), ("steps", C.c_int64),
     ]
 

@@ -880,6 +880,20 @@ mgc_status build_in_rows(mgc_sim* s)
     return MGC_OK;
 }
 
+void release_in_rows(mgc_sim* s)
+{
+    StepArgs& a = s->a;
+    if (a.pull || !a.in_ent) return;  // the pull method's rows are its synapses
+    cudaStreamSynchronize(s->stream);
+    for (void* p : {(void*)a.in_ptr, (void*)a.in_ent, (void*)a.hist_bits, (void*)a.bits_span}) s->release(p);
+    a.in_ptr = nullptr;
+    a.in_ent = nullptr;
+    a.hist_bits = nullptr;
+    a.bits_span = nullptr;
+    a.bits_words = 0;
+    a.pull_min = 0;
+}
+
 }  // namespace mgc
 
 extern "C" {

@@ -1016,6 +1016,8 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
 // before sa0: the prefixes of the n steps by the first n warps, then every
 // warp through the n steps' tasks without a barrier between them.  s, hslot:
 // a step and its history slot, for the slot arithmetic.
+constexpr int kPullUnroll = 8;  // incoming entries a lane loads at once in a pull step
+
 // fp32 addition with the rounding and subnormal flushing of red.add.f32
 __device__ __forceinline__ float fadd_ftz(float x, float y)
 {
@@ -1054,15 +1056,17 @@ __device__ __forceinline__ void pull_steps(const StepArgs& a, int64_t sa0, unsig
         int ce = 0, ci = 0;
         long long fe = 0, fi = 0;
         float we = 0.f, wi = 0.f;
-        for (int64_t q0 = rb; q0 < re; q0 += 32 * kDeliverUnroll) {
-            uint2 e[kDeliverUnroll];
+        for (int64_t q0 = rb; q0 < re; q0 += 32 * kPullUnroll) {
+            uint2 e[kPullUnroll];
 #pragma unroll
-            for (int u = 0; u < kDeliverUnroll; ++u) {
+            for (int u = 0; u < kPullUnroll; ++u) {
                 const int64_t q = q0 + u * 32 + lane;
-                e[u] = q < re ? __ldcs(a.in_ent + q) : make_uint2(0u, 0u);
+                // (cached normally: the rows stay in L2 for the next pulled
+                // step while the push's synapse words stream past evict-first)
+                e[u] = q < re ? __ldcg(a.in_ent + q) : make_uint2(0u, 0u);
             }
 #pragma unroll
-            for (int u = 0; u < kDeliverUnroll; ++u) {
+            for (int u = 0; u < kPullUnroll; ++u) {
                 if (q0 + u * 32 + lane >= re) continue;
                 const int32_t src = (int32_t)(e[u].x & a.tmask);
                 const int32_t d = (int32_t)(e[u].x >> a.tbits);

@@ -244,6 +244,8 @@ int32_t fx_shift_rule(double bound, int min_exp, bool exact);
 // The incoming rows and history bitmaps of the deferred method's pull steps,
 // built once (mgc_set_pull).
 mgc_status build_in_rows(mgc_sim* s);
+// Frees them again (pull steps off; the stream idle first).
+void release_in_rows(mgc_sim* s);
 // Segments of up to `gap` synapses cut into chunks of about `target`.
 void set_chunking(StepArgs& a, int64_t gap, int64_t target);
 

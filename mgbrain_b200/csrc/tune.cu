@@ -304,6 +304,42 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
         }
         if (st == MGC_OK) st = mgc_sync(s);
     }
+    // pull steps of the windowed group (mgc_set_pull) at thresholds of n/3,
+    // n/8 and n/20 arriving (spike, delay) pairs per step, on networks whose
+    // incoming rows are cheap to copy (a pull step reads all of them, so it
+    // pays only where that read costs less than a step's events: small dense
+    // networks in bursts)
+    int32_t best_pull = 0;
+    const bool pull_ok = s->fused && !s->partition && !(s->hetero && !s->a.fx) && s->S > 0 &&
+                         s->S <= (int64_t(1) << 27) && !sched_wanted(s);
+    const bool had_rows = s->a.in_ent != nullptr;
+    const int pull_window = rep->persistent == 3 ? best_window : std::min(kMaxWindow, s->dmin);
+    const int32_t ths[3] = {std::max(1, s->n / 3), std::max(1, s->n / 8), std::max(1, s->n / 20)};
+    for (int t = 0; t < 3 && st == MGC_OK && pull_ok; ++t) {
+        st = apply_cand(s, best_c, sms);
+        s->persistent = 3;
+        s->window = pull_window;
+        if (st == MGC_OK) st = mgc_set_pull(s, ths[t]);
+        if (st == MGC_OK) st = mgc_run(s, kGraphSteps);
+        if (st == MGC_OK) {
+            cudaEventRecord(e0, s->stream);
+            st = mgc_run(s, steps);
+            cudaEventRecord(e1, s->stream);
+        }
+        float ms = 0.f;
+        if (st == MGC_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) {
+            const double per = (double)ms / (double)steps;
+            rep->trials += 1;
+            if (per < best) {
+                best = per;
+                rep->persistent = 3;
+                best_window = pull_window;
+                best_pull = ths[t];
+            }
+        }
+        if (st == MGC_OK) st = mgc_sync(s);
+    }
+    if (pull_ok && st == MGC_OK) st = mgc_set_pull(s, 0);
     s->persistent = rep->persistent;
     s->window = best_window;
     rep->window = s->fused ? s->window : 0;
@@ -311,6 +347,11 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     cudaEventDestroy(e1);
     if (st != MGC_OK) return st;
     CKS(apply_cand(s, best_c, sms));
+    if (best_pull > 0)
+        CKS(mgc_set_pull(s, best_pull));
+    else if (pull_ok && !had_rows)
+        release_in_rows(s);  // the trials' incoming rows, not needed
+    rep->pull_min = best_pull;
     rep->ms_per_step = best;
     rep->chunk_len = s->a.deferred ? s->a.chunk_len : 0;
     rep->blocks_per_sm = best_c.blocks_per_sm;

@@ -159,3 +159,28 @@ def test_pull_steps_refused():
 def configs_c1():
     from cases import load
     return load("c1s")
+
+
+@pytest.mark.gpu
+def test_autotune_tries_pull_steps(burst):
+    """The autotuner times pull thresholds on this network (it is small
+    enough for a copy of its incoming rows); whatever it keeps, the end
+    state is the push's."""
+    sim = burst_net.simulator(burst, raster_ids=-1)
+    rep = sim.autotune(steps_per_trial=640)
+    assert rep["pull_min"] in (0, 11_000 // 3, 11_000 // 8, 11_000 // 20)
+    assert rep["persistent"] == 3 or rep["pull_min"] == 0
+    t = sim.info()["step"]
+    sim.run(500)
+    sim.sync()
+    got = sim.state()
+    sim.close()
+    ref = burst_net.simulator(burst, raster_ids=-1)
+    ref.set_persistent(3)
+    ref.set_window(8)
+    ref.run(t + 500)
+    ref.sync()
+    want = ref.state()
+    ref.close()
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
