@@ -1044,9 +1044,12 @@ def main():
                          "2 k_pipe groups, 3 k_window groups (window of min(8, minimum delay) steps)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner and run --group-mode (for launch lists)")
-    ap.add_argument("--kernel-profile", choices=["quiet", "driven"],
+    ap.add_argument("--kernel-profile", choices=["quiet", "driven", "burst"],
                     help="only build the network at --scale, run --warmup bench steps, 300 "
-                         "steps as timed, and 300 profiled steps (separate kernels); for ncu captures")
+                         "steps as timed, and 300 profiled steps (separate kernels); for ncu captures. "
+                         "burst: the bursting network with pull steps (--pull-min), 300 steps after the warm-up")
+    ap.add_argument("--pull-min", type=int, default=1500,
+                    help="with --kernel-profile burst: the pull-step threshold (arriving (spike, delay) pairs)")
     a = ap.parse_args()
     multi = int(os.environ.get("WORLD_SIZE", "1")) > 1
     split = a.impl == "ours" and (a.workload == "partition" or (a.workload == "brunel1m" and multi))
@@ -1062,6 +1065,17 @@ def main():
             run_sched(a, ws, rank, local)
         elif a.workload == "refgpu":
             run_refgpu(a, ws, rank, local)
+        elif a.kernel_profile == "burst":
+            # the bursting network with pull steps (the windowed group, 8 steps)
+            from mgbrain_b200 import brunel
+            sim = brunel.burst_simulator(brunel.burst_network(), device=local, raster_ids=-1)
+            sim.set_persistent(3)
+            sim.set_window(8)
+            sim.set_pull(a.pull_min)
+            sim.run(CHUNK * a.warmup)
+            sim.run(300)
+            sim.sync()
+            print(json.dumps({"kernel_profile": "burst", "pull_min": a.pull_min, "info": sim.info()}))
         elif a.kernel_profile:
             w = workload(a.scale, nu=NU_DRIVEN if a.kernel_profile == "driven" else NU_STEP)
             sim = make_sim(w, local, seed=1, record=False)
