@@ -163,6 +163,18 @@ __device__ __forceinline__ void red_add(float* p, float v)
 }
 __device__ __forceinline__ uint32_t as_u(float f) { return __float_as_uint(f); }
 
+// The same reduction with an L2 evict-last hint: the deferred method's
+// accumulators (a few MB per step buffer) keep their L2 lines while the
+// synapse words stream through L2 evict-first, so a reduction finds its line
+// in L2 instead of fetching the sector from DRAM.
+__device__ __forceinline__ void red_add_keep(float* p, float v)
+{
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_last.b64 pol, 1.0;\n\t"
+        "red.relaxed.gpu.global.add.L2::cache_hint.f32 [%0], %1, pol;\n\t}" ::"l"(p), "f"(v) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Fixed-point accumulation (FX), for networks in which some neuron receives
 // unequal weights of one sign.  fp32 additions of unequal values depend on
@@ -183,6 +195,13 @@ __device__ __forceinline__ float from_fx(long long x, float unscale) { return __
 __device__ __forceinline__ void red_add_fx(unsigned long long* p, long long v)
 {
     asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void red_add_fx_keep(unsigned long long* p, long long v)
+{
+    asm volatile(
+        "{\n\t.reg .b64 pol;\n\t"
+        "createpolicy.fractional.L2::evict_last.b64 pol, 1.0;\n\t"
+        "red.relaxed.gpu.global.add.L2::cache_hint.u64 [%0], %1, pol;\n\t}" ::"l"(p), "l"(v) : "memory");
 }
 
 // The accumulator entries of one step: fp32, or 64-bit fixed point.
@@ -710,10 +729,10 @@ __device__ __forceinline__ void deliver_tasks(const StepArgs& a, int64_t sa, int
                 const float wt = as_f(w[u].y);
                 const int64_t sx = sa + (NMAX > 1 ? st_of[u] : 0);
                 if (FX)
-                    red_add_fx(acc_buf<true, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask),
-                               to_fx(wt, a.fx_scale));
+                    red_add_fx_keep(acc_buf<true, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask),
+                                    to_fx(wt, a.fx_scale));
                 else
-                    red_add(acc_buf<false, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
+                    red_add_keep(acc_buf<false, MASK>(a, wt > 0.0f ? a.acc_e : a.acc_i, sx) + (w[u].x & a.tmask), wt);
             }
         }
     }
