@@ -44,8 +44,10 @@ enum {
                               each step, adding spiking sources in a fixed
                               order (deterministic for any weights) with STDP
                               fused in; cost grows with all synapses, so AUTO
-                              takes it only for plastic networks of <= 2^26
-                              synapses (explicit networks only) */
+                              never takes it (PUSH with STDP fused and
+                              fixed-point sums is deterministic too, and
+                              faster on the measured plastic networks);
+                              explicit networks only */
 };
 
 typedef struct mgc_sim mgc_sim;

@@ -58,7 +58,7 @@ def test_cuda_matches_oracle(name, mode):
         assert info["fx_shift"] == shift
     oc, oi, ost, osim = run_oracle(name, fx=info["fx_shift"] if fixed else None)
     if mode == "auto":
-        expect_mode = mgb.MODE_PULL if c["stdp"] else mgb.MODE_DEFERRED
+        expect_mode = mgb.MODE_PUSH if c["stdp"] else mgb.MODE_DEFERRED
     else:
         expect_mode = MODES[mode]
     assert gsim.info()["mode"] == expect_mode
