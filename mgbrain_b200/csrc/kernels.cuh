@@ -396,6 +396,21 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
     return fired;
 }
 
+// update_one's LIFB branch without branches (the same operations, selected):
+// the windowed group runs it for groups of four LIFB neurons, where the
+// per-neuron type and refractory branches would otherwise split the warp.
+// Returns whether the neuron fired; its fire count and last spike are the
+// caller's to record.
+__device__ __forceinline__ bool lifb_step(const StepArgs& a, float& v, int32_t& rf, float re, float ri)
+{
+    const bool ref = rf > 0;
+    const bool fire = !ref && v >= a.C[4];
+    const float nv = __fadd_rn(v, __fsub_rn(__fadd_rn(re, ri), __fmul_rn(a.lifb_leak, v)));
+    v = ref ? v : (fire ? a.C[3] : nv);
+    rf = ref ? rf - 1 : (fire ? a.refrac_steps : rf);
+    return fire;
+}
+
 // Updates the neuron groups with a warp-strided loop; `warp`/`nwarps` index
 // the warps taking part.  Each lane takes G groups per pass (groups
 // gb + h*32 + lane, h < G), all of whose loads are issued before the first
@@ -950,6 +965,7 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         }
         const int32_t i0 = (int32_t)(g << 2);
         const bool pois = t4.x == kPOISSON || t4.y == kPOISSON || t4.z == kPOISSON || t4.w == kPOISSON;
+        const bool lifb4 = t4.x == kLIFB && t4.y == kLIFB && t4.z == kLIFB && t4.w == kLIFB;
         // the window's steps four at a time: their input slots loaded at once
         // (one copy of the update in the code; the loop forms keep the
         // 3-blocks-per-SM instantiations within their 80 registers)
@@ -972,13 +988,21 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                 const int64_t s = w0 + h + k;
                 unsigned fm = 0;
                 if (have) {
-                    float u[4] = {0.f, 0.f, 0.f, 0.f};
-                    if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
                     const float4 e = e4[k].get(a), ii = i4[k].get(a);
-                    fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
-                    fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
-                    fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
-                    fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                    if (lifb4) {
+                        fm |= lifb_step(a, v4.x, r4.x, e.x, ii.x) ? 1u : 0u;
+                        fm |= lifb_step(a, v4.y, r4.y, e.y, ii.y) ? 2u : 0u;
+                        fm |= lifb_step(a, v4.z, r4.z, e.z, ii.z) ? 4u : 0u;
+                        fm |= lifb_step(a, v4.w, r4.w, e.w, ii.w) ? 8u : 0u;
+                        // (their fire counts and last spikes: with the compaction below)
+                    } else {
+                        float u[4] = {0.f, 0.f, 0.f, 0.f};
+                        if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
+                        fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
+                        fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
+                        fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
+                        fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                    }
                     // the step's input was used: its slot is cleared for step s + acc_mask + 1
                     In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
                     In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_i, s), g);
@@ -1014,6 +1038,10 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                     int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
                     for (int q = 0; q < 4; ++q)
                         if (fm & (1u << q)) {
+                            if (lifb4) {
+                                a.fire_cnt[i0 + q] += 1;
+                                a.last_fired[i0 + q] = (int32_t)s;
+                            }
                             if (!MGC_OK_INDEX(pos < a.n_src)) break;
                             ids[pos++] = a.src_base + i0 + q;
                         }
