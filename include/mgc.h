@@ -454,9 +454,12 @@ mgc_status mgc_set_persistent(mgc_sim* sim, int32_t mode);
  * spike counts the delivery already holds; results are those of the push
  * bit for bit (fixed-point sums exact; fp32 sums need one weight per sign,
  * else the call returns MGC_ERR_INVALID).  The first call builds the
- * incoming rows (8 bytes per synapse) and the bitmaps, which every step form
- * then writes; steps whose sources ran before it are pushed.  0 turns pull
- * steps off.  No reference counterpart (the reference always pushes,
+ * incoming rows (8 bytes per synapse) and the bitmaps; the windowed group
+ * writes a bitmap for every step it updates while pull steps are on, and a
+ * step is pulled only when every step its arrivals come from has one (steps
+ * run in another form, or before the call, or before a checkpoint load,
+ * have none: their arrivals are pushed).  0 turns pull steps off (the rows
+ * stay).  No reference counterpart (the reference always pushes,
  * mgcore.cu:271-305). */
 mgc_status mgc_set_pull(mgc_sim* sim, int32_t min_pairs);
 
