@@ -7,7 +7,8 @@ Workload (one bench step = 10,000 timesteps = 1 s simulated at dt = 0.1 ms):
   external per neuron (1.1e9 synapses, 8 B each on the device), J = 0.1 mV,
   g = 5, delays uniform in 10..50 steps.  Synthetic, seeded, generated on
   the device.  A driven variant (inputs at 200 Hz) is measured beside it
-  because the network as specified is quiescent apart from its inputs.
+  because the network as specified is quiescent apart from its inputs, and
+  a dense network firing in volleys (pull_variant) for the pull steps.
 
 Metric: synaptic events delivered per second of wall time (value), with
 simulated seconds per wall second and the HBM roofline of the dominant
