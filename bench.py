@@ -1045,10 +1045,11 @@ def main():
                          "2 k_pipe groups, 3 k_window groups (window of min(8, minimum delay) steps)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner and run --group-mode (for launch lists)")
-    ap.add_argument("--kernel-profile", choices=["quiet", "driven", "burst"],
+    ap.add_argument("--kernel-profile", choices=["quiet", "driven", "burst", "stdp"],
                     help="only build the network at --scale, run --warmup bench steps, 300 "
                          "steps as timed, and 300 profiled steps (separate kernels); for ncu captures. "
-                         "burst: the bursting network with pull steps (--pull-min), 300 steps after the warm-up")
+                         "burst: the bursting network with pull steps (--pull-min), 300 steps after the warm-up; "
+                         "stdp: config 3's STDP network (ring push with STDP), 710 steps")
     ap.add_argument("--pull-min", type=int, default=1500,
                     help="with --kernel-profile burst: the pull-step threshold (arriving (spike, delay) pairs)")
     a = ap.parse_args()
@@ -1066,6 +1067,20 @@ def main():
             run_sched(a, ws, rank, local)
         elif a.workload == "refgpu":
             run_refgpu(a, ws, rank, local)
+        elif a.kernel_profile == "stdp":
+            # config 3's STDP network at its stated size, the ring push with
+            # STDP fused (AUTO's method for plastic networks): one input epoch
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import stdp_net
+            import mgbrain_b200 as mgb
+            net = stdp_net.build(n_in=784, n_exc=1600)
+            sim = mgb.Simulator.from_arrays(net["n"], net["type"], net["src"], net["tar"], net["weight"],
+                                            net["delay"], net["lifconst"], net["stdpconst"], stdp=True,
+                                            plastic=net["plastic"], seed=11, device=local, raster_ids=-1)
+            sim.set_rates(stdp_net.rates(net, 0))
+            sim.run(stdp_net.REDRAW_STEPS + 10)
+            sim.sync()
+            print(json.dumps({"kernel_profile": "stdp", "info": sim.info()}))
         elif a.kernel_profile == "burst":
             # the bursting network with pull steps (the windowed group, 8 steps)
             from mgbrain_b200 import brunel
