@@ -398,7 +398,8 @@ mgc_status mgc_profile_steps(mgc_sim* sim, int64_t steps, float* ms);
 typedef struct mgc_tune_report {
     int32_t trials;               /* configurations timed */
     int32_t chunk_len;            /* chosen synapses per delivery task (deferred method) */
-    int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel */
+    int32_t blocks_per_sm;        /* chosen resident blocks per SM of the step's main kernel (0: the
+                                     ring or pull method's push on fewer blocks than SMs) */
     int32_t persistent;           /* chosen step-group mode of the fused method (mgc_set_persistent) */
     int32_t window;               /* chosen window of the windowed step group (mgc_set_window) */
     int32_t pull_min;             /* chosen pull-step threshold (mgc_set_pull), 0: none */

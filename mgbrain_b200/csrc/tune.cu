@@ -115,6 +115,7 @@ namespace {
 struct TuneCand {
     int64_t chunk_target;
     int blocks_per_sm;
+    int grid = 0;  // ring and pull methods: a grid of fewer blocks than SMs (0: blocks_per_sm per SM)
 };
 
 int& tuned_grid(mgc_sim* s)
@@ -137,7 +138,7 @@ mgc_status apply_cand(mgc_sim* s, const TuneCand& c, int sms)
         s->fused_grid = s->fused_grid_v[s->fused_variant];
         CKS(sched_put(s, &SchedState::static_variant, (int32_t)s->fused_variant));
     } else {
-        tuned_grid(s) = sms * c.blocks_per_sm;
+        tuned_grid(s) = c.grid > 0 ? c.grid : sms * c.blocks_per_sm;
     }
     return MGC_OK;
 }
@@ -226,6 +227,11 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
             if (s->a.deferred && t > kDefaultChunk && s->max_gap <= kDefaultChunk) continue;  // same chunking
             cands.push_back({t, b});
         }
+    // the ring and pull methods also at grids below one block per SM: a small
+    // network's step has few tasks, and every block of the push joins the
+    // step's epilogue counter
+    if (!s->a.deferred)
+        for (int g : {16, 37, 74}) cands.push_back({0, 1, g});
     const int64_t steps = (steps_per_trial + kGraphSteps - 1) / kGraphSteps * kGraphSteps;
     s->persistent = 0;  // the shapes are timed as graphs of single-step kernels, step groups after
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -354,7 +360,7 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     rep->pull_min = best_pull;
     rep->ms_per_step = best;
     rep->chunk_len = s->a.deferred ? s->a.chunk_len : 0;
-    rep->blocks_per_sm = best_c.blocks_per_sm;
+    rep->blocks_per_sm = best_c.grid > 0 ? 0 : best_c.blocks_per_sm;
     rep->steps = (int64_t)rep->trials * (steps + kGraphSteps);
     return MGC_OK;
 }

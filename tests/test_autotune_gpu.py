@@ -26,7 +26,8 @@ def test_autotune_keeps_results(n, delays, mode):
     rep = sim.autotune(steps_per_trial=64)
     assert rep["trials"] >= 1 and rep["ms_per_step"] > 0 and rep["default_ms_per_step"] > 0
     assert rep["ms_per_step"] <= rep["default_ms_per_step"]
-    assert rep["blocks_per_sm"] >= 1
+    # 0: the ring method's push on a grid of fewer blocks than SMs
+    assert rep["blocks_per_sm"] >= (0 if sim.info()["mode"] == mgb.MODE_PUSH else 1)
     sim.run(500)
     total = rep["steps"] + 500
     assert sim.info()["step"] == total
