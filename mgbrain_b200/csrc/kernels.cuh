@@ -452,21 +452,30 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
             }
         }
         unsigned fmask[G];
+        unsigned lifbm = 0;  // bit h: pass h's group is four LIFB neurons (branch-free update)
 #pragma unroll
         for (int h = 0; h < G; ++h) {
             const int64_t g = gb + h * 32 + lane;
             fmask[h] = 0;
             if (g < ngroups) {
                 const int32_t i0 = (int32_t)(g << 2);
-                // one Philox block serves the group's four POISSON draws
-                float u[4] = {0.f, 0.f, 0.f, 0.f};
-                if (t4[h].x == kPOISSON || t4[h].y == kPOISSON || t4[h].z == kPOISSON || t4[h].w == kPOISSON)
-                    poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
                 const float4 e = e4[h].get(a), ii = i4[h].get(a);
-                fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e.x, ii.x, ce4[h].x, ci4[h].x, u[0]) ? 1u : 0u;
-                fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e.y, ii.y, ce4[h].y, ci4[h].y, u[1]) ? 2u : 0u;
-                fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e.z, ii.z, ce4[h].z, ci4[h].z, u[2]) ? 4u : 0u;
-                fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e.w, ii.w, ce4[h].w, ci4[h].w, u[3]) ? 8u : 0u;
+                if (t4[h].x == kLIFB && t4[h].y == kLIFB && t4[h].z == kLIFB && t4[h].w == kLIFB) {
+                    lifbm |= 1u << h;
+                    fmask[h] |= lifb_step(a, v4[h].x, r4[h].x, e.x, ii.x) ? 1u : 0u;
+                    fmask[h] |= lifb_step(a, v4[h].y, r4[h].y, e.y, ii.y) ? 2u : 0u;
+                    fmask[h] |= lifb_step(a, v4[h].z, r4[h].z, e.z, ii.z) ? 4u : 0u;
+                    fmask[h] |= lifb_step(a, v4[h].w, r4[h].w, e.w, ii.w) ? 8u : 0u;
+                } else {
+                    // one Philox block serves the group's four POISSON draws
+                    float u[4] = {0.f, 0.f, 0.f, 0.f};
+                    if (t4[h].x == kPOISSON || t4[h].y == kPOISSON || t4[h].z == kPOISSON || t4[h].w == kPOISSON)
+                        poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
+                    fmask[h] |= update_one(a, t4[h].x, i0 + 0, s, v4[h].x, r4[h].x, e.x, ii.x, ce4[h].x, ci4[h].x, u[0]) ? 1u : 0u;
+                    fmask[h] |= update_one(a, t4[h].y, i0 + 1, s, v4[h].y, r4[h].y, e.y, ii.y, ce4[h].y, ci4[h].y, u[1]) ? 2u : 0u;
+                    fmask[h] |= update_one(a, t4[h].z, i0 + 2, s, v4[h].z, r4[h].z, e.z, ii.z, ce4[h].z, ci4[h].z, u[2]) ? 4u : 0u;
+                    fmask[h] |= update_one(a, t4[h].w, i0 + 3, s, v4[h].w, r4[h].w, e.w, ii.w, ce4[h].w, ci4[h].w, u[3]) ? 8u : 0u;
+                }
                 // the input is cleared only after it was used: a store issued
                 // while the load of the same line is in flight stalls the
                 // memory pipeline (measured 4-6x slower once the state
@@ -519,6 +528,10 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 const int32_t i0 = (int32_t)((gb + h * 32 + lane) << 2);
                 for (int k = 0; k < 4; ++k) {
                     if (fmask[h] & (1u << k)) {
+                        if ((lifbm >> h) & 1u) {  // (update_one records the others' itself)
+                            a.fire_cnt[i0 + k] += 1;
+                            a.last_fired[i0 + k] = (int32_t)s;
+                        }
                         if (!MGC_OK_INDEX(pos < (a.deferred ? a.n_src : a.n))) break;
                         ids[pos] = a.src_base + i0 + k;
                         if (pop_cnt) atomicAdd(pop_cnt + a.tpop[i0 + k], 1);
