@@ -69,6 +69,10 @@ public:
     // (mgc_create_generated): the same network, without the host synapse
     // list (Network::recipe)
     static bool DEVICE_NETGEN;
+    // addition: steps per trial of the autotuner that MGSimulator runs, with
+    // the trials undone (mgc_autotune_rewind), before the first step of a
+    // network on one handle; 0: off
+    static long long AUTOTUNE_STEPS;
 
     static void set_timestep(real time_step)
     {
@@ -94,6 +98,7 @@ public:
     static void set_seed(long long seed) { SEED = seed; }
     static void set_netgen_seed(long long seed) { NETGEN_SEED = seed; }
     static void set_device(int device) { DEVICE = device; }
+    static void enable_autotune(long long steps_per_trial = 640) { AUTOTUNE_STEPS = steps_per_trial; }
     static void set_netgen_threads(int threads, long long min_pairs = 1LL << 24)
     {
         NETGEN_THREADS = threads;

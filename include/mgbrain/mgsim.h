@@ -31,9 +31,8 @@
 #include <stdexcept>
 #include <vector>
 
+#include "../mgc.h"
 #include "network.h"
-
-struct mgc_sim;
 
 namespace MGBrain {
 
@@ -66,6 +65,7 @@ class MGSimulator {
     std::vector<long long> raster_counts;
     std::vector<int> raster_ids;
     bool raster_complete = true;
+    bool tuned = false;
     void check(int status, const char* what);
     void build_generated(Network& net);
     void drain_raster();
@@ -96,6 +96,10 @@ public:
     long long get_events();
     int get_min_delay() const { return min_delay; }
     int get_ring_len() const { return max_delay + 1; }
+    // Times the launch configurations and keeps the fastest, with the trial
+    // steps undone (mgc_autotune_rewind); one handle only.  Simulate() calls
+    // it before the first step when Config::AUTOTUNE_STEPS > 0.
+    mgc_tune_report autotune(long long steps_per_trial = 640);
     // The C ABI handle (of the first partition when they run separately).
     mgc_sim* handle() { return sim; }
     // Handles the network runs on: 1, or one per partition.

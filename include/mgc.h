@@ -426,6 +426,16 @@ typedef struct mgc_tune_report {
  * (its launch shapes are fixed, mgcore.cu:535-554). */
 mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
 
+/* mgc_autotune without advancing the simulation: saves a checkpoint of the
+ * state, runs the trials and loads the checkpoint back (also after a failed
+ * trial), so that the handle keeps the chosen launch configuration and
+ * continues from the step it was at, as a handle that ran no trial would
+ * (the raster restarts empty there; refused while it holds steps not yet
+ * read).  report->steps counts the trials' steps, which are undone.  Host
+ * memory of mgc_checkpoint_size bytes is held during the call.  No reference
+ * counterpart. */
+mgc_status mgc_autotune_rewind(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);
+
 /* How the fused method runs: 0 CUDA graphs of single-step kernels; 1
  * cooperative step groups of up to
  * 1024 steps with a grid barrier between steps; 2 pipelined step groups

@@ -31,7 +31,7 @@ EXPORTED = (
     "mgc_read_raster", "mgc_read_state", "mgc_read_weights", "mgc_export_csr", "mgc_get_info",
     "mgc_get_stream", "mgc_effective_steps", "mgc_destroy", "mgc_last_error",
     "mgc_kernel_launches", "mgc_profile_steps", "mgc_create_batch", "mgc_row_offsets_static",
-    "mgc_measure_scatter", "mgc_autotune", "mgc_set_persistent", "mgc_set_window", "mgc_set_pull", "mgc_checkpoint_size",
+    "mgc_measure_scatter", "mgc_autotune", "mgc_autotune_rewind", "mgc_set_persistent", "mgc_set_window", "mgc_set_pull", "mgc_checkpoint_size",
     "mgc_checkpoint_save", "mgc_checkpoint_load", "mgc_sched_set_mode", "mgc_sched_set_threshold",
     "mgc_sched_calibrate", "mgc_sched_collect", "mgc_sched_train", "mgc_sched_report", "mgc_mlp_gradient",
     "mgc_create_partition", "mgc_create_fixed_indegree_partition", "mgc_part_export", "mgc_part_import",
@@ -186,6 +186,8 @@ def lib():
     L.mgc_measure_scatter.restype = C.c_int
     L.mgc_autotune.argtypes = [vp, i64, C.POINTER(TuneReport)]
     L.mgc_autotune.restype = C.c_int
+    L.mgc_autotune_rewind.argtypes = [vp, i64, C.POINTER(TuneReport)]
+    L.mgc_autotune_rewind.restype = C.c_int
     L.mgc_set_persistent.argtypes = [vp, i32]
     L.mgc_set_persistent.restype = C.c_int
     L.mgc_set_pull.argtypes = [vp, i32]
@@ -551,11 +553,15 @@ class Simulator:
         ptr = C.c_void_p(bufs.data_ptr()) if bufs is not None else None
         check(lib().mgc_part_import_dev(self._h, int(count), int(nranks), int(self_rank), ptr, int(cap)))
 
-    def autotune(self, steps_per_trial=640):
+    def autotune(self, steps_per_trial=640, rewind=False):
         """Times the launch configurations and keeps the fastest; the trial
-        steps advance the simulation (report["steps"] of them)."""
+        steps advance the simulation (report["steps"] of them), or with
+        rewind=True are undone through a checkpoint, so that the simulation
+        continues from where it was (mgc_autotune_rewind; read the raster
+        first)."""
         r = TuneReport()
-        check(lib().mgc_autotune(self._h, int(steps_per_trial), C.byref(r)))
+        fn = lib().mgc_autotune_rewind if rewind else lib().mgc_autotune
+        check(fn(self._h, int(steps_per_trial), C.byref(r)))
         return {k: getattr(r, k) for k, _ in TuneReport._fields_ if k != "reserved"}
 
     # ---- step scheduler ---------------------------------------------------

@@ -353,12 +353,23 @@ void MGSimulator::drain_raster()
     }
 }
 
+mgc_tune_report MGSimulator::autotune(long long steps_per_trial)
+{
+    mgc_tune_report rep{};
+    if (pieces.size() != 1) check(MGC_ERR_INVALID, "autotune: the network runs on one handle per partition");
+    drain_raster();
+    check(mgc_autotune_rewind(sim, steps_per_trial, &rep), "mgc_autotune_rewind");
+    tuned = true;
+    return rep;
+}
+
 void MGSimulator::simulate(real time)
 {
     // mgsim.cpp:801-802: round(time/STEP) steps; when that is not a multiple
     // of the minimum delay the last partial cycle is not run.
     const long long steps = static_cast<int>(std::round(time / Config::STEP));
     const long long eff = mgc_effective_steps(steps, min_delay);
+    if (Config::AUTOTUNE_STEPS > 0 && !tuned && pieces.size() == 1) autotune(Config::AUTOTUNE_STEPS);
     timer t;
     if (pieces.size() == 1) {
         for (long long left = eff; left > 0;) {

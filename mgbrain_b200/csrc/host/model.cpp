@@ -39,6 +39,7 @@ bool Config::STDP_BY_TYPE = false;
 int Config::NETGEN_THREADS = 0;
 long long Config::NETGEN_PARALLEL_PAIRS = 1LL << 24;
 bool Config::DEVICE_NETGEN = false;
+long long Config::AUTOTUNE_STEPS = 0;
 
 Model::Model() { indexer = 0; }
 

@@ -365,4 +365,29 @@ mgc_status mgc_autotune(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* re
     return MGC_OK;
 }
 
+mgc_status mgc_autotune_rewind(mgc_sim* s, int64_t steps_per_trial, mgc_tune_report* rep)
+{
+    if (!s || !rep || steps_per_trial < 1) return fail(MGC_ERR_INVALID, "bad autotune arguments");
+    if (s->partition) return fail(MGC_ERR_INVALID, "partition handles run steps only between exchanges (mgc_run)");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    // the raster restarts at the restored step, so it must hold nothing unread
+    int64_t clock[3] = {0, 0, 0};
+    CK(cudaMemcpy(&clock[0], s->a.step, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&clock[1], s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&clock[2], s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
+    if (clock[0] != clock[1] || clock[2] != 0)
+        return fail(MGC_ERR_INVALID, "autotune with rewind: read the raster first (%lld steps unread)",
+                    (long long)(clock[0] - clock[1]));
+    int64_t bytes = 0;
+    CKS(mgc_checkpoint_size(s, &bytes));
+    std::vector<char> saved((size_t)bytes);
+    CKS(mgc_checkpoint_save(s, saved.data(), bytes));
+    const mgc_status st = mgc_autotune(s, steps_per_trial, rep);
+    // the state goes back even when a trial failed, so that the handle
+    // continues from where the call found it
+    const mgc_status back = mgc_checkpoint_load(s, saved.data(), bytes);
+    return st != MGC_OK ? st : back;
+}
+
 }  // extern "C"

@@ -8,6 +8,8 @@
 //   (npart > 1: SIMPLE partitions; "single" calls config::enable_single_gpu())
 //   env MGB_DEVICE_NETGEN=1: config::enable_device_netgen() (the network is
 //   generated on the device when the simulator is built)
+//   env MGB_AUTOTUNE=k: config::enable_autotune(k) (trials of k steps before
+//   the first step, undone)
 // simulate writes <out_prefix>.state (V, fire_cnt, weights) and .raster.
 #include <cstdio>
 #include <cstdlib>
@@ -66,6 +68,7 @@ int main(int argc, char** argv)
         if (atoi(argv[6])) config::enable_stdp();
         config::set_seed(env("MGB_SEED", 1));
         config::enable_fire_check();
+        if (env("MGB_AUTOTUNE", 0) > 0) config::enable_autotune(env("MGB_AUTOTUNE", 0));
         const int npart = argc == 9 ? atoi(argv[7]) : 1;
         if (argc == 9 && std::string(argv[8]) == "single") config::enable_single_gpu();
         std::vector<int> part = parter::part_network(net, npart, npart > 1 ? PartType::SIMPLE : PartType::MODEL);

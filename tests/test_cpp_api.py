@@ -43,17 +43,19 @@ def test_cpp_netgen_matches_reference(driver, tmp_path, name):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("autotune", [0, 64])
 @pytest.mark.parametrize("name", [n for n in NAMES if CASES[n].get("simulate")])
-def test_cpp_simulate_matches_oracle_and_reference(driver, tmp_path, name):
+def test_cpp_simulate_matches_oracle_and_reference(driver, tmp_path, name, autotune):
     """simulate(t) runs the reference's effective step count (the remainder
     after the last whole min_delay cycle is dropped) and ends in the state
-    the oracle reaches after that many steps."""
+    the oracle reaches after that many steps; with Config::enable_autotune
+    the tuner's trial steps before the first step are undone."""
     c, net, v0 = load(name)
     pre = str(tmp_path / "s")
     v0p = os.path.join(T.GOLDEN, name + ".v0")
     r = subprocess.run([driver, "simulate", os.path.join(T.GOLDEN, name + ".spec"), pre,
                         str(c["simulate"]), v0p if os.path.exists(v0p) else "-", str(c["stdp"])],
-                       check=True, env=_env(c), capture_output=True, text=True)
+                       check=True, env=dict(_env(c), MGB_AUTOTUNE=str(autotune)), capture_output=True, text=True)
     assert "fire rate:" in r.stdout
     o = T.OracleSim(net, c["seed"], v0=v0, stdp=c["stdp"])
     steps = T.oracle().mgbo_steps_for_time(np.float32(c["simulate"]), np.float32(net["step"]))
