@@ -610,7 +610,9 @@ mgc_status mgc_measure_scatter(int32_t device, int64_t n_events, int32_t n_targe
  * initial contents (the call zeroes it and its own counters).  The first call
  * on a device does a one-time set-up (it looks up the scratch array's address,
  * cudaGetSymbolAddress), so make that first call before any stream capture
- * begins.  All calls on one device share the one scratch array, which keeps
+ * begins.  Because every call waits for its stream, no call can be captured
+ * into a CUDA graph: do not make one on a capturing stream, nor on the legacy
+ * stream (NULL) while another thread runs a global-mode capture.  All calls on one device share the one scratch array, which keeps
  * the last call's contents, so calls that overlapped on the GPU would race on
  * it; the library serialises them with a lock per device, held until the
  * call's work on the stream has finished, on success and on failure alike.

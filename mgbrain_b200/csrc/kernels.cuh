@@ -830,20 +830,21 @@ __global__ void __launch_bounds__(kPushBlock, MINB) k_fused(StepArgs a)
 // ---------------------------------------------------------------------------
 constexpr unsigned int kBarrierSpins = 1u << 21;
 
+// Arrivals count up on a.bar[0], which is cleared before every launch: a
+// block's arrival returns the count before it, from which it knows the
+// total that completes this barrier (the next multiple of gridDim.x), so the
+// last block to arrive releases the others by its arrival alone.
 __device__ __forceinline__ bool grid_barrier(const StepArgs& a, int* abort_flag)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int* gen = a.bar + 1;
-        const unsigned int g0 = *gen;
         __threadfence();
-        if (atomicAdd(a.bar, 1u) == gridDim.x - 1) {
-            atomicExch(a.bar, 0u);
-            __threadfence();
-            atomicAdd(a.bar + 1, 1u);  // release the others
-        } else {
+        const unsigned int before = atomicAdd(a.bar, 1u);
+        const unsigned int target = (before / gridDim.x + 1u) * gridDim.x;
+        if (before + 1u != target) {
+            volatile unsigned int* arrived = a.bar;
             unsigned int it = 0;
-            while (*gen == g0) {
+            while (*arrived < target) {
                 if (++it > kBarrierSpins) {
                     atomicOr(a.status, kStatusBarrier);
                     *abort_flag = 1;
