@@ -321,6 +321,7 @@ __device__ __forceinline__ void step_epilogue(const StepArgs& a)
 // with the group when the network has such neurons and are stored back with it.
 // u: the neuron's POISSON draw of this step (poisson_uniform), computed for
 // its group of four.
+template <bool BOOK = true>
 __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, int64_t s, float& v, int32_t& rf,
                                            float re, float ri, float& ie_io, float& ii_io, float u)
 {
@@ -389,8 +390,8 @@ __device__ __forceinline__ bool update_one(const StepArgs& a, int t, int32_t i, 
         }
     }
     // RAW and LIF0 have no branch in the reference: never update, never fire.
-    if (fired) {
-        a.fire_cnt[i] += 1;
+    if (BOOK && fired) {
+        atomicAdd(a.fire_cnt + i, 1);  // a reduction: the update does not wait on the count
         a.last_fired[i] = (int32_t)s;
     }
     return fired;
@@ -529,7 +530,7 @@ __device__ __forceinline__ void neuron_groups(const StepArgs& a, int64_t s, int3
                 for (int k = 0; k < 4; ++k) {
                     if (fmask[h] & (1u << k)) {
                         if ((lifbm >> h) & 1u) {  // (update_one records the others' itself)
-                            a.fire_cnt[i0 + k] += 1;
+                            atomicAdd(a.fire_cnt + i0 + k, 1);
                             a.last_fired[i0 + k] = (int32_t)s;
                         }
                         if (!MGC_OK_INDEX(pos < (a.deferred ? a.n_src : a.n))) break;
@@ -980,6 +981,7 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         const int32_t i0 = (int32_t)(g << 2);
         const bool pois = t4.x == kPOISSON || t4.y == kPOISSON || t4.z == kPOISSON || t4.w == kPOISSON;
         const bool lifb4 = t4.x == kLIFB && t4.y == kLIFB && t4.z == kLIFB && t4.w == kLIFB;
+        unsigned fms = 0;  // the pass's spikes: bits 4j..4j+3 for step w0 + j
         // the window's steps four at a time: their input slots loaded at once
         // (one copy of the update in the code; the loop forms keep the
         // 3-blocks-per-SM instantiations within their 80 registers)
@@ -1008,14 +1010,14 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                         fm |= lifb_step(a, v4.y, r4.y, e.y, ii.y) ? 2u : 0u;
                         fm |= lifb_step(a, v4.z, r4.z, e.z, ii.z) ? 4u : 0u;
                         fm |= lifb_step(a, v4.w, r4.w, e.w, ii.w) ? 8u : 0u;
-                        // (their fire counts and last spikes: with the compaction below)
+                        // (fire counts and last spikes of every group: after the pass)
                     } else {
                         float u[4] = {0.f, 0.f, 0.f, 0.f};
                         if (pois) poisson_uniform4(a.seed, (int64_t)i0 + a.id_offset, s, u);
-                        fm |= update_one(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
-                        fm |= update_one(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
-                        fm |= update_one(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
-                        fm |= update_one(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
+                        fm |= update_one<false>(a, t4.x, i0 + 0, s, v4.x, r4.x, e.x, ii.x, ce4.x, ci4.x, u[0]) ? 1u : 0u;
+                        fm |= update_one<false>(a, t4.y, i0 + 1, s, v4.y, r4.y, e.y, ii.y, ce4.y, ci4.y, u[1]) ? 2u : 0u;
+                        fm |= update_one<false>(a, t4.z, i0 + 2, s, v4.z, r4.z, e.z, ii.z, ce4.z, ci4.z, u[2]) ? 4u : 0u;
+                        fm |= update_one<false>(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
                     }
                     // the step's input was used: its slot is cleared for step s + acc_mask + 1
                     In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
@@ -1031,34 +1033,61 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                     if ((lane & 7) == 0 && gb < ngroups)
                         a.hist_bits[(size_t)hb * (size_t)a.bits_words + (gb >> 3) + (lane >> 3)] = wv;
                 }
-                // the step's spikes into its history slot, in neuron order within
-                // the warp (no scan when no lane spiked)
-                if (!__any_sync(0xffffffffu, fm != 0)) continue;
-                const int c = __popc(fm);
-                int incl = c;
+                fms |= fm << (4 * (h + k));
+            }
+        }
+        // the pass's spikes into their steps' history slots, in neuron order
+        // within the warp: one scan for all steps (a warp's count of a step is
+        // at most 128, so four steps share a word, a byte each), the steps'
+        // positions reserved by lanes 0..wl-1 at once
+        if (__any_sync(0xffffffffu, fms != 0)) {
+            uint32_t ca = 0, cb = 0;
 #pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += v;
+            for (int j = 0; j < 4; ++j) {
+                ca |= (uint32_t)__popc((fms >> (4 * j)) & 15u) << (8 * j);
+                cb |= (uint32_t)__popc((fms >> (4 * j + 16)) & 15u) << (8 * j);
+            }
+            uint32_t ia = ca, ib = cb;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t va = __shfl_up_sync(0xffffffffu, ia, o), vb = __shfl_up_sync(0xffffffffu, ib, o);
+                if (lane >= o) {
+                    ia += va;
+                    ib += vb;
                 }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                if (total) {
-                    int32_t hs = hs0 + h + k;
+            }
+            const uint32_t ta = __shfl_sync(0xffffffffu, ia, 31), tb = __shfl_sync(0xffffffffu, ib, 31);
+            ia -= ca;  // exclusive
+            ib -= cb;
+            int32_t base = 0;
+            if (lane < wl) {
+                const int32_t tot = (int32_t)(((lane < 4 ? ta : tb) >> (8 * (lane & 3))) & 255u);
+                if (tot) {
+                    int32_t hs = hs0 + lane;
                     if (hs >= a.H) hs -= a.H;
-                    int32_t base = 0;
-                    if (lane == 31) base = atomicAdd(a.hist_cnt + hs, total);
-                    base = __shfl_sync(0xffffffffu, base, 31);
-                    int32_t pos = base + incl - c;
-                    int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
-                    for (int q = 0; q < 4; ++q)
-                        if (fm & (1u << q)) {
-                            if (lifb4) {
-                                a.fire_cnt[i0 + q] += 1;
-                                a.last_fired[i0 + q] = (int32_t)s;
-                            }
-                            if (!MGC_OK_INDEX(pos < a.n_src)) break;
-                            ids[pos++] = a.src_base + i0 + q;
-                        }
+                    base = atomicAdd(a.hist_cnt + hs, tot);
+                }
+            }
+            for (int j = 0; j < wl; ++j) {
+                const int32_t bj = __shfl_sync(0xffffffffu, base, j);
+                const unsigned f = (fms >> (4 * j)) & 15u;
+                if (!f) continue;
+                int32_t pos = bj + (int32_t)(((j < 4 ? ia : ib) >> (8 * (j & 3))) & 255u);
+                int32_t hs = hs0 + j;
+                if (hs >= a.H) hs -= a.H;
+                int32_t* ids = a.hist_ids + (size_t)hs * (size_t)a.n_src;
+                for (int q = 0; q < 4; ++q)
+                    if (f & (1u << q)) {
+                        if (!MGC_OK_INDEX(pos < a.n_src)) break;
+                        ids[pos++] = a.src_base + i0 + q;
+                    }
+            }
+            // each neuron's spikes of the pass: its count added once, its last step stored once
+            for (int q = 0; q < 4; ++q) {
+                const unsigned fq = fms & (0x11111111u << q);
+                if (fq) {
+                    atomicAdd(a.fire_cnt + i0 + q, __popc(fq));
+                    a.last_fired[i0 + q] = (int32_t)(w0 + ((31 - __clz(fq)) >> 2));
                 }
             }
         }
