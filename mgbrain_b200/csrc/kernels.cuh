@@ -981,6 +981,9 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
         const int32_t i0 = (int32_t)(g << 2);
         const bool pois = t4.x == kPOISSON || t4.y == kPOISSON || t4.z == kPOISSON || t4.w == kPOISSON;
         const bool lifb4 = t4.x == kLIFB && t4.y == kLIFB && t4.z == kLIFB && t4.w == kLIFB;
+        // four POISSON neurons ignore their input and keep their state (V holds
+        // the probability): no input slot is cleared, no state stored
+        const bool pois4 = t4.x == kPOISSON && t4.y == kPOISSON && t4.z == kPOISSON && t4.w == kPOISSON;
         unsigned fms = 0;  // the pass's spikes: bits 4j..4j+3 for step w0 + j
         // the window's steps four at a time: their input slots loaded at once
         // (one copy of the update in the code; the loop forms keep the
@@ -993,7 +996,7 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
             for (int k = 0; k < kWinLoad; ++k) {
                 e4[k].zero();
                 i4[k].zero();
-                if (have && h + k < wl) {
+                if (have && !pois4 && h + k < wl) {
                     e4[k].load(acc_buf<FX, WMAX - 1>(a, a.acc_e, w0 + h + k), g);
                     i4[k].load(acc_buf<FX, WMAX - 1>(a, a.acc_i, w0 + h + k), g);
                 }
@@ -1020,8 +1023,10 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                         fm |= update_one<false>(a, t4.w, i0 + 3, s, v4.w, r4.w, e.w, ii.w, ce4.w, ci4.w, u[3]) ? 8u : 0u;
                     }
                     // the step's input was used: its slot is cleared for step s + acc_mask + 1
-                    In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
-                    In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_i, s), g);
+                    if (!pois4) {
+                        In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_e, s), g);
+                        In4<FX>::clear(acc_buf<FX, WMAX - 1>(a, a.acc_i, s), g);
+                    }
                 }
                 if (PULL) {  // the step's spikes as a bitmap (pull steps read it)
                     int32_t hb = hs0 + h + k;
@@ -1091,7 +1096,7 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
                 }
             }
         }
-        if (have) {
+        if (have && !pois4) {
             reinterpret_cast<float4*>(a.V)[g] = v4;
             reinterpret_cast<int4*>(a.refrac)[g] = r4;
             if (CUR) {
