@@ -430,8 +430,8 @@ mgc_status mgc_autotune(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* 
  * state, runs the trials and loads the checkpoint back (also after a failed
  * trial), so that the handle keeps the chosen launch configuration and
  * continues from the step it was at, as a handle that ran no trial would
- * (the raster restarts empty there; refused while it holds steps not yet
- * read).  report->steps counts the trials' steps, which are undone.  Host
+ * (the raster restarts empty there; on a handle that records a raster,
+ * refused while it holds steps not yet read).  report->steps counts the trials' steps, which are undone.  Host
  * memory of mgc_checkpoint_size bytes is held during the call.  No reference
  * counterpart. */
 mgc_status mgc_autotune_rewind(mgc_sim* sim, int64_t steps_per_trial, mgc_tune_report* report);

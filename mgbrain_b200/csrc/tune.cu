@@ -371,11 +371,14 @@ mgc_status mgc_autotune_rewind(mgc_sim* s, int64_t steps_per_trial, mgc_tune_rep
     if (s->partition) return fail(MGC_ERR_INVALID, "partition handles run steps only between exchanges (mgc_run)");
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->stream));
-    // the raster restarts at the restored step, so it must hold nothing unread
+    // the raster restarts at the restored step, so a recording handle's
+    // raster must hold nothing unread
     int64_t clock[3] = {0, 0, 0};
-    CK(cudaMemcpy(&clock[0], s->a.step, 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&clock[1], s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&clock[2], s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
+    if (s->a.record) {
+        CK(cudaMemcpy(&clock[0], s->a.step, 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&clock[1], s->a.raster_step0, 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&clock[2], s->a.raster_pos, 8, cudaMemcpyDeviceToHost));
+    }
     if (clock[0] != clock[1] || clock[2] != 0)
         return fail(MGC_ERR_INVALID, "autotune with rewind: read the raster first (%lld steps unread)",
                     (long long)(clock[0] - clock[1]));

@@ -184,3 +184,28 @@ def test_autotune_tries_pull_steps(burst):
     ref.close()
     for k in want:
         assert np.array_equal(got[k], want[k]), k
+
+
+@pytest.mark.gpu
+def test_autotune_rewind_keeps_the_push_state(burst):
+    """The autotuner with its trials undone on the bursting network (whose
+    pull trials build incoming rows and spike bitmaps): the step clock and
+    the end state are those of a run that never tuned (a handle that
+    records no raster)."""
+    sim = burst_net.simulator(burst, raster_ids=-1)
+    sim.run(200)
+    rep = sim.autotune(steps_per_trial=640, rewind=True)
+    assert rep["trials"] >= 1 and sim.info()["step"] == 200
+    sim.run(500)
+    sim.sync()
+    got = sim.state()
+    sim.close()
+    ref = burst_net.simulator(burst, raster_ids=-1)
+    ref.set_persistent(3)
+    ref.set_window(8)
+    ref.run(700)
+    ref.sync()
+    want = ref.state()
+    ref.close()
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
