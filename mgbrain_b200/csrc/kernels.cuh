@@ -138,6 +138,8 @@ struct StepArgs {
                               //   pairs is delivered by pull (0: never)
     int64_t* bits_span;       // [2] the steps [from, end) whose bitmaps the group wrote, one run
                               //   of groups without other step forms between them
+    int64_t upd_rot;          // windowed update without pull steps: the lane at position p of a
+                              //   pass updates neuron group (p + upd_rot) mod groups
 };
 
 __device__ __forceinline__ float as_f(uint32_t u) { return __uint_as_float(u); }
@@ -964,8 +966,9 @@ __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int
     const int lane = threadIdx.x & 31;
     const int64_t ngroups = a.ns >> 2;
     for (int64_t gb = warp * 32; gb < ngroups; gb += nwarps * 32) {
-        const int64_t g = gb + lane;
-        const bool have = g < ngroups;
+        const bool have = gb + lane < ngroups;
+        int64_t g = gb + lane + (PULL ? 0 : a.upd_rot);  // the bitmaps' words follow the positions
+        if (g >= ngroups) g -= ngroups;
         char4 t4 = make_char4(0, 0, 0, 0);
         float4 v4 = make_float4(0.f, 0.f, 0.f, 0.f), ce4 = v4, ci4 = v4;
         int4 r4 = make_int4(0, 0, 0, 0);

@@ -42,6 +42,28 @@ __global__ void k_acc_move(float* acc_e, float* acc_i, const int64_t* step, int3
     }
 }
 
+// The windowed update's rotation of neuron groups over lane positions
+// (StepArgs::upd_rot) for a grid of `grid` blocks: the lanes whose last pass
+// is the pass before the others' extra one take the POISSON groups, whose
+// draws make theirs the costliest passes, when those neurons form one range
+// of the network and fit there; else 0.  A multiple of 32, so that a warp's
+// groups stay consecutive.
+int64_t update_rotation(const mgc_sim* s, int grid)
+{
+    const int64_t groups = s->a.ns >> 2;
+    const int64_t lanes = (int64_t)grid * kPushBlock;
+    if (s->pois_idx.empty() || groups < 1 || lanes < 1) return 0;
+    const int64_t first = s->pois_idx.front(), last = s->pois_idx.back();
+    if (last - first + 1 != (int64_t)s->pois_idx.size() || first % 4 != 0) return 0;
+    const int64_t ga = first / 4, gb = (last + 4) / 4;  // the POISSON groups [ga, gb)
+    const int64_t passes = groups / lanes, extra = groups % lanes;
+    if (passes < 1 || extra == 0) return 0;  // every lane runs as many passes
+    const int64_t t0 = (passes - 1) * lanes + extra;  // lanes without the extra pass, in their last one
+    const int64_t rot0 = ga - t0;
+    const int64_t rot = rot0 - (((rot0 % 32) + 32) % 32);
+    if ((gb - ga) + 31 > passes * lanes - t0) return 0;
+    return ((rot % groups) + groups) % groups;
+}
 
 }  // namespace
 
@@ -281,6 +303,7 @@ mgc_status mgc_run(mgc_sim* s, int64_t steps)
                 const int wide = w > kAccBuffers;
                 if (s->a.acc_mask != (wide ? kAccBuffersWide : kAccBuffers) - 1)
                     return fail(MGC_ERR_INVALID, "a window of %d steps in the %d-buffer cycle", w, s->a.acc_mask + 1);
+                ga.upd_rot = s->a.pull_min > 0 ? 0 : update_rotation(s, s->window_grid_v[wide][v]);
                 void* wargs[] = {&ga, &n, &w};
                 e = cudaLaunchCooperativeKernel((const void*)window_kernel(s, v, wide, s->a.pull_min > 0),
                                                 dim3(s->window_grid_v[wide][v]), dim3(kPushBlock), wargs,
