@@ -958,7 +958,10 @@ constexpr int kWinLoad = 4;  // input slots a lane holds at once
 // Neurons [first group, ...) advanced through the window's wl steps.  One
 // group of four neurons per lane per pass: its state is loaded once, its
 // input slots four steps at a time, the steps run in registers, the state is
-// stored once.
+// stored once, and the pass's spikes of all its steps are compacted into the
+// steps' history slots together at the end.  The lane at position p of a
+// pass takes group (p + upd_rot) mod groups (the host's rotation puts the
+// POISSON groups on lanes without an extra pass).
 template <bool CUR, bool FX, int WMAX, bool PULL>
 __device__ __forceinline__ void neuron_window(const StepArgs& a, int64_t w0, int wl, int32_t hs0, int64_t warp,
                                               int64_t nwarps)

@@ -20,9 +20,11 @@ __global__ void k_rate_to_v(const int8_t* type, const float* rate, float* V, int
 
 // The current step's arrivals from buffer s & from_mask to s & to_mask (both
 // accumulators; `words`: 32-bit words per entry).  Between runs only that
-// buffer holds anything (the step kernels clear a buffer when its step's
-// update reads it, and every step form ends with nothing delivered past the
-// current step), so the target is zero and the source is left zero.
+// buffer holds input that an update reads (the step kernels clear a buffer
+// when its step's update reads it, and every step form ends with nothing
+// delivered past the current step; the windowed update leaves the slots of
+// groups of four POISSON neurons, whose update ignores them), so the target
+// holds nothing read and the source is left zero.
 __global__ void k_acc_move(float* acc_e, float* acc_i, const int64_t* step, int32_t from_mask, int32_t to_mask,
                            int64_t ns, int32_t words)
 {
