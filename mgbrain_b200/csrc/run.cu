@@ -48,8 +48,8 @@ __global__ void k_acc_move(float* acc_e, float* acc_i, const int64_t* step, int3
 // (StepArgs::upd_rot) for a grid of `grid` blocks: the lanes whose last pass
 // is the pass before the others' extra one take the POISSON groups, whose
 // draws make theirs the costliest passes, when those neurons form one range
-// of the network and fit there; else 0.  A multiple of 32, so that a warp's
-// groups stay consecutive.
+// of the network and fit there; else 0.  A multiple of 32 before it is taken
+// modulo the groups.
 int64_t update_rotation(const mgc_sim* s, int grid)
 {
     const int64_t groups = s->a.ns >> 2;
